@@ -1,0 +1,346 @@
+#!/usr/bin/env python3
+"""Headline benchmark: bit-exact product throughput of a 2^24 x 2^24-limb
+mpn_mul on one B200 (Gbit/s of product = 64 (an + bn) / t).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mpn24|mpn24x20]
+
+Prints one JSON line (rank 0).  Our arm:
+  value       device-resident throughput: operands already in HBM, K products
+              timed with CUDA events on the launching stream;
+  e2e         the same metric through the host-pointer C-ABI call
+              (gpu_mpn_ctx_mpn_mul) from pinned host buffers, host<->device
+              copies inside the timed region;
+  roofline    the dominant kernel's algorithmic bytes / its mean launch time
+              (CUDA events recorded by the library between launches);
+  cpu_baseline the reference's own fft_small (oracle/_ref, compiled from the
+              reference tree) timed on this host's cores.
+The reference arm (--impl reference) times that CPU implementation alone.
+Under torchrun each rank runs an independent replica (no collective on the
+data path); the device time is the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "bit-exact product Gbit/s, mpn_mul 2^24 limbs + uneven batch: learned vs plain"
+WORKLOADS = {
+    "mpn24": (1 << 24, 1 << 24, "mpn_mul 2^24 x 2^24 limbs, uniform random limbs"),
+    "mpn24x20": (1 << 24, 1 << 20, "mpn_mul 2^24 x 2^20 limbs (unbalanced), uniform random limbs"),
+    # profiling-sized case: operands 64 MB, residues 320 MB (larger than L2)
+    "mpn22": (1 << 22, 1 << 22, "mpn_mul 2^22 x 2^22 limbs, uniform random limbs"),
+}
+NS_LIMB_BITS = 64
+
+
+def splitmix_limbs(seed, n):
+    """Same generator as the test fixtures (splitmix64), vectorised."""
+    i = np.arange(1, n + 1, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        x = np.uint64(seed) + i * np.uint64(0x9E3779B97F4A7C15)
+        x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        x = x ^ (x >> np.uint64(31))
+    if n and x[-1] == 0:
+        x[-1] = 1
+    return x
+
+
+def to_int(x):
+    return int.from_bytes(np.ascontiguousarray(x, dtype=np.uint64).tobytes(), "little")
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def ref_library():
+    import oracle
+    if oracle.have_ref():
+        L = oracle.ref()
+        n = os.cpu_count() or 1
+        L.flint_set_num_threads(n)
+        return L, "reference", n
+    return None, "port", 1
+
+
+def cpu_baseline_run(an, bn, steps, warmup, max_seconds=60.0):
+    """Time the reference's fft_small mpn_mul (or, when it is not built, the
+    oracle's C restatement on a smaller sample) on this host."""
+    import oracle
+    L, kind, nthreads = ref_library()
+    if L is not None:
+        a, b = splitmix_limbs(3, an), splitmix_limbs(4, bn)
+        fn = lambda: oracle.ref_mpn_mul(a, b)  # noqa: E731
+        sample = "full %dx%d-limb product per step" % (an, bn)
+        bits = NS_LIMB_BITS * (an + bn)
+        # fft_small caps its pool at 8 threads (mpn_mul.c:1257)
+        cores = min(nthreads, 8)
+    else:
+        n = 1 << 16
+        a, b = splitmix_limbs(3, n), splitmix_limbs(4, n)
+        fn = lambda: oracle.port_mpn_mul(a, b)  # noqa: E731
+        sample = "2^16 x 2^16-limb product per step (C restatement, 1 thread)"
+        bits = NS_LIMB_BITS * 2 * n
+        cores = 1
+    for _ in range(max(warmup, 1)):
+        fn()
+    times = []
+    t_all = time.perf_counter()
+    for _ in range(steps):
+        t = time.perf_counter()
+        fn()
+        times.append(time.perf_counter() - t)
+        if time.perf_counter() - t_all > max_seconds:
+            break
+    med = statistics.median(times)
+    return {"value": bits / med / 1e9, "unit": "Gbit/s", "cores": cores, "kind": kind,
+            "sample": sample + ", median of %d, host threads available %d" %
+            (len(times), os.cpu_count() or 1),
+            "ms_per_step": med * 1e3, "steps_timed": len(times)}
+
+
+def kernel_bytes(name, an, bn, np_, M, L):
+    """Algorithmic bytes each kernel must move in the four-pass design:
+    residues are 4-byte words, np primes, M-point transforms."""
+    r = 4 * np_ * M
+    return {
+        "k_fwd_cols": 8 * (an + bn) + 2 * r,      # limbs in, a and b residues out
+        "k_rows": 3 * r,                          # a, b rows in, product rows out
+        "k_inv_cols": 2 * r,                      # in place
+        "k_crt_carry": 4 * np_ * L + 8 * (an + bn),   # residues in, limbs out
+    }[name]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mpn24", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    an, bn, desc = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    config = {"workload": desc + " (configs[1])" if args.workload == "mpn24" else desc,
+              "an": an, "bn": bn}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        cb = cpu_baseline_run(an, bn, args.steps, args.warmup, max_seconds=240.0)
+        line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "Gbit/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (splitmix64 limbs)",
+                "config": dict(config, parallelism="host threads"),
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": cb["value"], "unit": "Gbit/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import flint_b200 as FB
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    a = splitmix_limbs(3 + 1000 * rank, an)
+    b = splitmix_limbs(4 + 1000 * rank, bn)
+    ctx = FB.MpnCtx()
+    np_, logM = FB.mpn_mul_plan(an, bn)
+    M, L = 1 << logM, an + bn - 1
+    da = torch.from_numpy(a.view(np.int64)).to(dev)
+    db = torch.from_numpy(b.view(np.int64)).to(dev)
+    dz = torch.empty(an + bn, dtype=torch.int64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        ctx.mpn_mul_device(dz.data_ptr(), da.data_ptr(), an, db.data_ptr(), bn, stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize(dev)
+    # exactness spot check of the benchmarked output: residues mod 61-bit primes
+    z = dz.cpu().numpy().view(np.uint64)
+    ai, bi, zi = to_int(a), to_int(b), to_int(z)
+    verified = all((ai % q) * (bi % q) % q == zi % q
+                   for q in (2305843009213693951, 2305843009213693921))
+
+    clocks = ClockSampler(local)
+    ctx.set_timing(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    ktimes = ctx.kernel_times()
+    ctx.set_timing(False)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    gbits_step = NS_LIMB_BITS * (an + bn) / 1e9
+    value = world * gbits_step / (ms_step / 1e3)
+
+    # e2e: host-pointer C-ABI call from pinned host buffers
+    ha = torch.from_numpy(a.view(np.int64)).pin_memory()
+    hb = torch.from_numpy(b.view(np.int64)).pin_memory()
+    hz = torch.empty(an + bn, dtype=torch.int64).pin_memory()
+    lib = FB.lib()
+
+    def e2e_step():
+        rc = lib.gpu_mpn_ctx_mpn_mul_status(ctx.ptr, hz.data_ptr(), ha.data_ptr(), an,
+                                            hb.data_ptr(), bn)
+        if rc:
+            raise RuntimeError(lib.gpu_fft_small_last_error().decode())
+
+    for _ in range(2):
+        e2e_step()
+    e2e_steps = max(3, min(args.steps, 10))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    clk = clocks.stop()
+    e2e_ok = bool(np.array_equal(hz.numpy().view(np.uint64), z))
+
+    peak, peak_kind = load_peaks()
+    kern = {}
+    for name, (tot, cnt) in ktimes.items():
+        if cnt:
+            per = tot / cnt
+            byt = kernel_bytes(name, an, bn, np_, M, L)
+            kern[name] = {"ms_per_launch": per, "share": None, "alg_bytes": byt,
+                          "GBps": byt / (per / 1e3) / 1e9}
+    tot_ms = sum(v["ms_per_launch"] for v in kern.values()) or 1.0
+    for v in kern.values():
+        v["share"] = v["ms_per_launch"] / tot_ms
+    dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
+    alg_pipeline = 208 * (an + bn)
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["GBps"], "peak": peak,
+                "unit": "GB/s", "frac": kern[dom]["GBps"] / peak, "traffic": None,
+                "peak_kind": peak_kind,
+                "pipeline": {"alg_bytes": alg_pipeline,
+                             "achieved": alg_pipeline / (ms_step / 1e3) / 1e9,
+                             "frac": alg_pipeline / (ms_step / 1e3) / 1e9 / peak},
+                "kernels": kern}
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline_run(an, bn, steps=2, warmup=1, max_seconds=30.0)
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    line = {
+        "metric": METRIC, "value": value, "unit": "Gbit/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (splitmix64 uniform limbs, top limb nonzero)",
+        "config": dict(config, primes=np_, transform="2^%d four-step" % logM,
+                       l2="inputs larger than L2 (%d MB operands)" % ((an + bn) * 8 >> 20),
+                       parallelism="replicas" if world > 1 else "single GPU"),
+        "verified_mod_q": bool(verified), "e2e_matches_device": e2e_ok,
+        "e2e": {"value": world * gbits_step / e2e_s, "unit": "Gbit/s",
+                "h2d_bytes_per_step": 8 * (an + bn), "d2h_bytes_per_step": 8 * (an + bn),
+                "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": 4 * args.steps,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

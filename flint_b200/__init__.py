@@ -1,0 +1,190 @@
+"""flint_b200 -- B200 small-prime NTT multiplication (FLINT fft_small, mpn_ctx route).
+
+Python mirror of the C ABI in include/gpu_fft_small.h, bound with ctypes to
+the in-tree CUDA library libflint_b200.so.  Names follow the reference's
+functions (src/fft_small.h):
+
+    MpnCtx(p)                      mpn_ctx_init / mpn_ctx_clear
+    MpnCtx.mpn_mul(a, b)           mpn_ctx_mpn_mul
+    MpnCtx.mpn_mul_range(..)       _mpn_ctx_mpn_mul_range
+    MpnCtx.nmod_poly_mul_mid(..)   _nmod_poly_mul_mid_mpn_ctx
+    MpnCtx.mpn_mul_device(..)      device-pointer twin (no host copies)
+
+There is no CPU fallback: if the library or a GPU is missing, every call
+raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libflint_b200.so")
+DEFAULT_PRIME = 0x0003F00000000001
+
+OK, EINVAL, ETOOBIG, ECUDA, ETIMEOUT, ENOPRIMES = 0, 1, 2, 3, 4, 5
+
+_lib = None
+
+
+class GpuFftSmallError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("gpu_fft_small error %d: %s" % (code, msg))
+        self.code = code
+
+
+class _Ctx(ctypes.Structure):
+    _fields_ = [("impl", ctypes.c_void_p)]
+
+
+class _Nmod(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_ulong), ("ninv", ctypes.c_ulong), ("norm", ctypes.c_ulong)]
+
+
+# symbol -> (restype, argtypes); every symbol include/gpu_fft_small.h declares
+_P = ctypes.c_void_p
+_U = ctypes.c_ulong
+_S = ctypes.c_long
+_CTX = ctypes.POINTER(_Ctx)
+SIGNATURES = {
+    "gpu_mpn_ctx_init": (None, [_CTX, _U]),
+    "gpu_mpn_ctx_init_status": (ctypes.c_int, [_CTX, _U]),
+    "gpu_mpn_ctx_clear": (None, [_CTX]),
+    "gpu_mpn_ctx_mpn_mul": (None, [_CTX, _P, _P, _U, _P, _U]),
+    "gpu_mpn_ctx_mpn_mul_status": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U]),
+    "_gpu_mpn_ctx_mpn_mul_range": (None, [_CTX, _P, _U, _U, _P, _U, _P, _U]),
+    "gpu_mpn_mul_device": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, _P]),
+    "_gpu_nmod_poly_mul_mid_mpn_ctx": (None, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
+    "_gpu_nmod_poly_mul_mid_status": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
+    "gpu_get_default_mpn_ctx": (_CTX, []),
+    "gpu_mpn_mul_default_mpn_ctx": (None, [_P, _P, _S, _P, _S]),
+    "_gpu_nmod_poly_mul_mid_default_mpn_ctx": (None, [_P, _S, _S, _P, _S, _P, _S, _Nmod]),
+    "gpu_fft_small_set_throw": (None, [_P]),
+    "gpu_fft_small_last_error": (ctypes.c_char_p, []),
+    "gpu_mpn_mul_plan": (ctypes.c_int, [_U, _U, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_int)]),
+    "gpu_fft_small_prime": (_U, [ctypes.c_int]),
+    "gpu_mpn_ctx_last_launches": (ctypes.c_int, [_CTX]),
+    "gpu_mpn_ctx_set_timing": (ctypes.c_int, [_CTX, ctypes.c_int]),
+    "gpu_mpn_ctx_kernel_times": (ctypes.c_int, [_CTX, ctypes.POINTER(ctypes.c_double),
+                                                ctypes.POINTER(ctypes.c_long), ctypes.c_int]),
+}
+
+KERNEL_SLOTS = ("k_fwd_cols", "k_rows", "k_inv_cols", "k_crt_carry")
+
+
+def lib():
+    """Load libflint_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libflint_b200.so is not built; run "
+                              "`python -m flint_b200.build` (needs nvcc)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise GpuFftSmallError(rc, lib().gpu_fft_small_last_error().decode())
+
+
+def _limbs(x):
+    x = np.ascontiguousarray(x, dtype=np.uint64)
+    if x.ndim != 1:
+        raise ValueError("limb arrays are one-dimensional")
+    return x
+
+
+def mpn_mul_plan(an, bn):
+    """(number of primes, log2 transform length) the GPU path uses."""
+    np_, lm = ctypes.c_int(), ctypes.c_int()
+    _check(lib().gpu_mpn_mul_plan(an, bn, ctypes.byref(np_), ctypes.byref(lm)))
+    return np_.value, lm.value
+
+
+def prime(i):
+    return int(lib().gpu_fft_small_prime(i))
+
+
+class MpnCtx:
+    """GPU counterpart of mpn_ctx_t (src/fft_small.h:382-433)."""
+
+    def __init__(self, p=DEFAULT_PRIME):
+        self._c = _Ctx()
+        _check(lib().gpu_mpn_ctx_init_status(ctypes.byref(self._c), p))
+
+    @property
+    def ptr(self):
+        return ctypes.byref(self._c)
+
+    def close(self):
+        if self._c.impl:
+            lib().gpu_mpn_ctx_clear(ctypes.byref(self._c))
+            self._c.impl = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mpn_mul(self, a, b, out=None):
+        """a * b as an+bn limbs (mpn_ctx_mpn_mul)."""
+        a = _limbs(a)
+        b = a if b is a else _limbs(b)
+        an, bn = len(a), len(b)
+        z = np.empty(an + bn, dtype=np.uint64) if out is None else out
+        _check(lib().gpu_mpn_ctx_mpn_mul_status(self.ptr, z.ctypes.data, a.ctypes.data, an,
+                                                b.ctypes.data, bn))
+        return z
+
+    def mpn_mul_range(self, lo, hi, a, b):
+        """limbs [lo, hi) of a * b (_mpn_ctx_mpn_mul_range, exact)."""
+        a = _limbs(a)
+        b = a if b is a else _limbs(b)
+        z = np.empty(max(hi - lo, 0), dtype=np.uint64)
+        if hi > lo:
+            lib()._gpu_mpn_ctx_mpn_mul_range(self.ptr, z.ctypes.data, lo, hi, a.ctypes.data,
+                                             len(a), b.ctypes.data, len(b))
+        return z
+
+    def mpn_mul_device(self, z_ptr, a_ptr, an, b_ptr, bn, stream=None):
+        """Queue z = a * b on device pointers (ints); returns without syncing."""
+        _check(lib().gpu_mpn_mul_device(self.ptr, z_ptr, a_ptr, an, b_ptr, bn, stream))
+
+    def nmod_poly_mul_mid(self, zl, zh, a, b, n):
+        """coefficients [zl, zh) of a * b mod n (_nmod_poly_mul_mid_mpn_ctx)."""
+        a = _limbs(a)
+        b = a if b is a else _limbs(b)
+        z = np.empty(max(zh - zl, 0), dtype=np.uint64)
+        _check(lib()._gpu_nmod_poly_mul_mid_status(z.ctypes.data, zl, zh, a.ctypes.data, len(a),
+                                                   b.ctypes.data, len(b), _Nmod(n, 0, 0),
+                                                   self.ptr))
+        return z
+
+    @property
+    def last_launches(self):
+        return int(lib().gpu_mpn_ctx_last_launches(self.ptr))
+
+    def set_timing(self, on=True):
+        """Per-kernel CUDA-event timing on the launching stream (resets totals)."""
+        _check(lib().gpu_mpn_ctx_set_timing(self.ptr, 1 if on else 0))
+
+    def kernel_times(self):
+        """{kernel: (total ms, launches)} since the last set_timing()."""
+        ms = (ctypes.c_double * 8)()
+        cnt = (ctypes.c_long * 8)()
+        n = lib().gpu_mpn_ctx_kernel_times(self.ptr, ms, cnt, 8)
+        return {KERNEL_SLOTS[k]: (ms[k], cnt[k]) for k in range(n)}

@@ -1,0 +1,731 @@
+// Host side of the B200 small-prime NTT multiplication library: context
+// set-up (primes, twiddle and CRT tables), plan selection, kernel launches
+// and the C ABI declared in include/gpu_fft_small.h.
+//
+// Everything here is plain CUDA runtime + C++; no torch types cross the ABI.
+#include "../../include/gpu_fft_small.h"
+#include "mpn_kernels.cuh"
+#include "nmod_kernels.cuh"
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <algorithm>
+#include <string>
+#include <vector>
+
+using namespace fb;
+
+// ---------------------------------------------------------------------------
+// Prime set: every prime 2^30 < p < 2^31 with 2^25 | p - 1, largest first,
+// plus the two smaller ones with the same 2-adic valuation.  Five of them
+// hold coefficients of 64-bit-chunk products up to min(an, bn) ~ 2^24.3
+// limbs; six go to ~2^53.
+static const uint32_t PRIMES[MAX_NP] = {
+    2113929217u, 2013265921u, 1811939329u, 1711276033u, 1107296257u,
+    469762049u, 167772161u};
+
+// ---------------------------------------------------------------------------
+// errors
+static thread_local std::string g_last_error;
+static void (*g_throw_handler)(int, const char *) = nullptr;
+
+static int set_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+static void raise_error(int code)
+{
+    if (g_throw_handler) {
+        g_throw_handler(code, g_last_error.c_str());
+        return;
+    }
+    fprintf(stderr, "gpu_fft_small: error %d: %s\n", code, g_last_error.c_str());
+    fflush(stderr);
+    abort();
+}
+
+#define CU(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess)                                                \
+            return set_error(GPU_FFT_SMALL_ECUDA, "%s: %s (%s:%d)", #call,    \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);     \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// host number theory
+static uint32_t primitive_root(uint32_t p)
+{
+    uint32_t m = p - 1;
+    std::vector<uint32_t> f;
+    for (uint32_t q = 2; (uint64_t)q * q <= m; q++)
+        if (m % q == 0) {
+            f.push_back(q);
+            while (m % q == 0) m /= q;
+        }
+    if (m > 1) f.push_back(m);
+    for (uint32_t g = 2;; g++) {
+        bool ok = true;
+        for (uint32_t q : f)
+            if (h_powmod(g, (p - 1) / q, p) == 1) { ok = false; break; }
+        if (ok) return g;
+    }
+}
+
+static uint2 shoup_pair(uint32_t w, uint32_t p)
+{
+    return make_uint2(w, shoup_companion(w, p));
+}
+
+// multiword helpers, 32-bit little-endian words
+static void mw_mul_small(std::vector<uint32_t> &x, uint32_t m)
+{
+    uint64_t c = 0;
+    for (auto &w : x) {
+        uint64_t t = (uint64_t)w * m + c;
+        w = (uint32_t)t;
+        c = t >> 32;
+    }
+    if (c) x.push_back((uint32_t)c);
+}
+
+static std::vector<uint32_t> mw_div_small(const std::vector<uint32_t> &x, uint32_t d)
+{
+    std::vector<uint32_t> q(x.size());
+    uint64_t r = 0;
+    for (size_t i = x.size(); i-- > 0;) {
+        uint64_t t = (r << 32) | x[i];
+        q[i] = (uint32_t)(t / d);
+        r = t % d;
+    }
+    while (q.size() > 1 && q.back() == 0) q.pop_back();
+    return q;
+}
+
+static uint32_t mw_mod_small(const std::vector<uint32_t> &x, uint32_t d)
+{
+    uint64_t r = 0;
+    for (size_t i = x.size(); i-- > 0;) r = ((r << 32) | x[i]) % d;
+    return (uint32_t)r;
+}
+
+static double log2_product(int np)
+{
+    double s = 0;
+    for (int j = 0; j < np; j++) s += log2((double)PRIMES[j]);
+    return s;
+}
+
+// ---------------------------------------------------------------------------
+// context
+
+// Per-kernel timing record: events before the first and after each of the
+// four kernels of one product (slot k spans ev[k] .. ev[k+1]).
+constexpr int TIMING_SLOTS = 4;
+constexpr size_t TIMING_RING = 512;
+struct TimingRecord {
+    cudaEvent_t ev[TIMING_SLOTS + 1];
+    bool used;
+};
+
+struct Ctx;
+static TimingRecord *timing_begin(Ctx *X, cudaStream_t st);
+static void timing_mark(TimingRecord *r, int k, cudaStream_t st)
+{
+    if (r) cudaEventRecord(r->ev[k], st);
+}
+
+struct Ctx {
+    int device = -1;
+    gpu_ulong p0 = 0;
+    cudaStream_t stream = nullptr;
+    void *d_tables = nullptr;
+    DevTables T{};
+    uint32_t *d_scale = nullptr;          // [MAX_NP]
+    int *d_err = nullptr;
+    unsigned long long *d_ticket = nullptr;
+    unsigned long long ticket_base = 0;
+    uint32_t *d_status = nullptr;
+    size_t status_cap = 0;                // tiles
+    uint32_t epoch = 0;
+    uint32_t *d_res = nullptr;
+    size_t res_cap = 0;                   // bytes
+    uint64_t *d_io = nullptr;
+    size_t io_cap = 0;                    // bytes
+    int last_launches = 0;
+    // opt-in per-kernel timing: a ring of event records, read lazily
+    bool timing = false;
+    std::vector<TimingRecord> rec;
+    size_t rec_head = 0, rec_tail = 0;
+    double kernel_ms[TIMING_SLOTS] = {0};
+    long kernel_count[TIMING_SLOTS] = {0};
+    CrtConst crt[MAX_NP + 1];
+    uint32_t cof_red[MAX_NP + 1][MAX_NP]; // (P/p_j) mod p_j for each np
+};
+
+static int grow(void **ptr, size_t *cap, size_t need)
+{
+    if (need <= *cap) return 0;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    size_t sz = std::max(need, *cap + *cap / 8);
+    CU(cudaMalloc(ptr, sz));
+    *cap = sz;
+    return 0;
+}
+
+static int ctx_build_tables(Ctx *X)
+{
+    const size_t n_twf = (size_t)MAX_NP * TW_SZ;
+    const size_t n_th = (size_t)MAX_NP * TH_SZ;
+    const size_t n_tl = (size_t)MAX_NP * TL_SZ;
+    std::vector<PrimeInfo> pi(MAX_NP);
+    std::vector<uint2> twf(n_twf), twi(n_twf), th(n_th), tl(n_tl), thi(n_th), tli(n_tl);
+    for (int j = 0; j < MAX_NP; j++) {
+        const uint32_t p = PRIMES[j];
+        PrimeInfo &P = pi[j];
+        memset(&P, 0, sizeof P);
+        P.p = p;
+        uint32_t inv = 1;                 // p^-1 mod 2^32 by Newton iteration
+        for (int it = 0; it < 5; it++) inv *= 2 - p * inv;
+        P.pneg_inv = 0u - inv;
+        P.c32 = (uint32_t)((1ull << 32) % p);
+        P.r2 = h_mulmod(P.c32, P.c32, p);
+        P.finv = 1.0f / (float)p;
+        const uint32_t g = primitive_root(p);
+        const uint32_t w = h_powmod(g, (p - 1) >> LOG_MAXM, p);   // order 2^25
+        const uint32_t wi = h_invmod(w, p);
+        // local twiddles: entry h + jj = w_{2h}^jj, w_{2h} = w^(2^25 / 2h)
+        twf[(size_t)j * TW_SZ] = make_uint2(1, 0);
+        twi[(size_t)j * TW_SZ] = make_uint2(1, 0);
+        for (int h = 1; h < TW_SZ; h <<= 1) {
+            const int lh = __builtin_ctz(h);
+            const uint32_t r = h_powmod(w, 1ull << (LOG_MAXM - lh - 1), p);
+            const uint32_t ri = h_powmod(wi, 1ull << (LOG_MAXM - lh - 1), p);
+            uint32_t x = 1, xi = 1;
+            for (int jj = 0; jj < h; jj++) {
+                twf[(size_t)j * TW_SZ + h + jj] = shoup_pair(x, p);
+                twi[(size_t)j * TW_SZ + h + jj] = shoup_pair(xi, p);
+                x = h_mulmod(x, r, p);
+                xi = h_mulmod(xi, ri, p);
+            }
+        }
+        // twist tables
+        {
+            const uint32_t step = h_powmod(w, 1u << 13, p), stepi = h_powmod(wi, 1u << 13, p);
+            uint32_t x = 1, xi = 1;
+            for (int t = 0; t < TH_SZ; t++) {
+                th[(size_t)j * TH_SZ + t] = shoup_pair(x, p);
+                thi[(size_t)j * TH_SZ + t] = shoup_pair(xi, p);
+                x = h_mulmod(x, step, p);
+                xi = h_mulmod(xi, stepi, p);
+            }
+            x = 1; xi = 1;
+            for (int t = 0; t < TL_SZ; t++) {
+                tl[(size_t)j * TL_SZ + t] = shoup_pair(x, p);
+                tli[(size_t)j * TL_SZ + t] = shoup_pair(xi, p);
+                x = h_mulmod(x, w, p);
+                xi = h_mulmod(xi, wi, p);
+            }
+        }
+    }
+    // CRT constants for every prime count
+    for (int np = 1; np <= MAX_NP; np++) {
+        CrtConst &K = X->crt[np];
+        memset(&K, 0, sizeof K);
+        K.np = np;
+        std::vector<uint32_t> P = {1};
+        for (int j = 0; j < np; j++) mw_mul_small(P, PRIMES[j]);
+        for (size_t w = 0; w < P.size() && w < (size_t)MAX_NP; w++) K.P[w] = P[w];
+        for (int j = 0; j < np; j++) {
+            std::vector<uint32_t> c = mw_div_small(P, PRIMES[j]);
+            for (size_t w = 0; w < c.size() && w < (size_t)MAX_NP; w++) K.cof[j][w] = c[w];
+            X->cof_red[np][j] = mw_mod_small(c, PRIMES[j]);
+            K.finv[j] = 1.0f / (float)PRIMES[j];
+        }
+    }
+
+    size_t off = 0;
+    auto place = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~(size_t)255; return o; };
+    const size_t o_pi = place(sizeof(PrimeInfo) * MAX_NP);
+    const size_t o_twf = place(sizeof(uint2) * n_twf), o_twi = place(sizeof(uint2) * n_twf);
+    const size_t o_th = place(sizeof(uint2) * n_th), o_tl = place(sizeof(uint2) * n_tl);
+    const size_t o_thi = place(sizeof(uint2) * n_th), o_tli = place(sizeof(uint2) * n_tl);
+    CU(cudaMalloc(&X->d_tables, off));
+    char *base = (char *)X->d_tables;
+    CU(cudaMemcpy(base + o_pi, pi.data(), sizeof(PrimeInfo) * MAX_NP, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_twf, twf.data(), sizeof(uint2) * n_twf, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_twi, twi.data(), sizeof(uint2) * n_twf, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_th, th.data(), sizeof(uint2) * n_th, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_tl, tl.data(), sizeof(uint2) * n_tl, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_thi, thi.data(), sizeof(uint2) * n_th, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_tli, tli.data(), sizeof(uint2) * n_tl, cudaMemcpyHostToDevice));
+    X->T.pi = (const PrimeInfo *)(base + o_pi);
+    X->T.twf = (const uint2 *)(base + o_twf);
+    X->T.twi = (const uint2 *)(base + o_twi);
+    X->T.th = (const uint2 *)(base + o_th);
+    X->T.tl = (const uint2 *)(base + o_tl);
+    X->T.thi = (const uint2 *)(base + o_thi);
+    X->T.tli = (const uint2 *)(base + o_tli);
+    return 0;
+}
+
+static int configure_kernels()
+{
+    static bool done = false;
+    if (done) return 0;
+    CU(cudaFuncSetAttribute(k_fwd_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    CU(cudaFuncSetAttribute(k_inv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    CU(cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    done = true;
+    return 0;
+}
+
+static int ctx_create(Ctx **out, gpu_ulong p)
+{
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0)
+        return set_error(GPU_FFT_SMALL_ECUDA, "no CUDA device available (%s)",
+                         e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+    Ctx *X = new Ctx();
+    X->p0 = p;
+    int rc = 0;
+    if (cudaGetDevice(&X->device) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaGetDevice failed");
+    if (!rc && cudaStreamCreateWithFlags(&X->stream, cudaStreamNonBlocking) != cudaSuccess)
+        rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaStreamCreate failed");
+    if (!rc) rc = configure_kernels();
+    if (!rc) rc = ctx_build_tables(X);
+    if (!rc) {
+        cudaError_t e1 = cudaMalloc(&X->d_scale, sizeof(uint32_t) * MAX_NP);
+        cudaError_t e2 = cudaMalloc(&X->d_err, sizeof(int));
+        cudaError_t e3 = cudaMalloc(&X->d_ticket, sizeof(unsigned long long));
+        if (e1 || e2 || e3) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaMalloc of context state failed");
+        else {
+            cudaMemset(X->d_err, 0, sizeof(int));
+            cudaMemset(X->d_ticket, 0, sizeof(unsigned long long));
+        }
+    }
+    if (rc) {
+        delete X;
+        return rc;
+    }
+    *out = X;
+    return 0;
+}
+
+// fold finished records into the per-kernel totals (blocks on pending ones)
+static void timing_drain(Ctx *X)
+{
+    while (X->rec_tail != X->rec_head) {
+        TimingRecord &r = X->rec[X->rec_tail % TIMING_RING];
+        cudaEventSynchronize(r.ev[TIMING_SLOTS]);
+        for (int k = 0; k < TIMING_SLOTS; k++) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, r.ev[k], r.ev[k + 1]) == cudaSuccess) {
+                X->kernel_ms[k] += ms;
+                X->kernel_count[k]++;
+            }
+        }
+        X->rec_tail++;
+    }
+}
+
+static TimingRecord *timing_begin(Ctx *X, cudaStream_t st)
+{
+    if (!X->timing) return nullptr;
+    if (X->rec.empty()) {
+        X->rec.resize(TIMING_RING);
+        for (auto &r : X->rec) {
+            for (auto &e : r.ev) cudaEventCreate(&e);
+            r.used = true;
+        }
+    }
+    if (X->rec_head - X->rec_tail >= TIMING_RING) {   // ring full: fold the oldest
+        TimingRecord &r = X->rec[X->rec_tail % TIMING_RING];
+        cudaEventSynchronize(r.ev[TIMING_SLOTS]);
+        for (int k = 0; k < TIMING_SLOTS; k++) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, r.ev[k], r.ev[k + 1]) == cudaSuccess) {
+                X->kernel_ms[k] += ms;
+                X->kernel_count[k]++;
+            }
+        }
+        X->rec_tail++;
+    }
+    TimingRecord *r = &X->rec[X->rec_head % TIMING_RING];
+    X->rec_head++;
+    cudaEventRecord(r->ev[0], st);
+    return r;
+}
+
+static void ctx_destroy(Ctx *X)
+{
+    if (!X) return;
+    if (X->stream) cudaStreamSynchronize(X->stream);
+    for (auto &r : X->rec)
+        for (auto &e : r.ev) cudaEventDestroy(e);
+    cudaFree(X->d_tables);
+    cudaFree(X->d_scale);
+    cudaFree(X->d_err);
+    cudaFree(X->d_ticket);
+    cudaFree(X->d_status);
+    cudaFree(X->d_res);
+    cudaFree(X->d_io);
+    if (X->stream) cudaStreamDestroy(X->stream);
+    delete X;
+}
+
+// ---------------------------------------------------------------------------
+// plans
+struct MulPlan {
+    int np;
+    int logM;
+    MulShape S;
+};
+
+static int ceil_log2_u64(uint64_t x)
+{
+    int l = 0;
+    while (((uint64_t)1 << l) < x) l++;
+    return l;
+}
+
+static int plan_mpn(uint64_t an, uint64_t bn, MulPlan *P)
+{
+    if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
+    const uint64_t L = an + bn - 1;
+    const uint64_t mn = std::min(an, bn);
+    // every coefficient is < mn 2^128; the CRT needs P > 2 * bound
+    const double need = log2((double)mn) + 128.0 + 1.0 + 1e-3;
+    int np = 0;
+    for (int k = 1; k <= 6; k++)
+        if (log2_product(k) > need) { np = k; break; }
+    if (np == 0) return set_error(GPU_FFT_SMALL_ENOPRIMES, "operand length %llu beyond the prime set",
+                                  (unsigned long long)mn);
+    np = std::max(np, 5);
+    int logM = std::max(ceil_log2_u64(L), 4);
+    if (logM > LOG_MAXM)
+        return set_error(GPU_FFT_SMALL_ETOOBIG, "product of %llu coefficients exceeds 2^%d",
+                         (unsigned long long)L, LOG_MAXM);
+    P->np = np;
+    P->logM = logM;
+    P->S.logC = std::min(logM, 13);
+    P->S.logR = logM - P->S.logC;
+    const int R = 1 << P->S.logR, C = 1 << P->S.logC;
+    P->S.G = std::min(C, std::max(8, (1 << 14) / R));
+    return 0;
+}
+
+// pointwise scale: M^-1 (P/p_j)^-1 2^128, see k_rows / limb_redc
+static void fill_scale(const Ctx *X, int np, int logM, uint32_t *scale, int extra_redc)
+{
+    for (int j = 0; j < np; j++) {
+        const uint32_t p = PRIMES[j];
+        uint32_t s = h_invmod(h_powmod(2, logM, p), p);
+        s = h_mulmod(s, h_invmod(X->cof_red[np][j], p), p);
+        s = h_mulmod(s, h_powmod(2, 32 * (uint64_t)extra_redc, p), p);
+        scale[j] = s;
+    }
+}
+
+static int ensure_status(Ctx *X, size_t tiles)
+{
+    if (tiles <= X->status_cap) return 0;
+    if (X->d_status) cudaFree(X->d_status);
+    X->d_status = nullptr;
+    X->status_cap = 0;
+    CU(cudaMalloc(&X->d_status, tiles * sizeof(uint32_t)));
+    CU(cudaMemsetAsync(X->d_status, 0, tiles * sizeof(uint32_t), X->stream));
+    X->status_cap = tiles;
+    return 0;
+}
+
+// Enqueue z = a * b on `st` with device pointers.
+static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
+                           const uint64_t *b, uint64_t bn, cudaStream_t st)
+{
+    MulPlan P;
+    int rc = plan_mpn(an, bn, &P);
+    if (rc) return rc;
+    const bool sq = (a == b) && (an == bn);
+    const int np = P.np, logM = P.logM;
+    const size_t M = (size_t)1 << logM;
+    const size_t res_bytes = (sq ? 1 : 2) * (size_t)np * M * sizeof(uint32_t);
+    rc = grow((void **)&X->d_res, &X->res_cap, res_bytes);
+    if (rc) return rc;
+    uint32_t *ra = X->d_res, *rb = X->d_res + (size_t)np * M;
+    uint32_t scale[MAX_NP];
+    fill_scale(X, np, logM, scale, 4);
+    CU(cudaMemcpyAsync(X->d_scale, scale, sizeof(uint32_t) * np, cudaMemcpyHostToDevice, st));
+
+    const int R = 1 << P.S.logR, C = 1 << P.S.logC, G = P.S.G;
+    const size_t col_smem = (size_t)R * G * sizeof(uint32_t);
+    const size_t row_smem = (size_t)2 * C * sizeof(uint32_t);
+    const uint64_t zn = an + bn;
+    constexpr int THREADS = 256, TILE = 4 * THREADS;
+    const size_t tiles = (zn + TILE - 1) / TILE;
+    rc = ensure_status(X, tiles);
+    if (rc) return rc;
+    X->epoch = (X->epoch + 1) & 0x0fffffffu;
+    if (X->epoch == 0) {   // epoch wrapped: clear stale status words
+        CU(cudaMemsetAsync(X->d_status, 0, X->status_cap * sizeof(uint32_t), st));
+        X->epoch = 1;
+    }
+    const CrtConst &K = X->crt[np];
+
+    int launches = 0;
+    TimingRecord *tr = timing_begin(X, st);
+    k_fwd_cols<<<dim3(C / G, np, sq ? 1 : 2), 512, col_smem, st>>>(X->T, a, an, b, bn, ra, rb, P.S);
+    launches++;
+    timing_mark(tr, 1, st);
+    k_rows<<<dim3(R, np), 512, row_smem, st>>>(X->T, ra, rb, P.S, X->d_scale, sq ? 1 : 0);
+    launches++;
+    timing_mark(tr, 2, st);
+    k_inv_cols<<<dim3(C / G, np), 512, col_smem, st>>>(X->T, ra, P.S);
+    launches++;
+    timing_mark(tr, 3, st);
+    if (np == 5)
+        k_crt_carry<5, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
+                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err);
+    else
+        k_crt_carry<6, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
+                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err);
+    launches++;
+    timing_mark(tr, 4, st);
+    X->ticket_base += tiles;
+    X->last_launches = launches;
+    CU(cudaGetLastError());
+    return 0;
+}
+
+static int check_device_error(Ctx *X)
+{
+    int err = 0;
+    CU(cudaMemcpyAsync(&err, X->d_err, sizeof(int), cudaMemcpyDeviceToHost, X->stream));
+    CU(cudaStreamSynchronize(X->stream));
+    if (err) {
+        cudaMemsetAsync(X->d_err, 0, sizeof(int), X->stream);
+        return set_error(GPU_FFT_SMALL_ETIMEOUT, "carry look-back wait exceeded its limit");
+    }
+    return 0;
+}
+
+static int io_buffers(Ctx *X, size_t words, uint64_t **p)
+{
+    int rc = grow((void **)&X->d_io, &X->io_cap, words * sizeof(uint64_t));
+    if (rc) return rc;
+    *p = X->d_io;
+    return 0;
+}
+
+static Ctx *get_ctx(gpu_mpn_ctx_t R) { return (Ctx *)R->impl; }
+
+static int bind_device(Ctx *X)
+{
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != X->device) CU(cudaSetDevice(X->device));
+    return 0;
+}
+
+static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
+                        const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
+{
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    const bool sq = (a == b) && (an == bn);
+    const size_t zn = an + bn;
+    uint64_t *buf;
+    rc = io_buffers(X, (sq ? an : an + bn) + zn, &buf);
+    if (rc) return rc;
+    uint64_t *da = buf, *db = sq ? buf : buf + an, *dz = buf + (sq ? an : an + bn);
+    CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, X->stream));
+    if (!sq) CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, X->stream));
+    rc = mpn_mul_enqueue(X, dz, da, an, db, bn, X->stream);
+    if (rc) return rc;
+    const gpu_ulong top = std::min<gpu_ulong>(hi, zn);
+    if (top > lo) CU(cudaMemcpyAsync(z, dz + lo, (top - lo) * 8, cudaMemcpyDeviceToHost, X->stream));
+    rc = check_device_error(X);
+    if (rc) return rc;
+    if (hi > zn) memset(z + (zn > lo ? zn - lo : 0), 0, (hi - std::max<gpu_ulong>(zn, lo)) * 8);
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// nmod polynomials
+#include "nmod_host.inc"
+
+// ---------------------------------------------------------------------------
+// C ABI
+extern "C" {
+
+int gpu_mpn_ctx_init_status(gpu_mpn_ctx_t R, gpu_ulong p)
+{
+    R->impl = nullptr;
+    Ctx *X = nullptr;
+    int rc = ctx_create(&X, p);
+    if (rc) return rc;
+    R->impl = X;
+    return 0;
+}
+
+void gpu_mpn_ctx_init(gpu_mpn_ctx_t R, gpu_ulong p)
+{
+    int rc = gpu_mpn_ctx_init_status(R, p);
+    if (rc) raise_error(rc);
+}
+
+void gpu_mpn_ctx_clear(gpu_mpn_ctx_t R)
+{
+    ctx_destroy(get_ctx(R));
+    R->impl = nullptr;
+}
+
+int gpu_mpn_ctx_mpn_mul_status(gpu_mpn_ctx_t R, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
+                               const gpu_ulong *b, gpu_ulong bn)
+{
+    return mpn_mul_host(get_ctx(R), z, a, an, b, bn, 0, an + bn);
+}
+
+void gpu_mpn_ctx_mpn_mul(gpu_mpn_ctx_t R, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
+                         const gpu_ulong *b, gpu_ulong bn)
+{
+    int rc = gpu_mpn_ctx_mpn_mul_status(R, z, a, an, b, bn);
+    if (rc) raise_error(rc);
+}
+
+void _gpu_mpn_ctx_mpn_mul_range(gpu_mpn_ctx_t R, gpu_ulong *z, gpu_ulong lo, gpu_ulong hi,
+                                const gpu_ulong *a, gpu_ulong an, const gpu_ulong *b, gpu_ulong bn)
+{
+    if (lo >= hi) return;
+    int rc = mpn_mul_host(get_ctx(R), z, a, an, b, bn, lo, hi);
+    if (rc) raise_error(rc);
+}
+
+int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong an,
+                       const uint64_t *b_dev, gpu_ulong bn, void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn,
+                           stream ? (cudaStream_t)stream : X->stream);
+}
+
+int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
+                                  const gpu_ulong *a, gpu_ulong an, const gpu_ulong *b, gpu_ulong bn,
+                                  gpu_nmod_t mod, gpu_mpn_ctx_t R)
+{
+    return nmod_mul_mid_host(get_ctx(R), z, zl, zh, a, an, b, bn, mod.n);
+}
+
+void _gpu_nmod_poly_mul_mid_mpn_ctx(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
+                                    const gpu_ulong *a, gpu_ulong an, const gpu_ulong *b, gpu_ulong bn,
+                                    gpu_nmod_t mod, gpu_mpn_ctx_t R)
+{
+    int rc = _gpu_nmod_poly_mul_mid_status(z, zl, zh, a, an, b, bn, mod, R);
+    if (rc) raise_error(rc);
+}
+
+static thread_local gpu_mpn_ctx_struct g_default_ctx = {nullptr};
+static thread_local bool g_default_registered = false;
+
+struct DefaultCtxReaper {
+    ~DefaultCtxReaper() {}
+};
+
+gpu_mpn_ctx_struct *gpu_get_default_mpn_ctx(void)
+{
+    if (!g_default_ctx.impl) {
+        // same starting prime as the reference's DEFAULT_PRIME
+        gpu_mpn_ctx_init(&g_default_ctx, 0x0003f00000000001ull);
+        g_default_registered = true;
+    }
+    return &g_default_ctx;
+}
+
+void gpu_mpn_mul_default_mpn_ctx(gpu_ulong *r1, const gpu_ulong *i1, gpu_slong n1,
+                                 const gpu_ulong *i2, gpu_slong n2)
+{
+    gpu_mpn_ctx_mpn_mul(gpu_get_default_mpn_ctx(), r1, i1, (gpu_ulong)n1, i2, (gpu_ulong)n2);
+}
+
+void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gpu_slong zl, gpu_slong zh,
+                                            const gpu_ulong *a, gpu_slong an,
+                                            const gpu_ulong *b, gpu_slong bn, gpu_nmod_t mod)
+{
+    _gpu_nmod_poly_mul_mid_mpn_ctx(res, (gpu_ulong)zl, (gpu_ulong)zh, a, (gpu_ulong)an, b,
+                                   (gpu_ulong)bn, mod, gpu_get_default_mpn_ctx());
+}
+
+void gpu_fft_small_set_throw(void (*handler)(int code, const char *msg))
+{
+    g_throw_handler = handler;
+}
+
+const char *gpu_fft_small_last_error(void) { return g_last_error.c_str(); }
+
+int gpu_mpn_mul_plan(gpu_ulong an, gpu_ulong bn, int *np, int *logM)
+{
+    MulPlan P;
+    int rc = plan_mpn(an, bn, &P);
+    if (rc) return rc;
+    *np = P.np;
+    *logM = P.logM;
+    return 0;
+}
+
+gpu_ulong gpu_fft_small_prime(int i)
+{
+    return (i >= 0 && i < MAX_NP) ? PRIMES[i] : 0;
+}
+
+int gpu_mpn_ctx_last_launches(gpu_mpn_ctx_t R)
+{
+    Ctx *X = get_ctx(R);
+    return X ? X->last_launches : 0;
+}
+
+int gpu_mpn_ctx_set_timing(gpu_mpn_ctx_t R, int on)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    timing_drain(X);
+    for (int k = 0; k < TIMING_SLOTS; k++) {
+        X->kernel_ms[k] = 0;
+        X->kernel_count[k] = 0;
+    }
+    X->timing = on != 0;
+    return 0;
+}
+
+int gpu_mpn_ctx_kernel_times(gpu_mpn_ctx_t R, double *ms, long *count, int max)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return 0;
+    timing_drain(X);
+    const int n = std::min(max, TIMING_SLOTS);
+    for (int k = 0; k < n; k++) {
+        ms[k] = X->kernel_ms[k];
+        count[k] = X->kernel_count[k];
+    }
+    return n;
+}
+
+}  // extern "C"

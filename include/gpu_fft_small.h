@@ -1,0 +1,164 @@
+/*
+    gpu_fft_small.h -- C ABI of the B200 small-prime NTT multiplication path.
+
+    A drop-in, at function level, for the mpn_ctx route of FLINT's fft_small
+    module.  Each entry point has the shape of the reference function it
+    replaces (named beside it, file:line in the reference tree); the context
+    type is opaque because the reference's mpn_ctx_struct holds CPU twiddle
+    tables (src/fft_small.h:382-413) that have no meaning here.
+
+    Conventions (same as the reference, src/fft_small.h and
+    doc/source/fft_small.rst):
+      * limbs are 64-bit, little-endian; the caller owns every array;
+      * z must not overlap a or b; z receives an + bn limbs (mpn products)
+        or zh - zl coefficients (polynomial windows);
+      * a == b with an == bn is a squaring;
+      * a context is not reentrant: calls on one context must not overlap
+        (the reference's context shares one scratch buffer the same way,
+        src/fft_small/mpn_mul.c:1342-1362).
+
+    Errors: the void functions report failures through the throw handler
+    (default: print and abort(), like flint_throw in
+    src/generic_files/exception.c); the *_status variants and the
+    device-pointer variants return 0 on success or a GPU_FFT_SMALL_E* code.
+    There is no CPU fallback: without a usable GPU every call fails.
+*/
+#ifndef GPU_FFT_SMALL_H
+#define GPU_FFT_SMALL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define GPU_FFT_SMALL_API __attribute__((visibility("default")))
+#else
+#define GPU_FFT_SMALL_API
+#endif
+
+typedef unsigned long gpu_ulong;   /* FLINT ulong / mp_limb_t on LP64 */
+typedef long gpu_slong;
+
+/* status codes */
+#define GPU_FFT_SMALL_OK          0
+#define GPU_FFT_SMALL_EINVAL      1   /* bad argument (sizes, aliasing, modulus) */
+#define GPU_FFT_SMALL_ETOOBIG     2   /* beyond the supported transform length */
+#define GPU_FFT_SMALL_ECUDA       3   /* CUDA runtime error (no GPU, OOM, ...) */
+#define GPU_FFT_SMALL_ETIMEOUT    4   /* a bounded device wait gave up */
+#define GPU_FFT_SMALL_ENOPRIMES   5   /* coefficient bound exceeds the primes */
+
+/* Opaque context, used exactly like mpn_ctx_t: declare, init, use, clear. */
+typedef struct {
+    void *impl;
+} gpu_mpn_ctx_struct;
+typedef gpu_mpn_ctx_struct gpu_mpn_ctx_t[1];
+
+/* nmod_t of the reference (src/flint.h.in:440-447): n, its preinverse, and
+   the normalisation shift; only n is read. */
+typedef struct {
+    gpu_ulong n;
+    gpu_ulong ninv;
+    gpu_ulong norm;
+} gpu_nmod_t;
+
+/* --- context (replaces mpn_ctx_init / mpn_ctx_clear, src/fft_small.h:422-423) */
+
+/* p plays the role of the reference's starting prime (DEFAULT_PRIME,
+   src/fft_small/default_ctx.c:17); the GPU path uses its own fixed set of
+   31-bit primes and records p only for identification.  Binds the context to
+   the current CUDA device. */
+GPU_FFT_SMALL_API void gpu_mpn_ctx_init(gpu_mpn_ctx_t R, gpu_ulong p);
+GPU_FFT_SMALL_API int gpu_mpn_ctx_init_status(gpu_mpn_ctx_t R, gpu_ulong p);
+GPU_FFT_SMALL_API void gpu_mpn_ctx_clear(gpu_mpn_ctx_t R);
+
+/* --- integer products ---------------------------------------------------- */
+
+/* z[0, an+bn) = a * b.  Replaces mpn_ctx_mpn_mul (src/fft_small.h:433,
+   src/fft_small/mpn_mul.c:1980-1983).  Requires an, bn >= 1. */
+GPU_FFT_SMALL_API void gpu_mpn_ctx_mpn_mul(gpu_mpn_ctx_t R, gpu_ulong *z,
+                         const gpu_ulong *a, gpu_ulong an,
+                         const gpu_ulong *b, gpu_ulong bn);
+GPU_FFT_SMALL_API int gpu_mpn_ctx_mpn_mul_status(gpu_mpn_ctx_t R, gpu_ulong *z,
+                               const gpu_ulong *a, gpu_ulong an,
+                               const gpu_ulong *b, gpu_ulong bn);
+
+/* Limbs [lo, hi) of a * b into z[0, hi-lo).  Replaces _mpn_ctx_mpn_mul_range
+   (src/fft_small.h:462, src/fft_small/mpn_mul.c:1617-1978).  The reference
+   returns, for lo > 0, a lower approximation with a bounded deficit; this
+   implementation returns the exact limbs, which satisfies that contract. */
+GPU_FFT_SMALL_API void _gpu_mpn_ctx_mpn_mul_range(gpu_mpn_ctx_t R, gpu_ulong *z,
+                                gpu_ulong lo, gpu_ulong hi,
+                                const gpu_ulong *a, gpu_ulong an,
+                                const gpu_ulong *b, gpu_ulong bn);
+
+/* Device-pointer twin of gpu_mpn_ctx_mpn_mul: a, b, z are device addresses,
+   the work is queued on `stream` (a cudaStream_t, NULL = the context's own
+   stream) and the call returns without synchronising when it succeeds. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev,
+                       const uint64_t *a_dev, gpu_ulong an,
+                       const uint64_t *b_dev, gpu_ulong bn, void *stream);
+
+/* --- nmod polynomials ---------------------------------------------------- */
+
+/* z[0, zh-zl) = coefficients [zl, zh) of a * b mod n, inputs reduced mod n.
+   Replaces _nmod_poly_mul_mid_mpn_ctx (src/fft_small.h:769-774,
+   src/fft_small/nmod_poly_mul.c:904-972). */
+GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_mpn_ctx(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
+                                    const gpu_ulong *a, gpu_ulong an,
+                                    const gpu_ulong *b, gpu_ulong bn,
+                                    gpu_nmod_t mod, gpu_mpn_ctx_t R);
+GPU_FFT_SMALL_API int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
+                                  const gpu_ulong *a, gpu_ulong an,
+                                  const gpu_ulong *b, gpu_ulong bn,
+                                  gpu_nmod_t mod, gpu_mpn_ctx_t R);
+
+/* --- default context (replaces src/fft_small/default_ctx.c:29-51) ---------- */
+
+/* One context per host thread, created on first use with the reference's
+   default starting prime. */
+GPU_FFT_SMALL_API gpu_mpn_ctx_struct *gpu_get_default_mpn_ctx(void);
+
+/* Same signature and argument meaning as mpn_mul_default_mpn_ctx
+   (src/fft_small.h:852): r1 = i1 * i2, n1 >= n2 >= 1. */
+GPU_FFT_SMALL_API void gpu_mpn_mul_default_mpn_ctx(gpu_ulong *r1, const gpu_ulong *i1, gpu_slong n1,
+                                 const gpu_ulong *i2, gpu_slong n2);
+
+/* Same signature as _nmod_poly_mul_mid_default_mpn_ctx (src/fft_small.h:853). */
+GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gpu_slong zl, gpu_slong zh,
+                                            const gpu_ulong *a, gpu_slong an,
+                                            const gpu_ulong *b, gpu_slong bn,
+                                            gpu_nmod_t mod);
+
+/* --- error handling ------------------------------------------------------ */
+
+/* Handler called by the void entry points on failure (the analogue of
+   flint_set_throw); NULL restores the default print-and-abort. */
+GPU_FFT_SMALL_API void gpu_fft_small_set_throw(void (*handler)(int code, const char *msg));
+/* Message of the most recent failure on this host thread. */
+GPU_FFT_SMALL_API const char *gpu_fft_small_last_error(void);
+
+/* --- introspection (for tests and benchmarks) ----------------------------- */
+
+/* Number of primes the GPU path would use and the transform length 2^logM
+   for an an x bn product; returns 0 on success. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_plan(gpu_ulong an, gpu_ulong bn, int *np, int *logM);
+/* The i-th prime of the GPU prime set (0 if out of range). */
+GPU_FFT_SMALL_API gpu_ulong gpu_fft_small_prime(int i);
+/* Kernel launches issued by the most recent call on this context. */
+GPU_FFT_SMALL_API int gpu_mpn_ctx_last_launches(gpu_mpn_ctx_t R);
+/* Per-kernel device timing with CUDA events on the launching stream, off by
+   default.  set_timing resets the totals; kernel_times returns the number of
+   kernel slots filled (split+column pass, row pass, inverse column pass,
+   CRT+carry) with total milliseconds and launch counts for each. */
+GPU_FFT_SMALL_API int gpu_mpn_ctx_set_timing(gpu_mpn_ctx_t R, int on);
+GPU_FFT_SMALL_API int gpu_mpn_ctx_kernel_times(gpu_mpn_ctx_t R, double *ms, long *count,
+                                               int max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,102 @@
+"""Pin the oracle before trusting it (CPU only).
+
+The plain-C restatement (oracle/fft_small_oracle.c) is checked against the
+golden fixtures produced by the reference itself, against GMP's mpn_mul,
+against Python integers, and -- where the compiled reference is present --
+against the reference directly on fresh seeded inputs.  These mirror the
+reference's own randomized property tests (src/fft_small/test/t-mul.c:17-101
+vs GMP, t-nmod_poly_mul.c:18-268 vs a classical product).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from tests.golden.make_golden import mpn_inputs, nmod_inputs
+
+
+def _check_record(rec, z):
+    if "full" in rec:
+        assert ["%016x" % int(v) for v in z] == rec["full"]
+    else:
+        assert len(z) == rec["len"]
+        assert O.digest(z) == rec["digest"]
+
+
+@pytest.mark.parametrize("i", range(12))
+def test_port_matches_golden_mpn(golden, i):
+    case = golden["mpn"][i]
+    if case.get("large") or case["an"] + case["bn"] > 40000:
+        pytest.skip("large case is covered on the GPU")
+    a, b = mpn_inputs(case)
+    _check_record(case, O.port_mpn_mul(a, b))
+
+
+@pytest.mark.parametrize("i", range(5))
+def test_port_matches_golden_nmod(golden, i):
+    case = golden["nmod"][i]
+    n, a, b = nmod_inputs(case)
+    _check_record(case, O.port_nmod_mul_mid(case["zl"], case["zh"], a, b, n))
+
+
+def test_golden_fixture_covers_configs(golden):
+    names = [c["name"] for c in golden["mpn"]] + [c["name"] for c in golden["nmod"]]
+    for want in ("config1_2^16x2^16", "config2_2^24x2^24", "config2b_2^24x2^20",
+                 "config3_2^20_mulmid"):
+        assert want in names
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_port_vs_gmp_and_python(seed):
+    rng = np.random.default_rng(seed)
+    an = int(rng.integers(1, 3000))
+    bn = int(rng.integers(1, 3000))
+    a = O.rand_limbs(1000 + seed, an)
+    b = O.rand_limbs(2000 + seed, bn)
+    z = O.port_mpn_mul(a, b)
+    assert (z == O.gmp_mpn_mul(a, b)).all()
+    assert O.to_int(z) == O.to_int(a) * O.to_int(b)
+
+
+def test_port_edge_cases():
+    ones = np.full(77, (1 << 64) - 1, dtype=np.uint64)
+    z = O.port_mpn_mul(ones, ones[:13])
+    assert O.to_int(z) == O.to_int(ones) * O.to_int(ones[:13])
+    zero = np.zeros(5, dtype=np.uint64)
+    assert (O.port_mpn_mul(zero, ones[:3]) == 0).all()
+    a = O.rand_limbs(5, 400)
+    assert (O.port_mpn_mul(a, a) == O.gmp_mpn_mul(a, a)).all()
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_port_nmod_vs_python(seed):
+    rng = np.random.default_rng(100 + seed)
+    an, bn = int(rng.integers(1, 120)), int(rng.integers(1, 120))
+    bits = int(rng.integers(2, 65))
+    n = (int(O.rand_limbs(seed, 1, False)[0]) >> (64 - bits)) | (1 << (bits - 1))
+    n = max(n, 2)
+    a, b = O.rand_below(seed, an, n), O.rand_below(seed + 50, bn, n)
+    zl = int(rng.integers(0, an + bn))
+    zh = zl + int(rng.integers(1, an + bn + 5))
+    z = O.port_nmod_mul_mid(zl, zh, a, b, n)
+    zn = an + bn - 1
+    ref = O.nmod_mul_mid_python(zl, min(zh, zn), a, b, n) if zl < zn else np.zeros(0, np.uint64)
+    assert (z[:len(ref)] == ref).all()
+    assert (z[len(ref):] == 0).all()
+
+
+def test_port_context_matches_reference_primes():
+    """The restated prime walk reproduces the primes listed in the reference
+    (src/fft_small/mpn_mul.c:65-72)."""
+    want = [1108307720798209, 659706976665601, 1086317488242689, 910395627798529,
+            699289395265537, 1022545813831681, 1013749720809473, 868614185943041]
+    assert [O.port().oracle_prime(i) for i in range(8)] == want
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference not built")
+@pytest.mark.parametrize("seed", range(4))
+def test_port_vs_compiled_reference(seed):
+    rng = np.random.default_rng(7 + seed)
+    an = int(rng.integers(1, 60000))
+    bn = int(rng.integers(1, 60000))
+    a, b = O.rand_limbs(300 + seed, an), O.rand_limbs(400 + seed, bn)
+    assert (O.port_mpn_mul(a, b) == O.ref_mpn_mul(a, b)).all()
