@@ -152,7 +152,7 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     void *d_tables = nullptr;
     DevTables T{};
-    uint32_t *d_scale = nullptr;          // [MAX_NP]
+    uint32_t *d_scale = nullptr;          // [np][logM][MAX_NP] pointwise scales
     int *d_err = nullptr;
     unsigned long long *d_ticket = nullptr;
     unsigned long long ticket_base = 0;
@@ -193,6 +193,7 @@ static int ctx_build_tables(Ctx *X)
     const size_t n_tl = (size_t)MAX_NP * TL_SZ;
     std::vector<PrimeInfo> pi(MAX_NP);
     std::vector<uint2> twf(n_twf), twi(n_twf), th(n_th), tl(n_tl), thi(n_th), tli(n_tl);
+    std::vector<W32Table> w32tab(MAX_NP);
     for (int j = 0; j < MAX_NP; j++) {
         const uint32_t p = PRIMES[j];
         PrimeInfo &P = pi[j];
@@ -220,6 +221,19 @@ static int ctx_build_tables(Ctx *X)
                 twi[(size_t)j * TW_SZ + h + jj] = shoup_pair(xi, p);
                 x = h_mulmod(x, r, p);
                 xi = h_mulmod(xi, ri, p);
+            }
+        }
+        // uniform twiddles of the radix-32 pass: w_32^k, w_32^-k
+        {
+            const uint32_t w32 = h_powmod(w, 1u << (LOG_MAXM - 5), p);
+            const uint32_t w32i = h_invmod(w32, p);
+            W32Table &C = w32tab[j];
+            uint32_t x = 1, xi = 1;
+            for (int k = 0; k < 16; k++) {
+                C.f[k] = shoup_pair(x, p);
+                C.i[k] = shoup_pair(xi, p);
+                x = h_mulmod(x, w32, p);
+                xi = h_mulmod(xi, w32i, p);
             }
         }
         // twist tables
@@ -279,16 +293,82 @@ static int ctx_build_tables(Ctx *X)
     X->T.tl = (const uint2 *)(base + o_tl);
     X->T.thi = (const uint2 *)(base + o_thi);
     X->T.tli = (const uint2 *)(base + o_tli);
+    // constant memory belongs to the current device's module instance
+    CU(cudaMemcpyToSymbol(c_w32, w32tab.data(), sizeof(W32Table) * MAX_NP));
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// kernel dispatch by transform shape (column length 2^logR, row length 2^logC)
+typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t,
+                            uint32_t *, uint32_t *, int, int);
+typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int);
+typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, const uint32_t *, int);
+
+template <int LOGR>
+constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
+
+#define FB_COLS(X) X<0, tmpl_cols<0>()>, X<1, tmpl_cols<1>()>, X<2, tmpl_cols<2>()>,      \
+                   X<3, tmpl_cols<3>()>, X<4, tmpl_cols<4>()>, X<5, tmpl_cols<5>()>,      \
+                   X<6, tmpl_cols<6>()>, X<7, tmpl_cols<7>()>, X<8, tmpl_cols<8>()>,      \
+                   X<9, tmpl_cols<9>()>, X<10, tmpl_cols<10>()>, X<11, tmpl_cols<11>()>
+static const fwd_cols_fn FWD_COLS[12] = {FB_COLS(k_fwd_cols)};
+static const inv_cols_fn INV_COLS[12] = {FB_COLS(k_inv_cols)};
+static const rows_fn ROWS[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
+                                 k_rows<5>, k_rows<6>, k_rows<7>, k_rows<8>, k_rows<9>,
+                                 k_rows<10>, k_rows<11>, k_rows<12>, k_rows<13>, k_rows<14>};
+#undef FB_COLS
+
+constexpr int MIN_LOGM = 5;
+
+struct LaunchShape {
+    MulShape S;
+    int col_threads, col_grid;   // column kernels
+    size_t col_smem;
+    int nv, row_threads, row_grid;
+    size_t row_smem;
+};
+
+static LaunchShape make_shape(int logM)
+{
+    LaunchShape L;
+    L.S.logC = std::min(logM, LOG_MAXC);
+    L.S.logR = logM - L.S.logC;
+    const int R = 1 << L.S.logR, C = 1 << L.S.logC;
+    if (L.S.logR >= 5) {
+        L.S.G = cols_per_tile(L.S.logR);
+        L.col_threads = std::min(512, L.S.G * R / 32);
+    } else {
+        L.S.G = std::min(C, (1 << 14) >> L.S.logR);
+        L.col_threads = std::min(512, L.S.G);
+    }
+    L.col_grid = C / L.S.G;
+    L.col_smem = (size_t)(padw(R * L.S.G) + 32) * sizeof(uint32_t);
+    L.nv = std::min(R, std::max(1, 1 << (LOG_MAXC - L.S.logC)));
+    L.row_threads = L.nv * C / 32;
+    L.row_grid = (R + L.nv - 1) / L.nv;
+    L.row_smem = (size_t)L.nv * padw(C) * sizeof(uint32_t);
+    return L;
+}
+
+// the three transform launches shared by every product type
+static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
+                              uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
+                              uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
+                              TimingRecord *tr);
+
+static int upload_scales(Ctx *X);
 
 static int configure_kernels()
 {
     static bool done = false;
     if (done) return 0;
-    CU(cudaFuncSetAttribute(k_fwd_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    CU(cudaFuncSetAttribute(k_inv_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
-    CU(cudaFuncSetAttribute(k_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+    for (int r = 0; r < 12; r++) {
+        CU(cudaFuncSetAttribute(FWD_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    }
+    for (int c = 5; c <= LOG_MAXC; c++)
+        CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     done = true;
     return 0;
 }
@@ -309,7 +389,7 @@ static int ctx_create(Ctx **out, gpu_ulong p)
     if (!rc) rc = configure_kernels();
     if (!rc) rc = ctx_build_tables(X);
     if (!rc) {
-        cudaError_t e1 = cudaMalloc(&X->d_scale, sizeof(uint32_t) * MAX_NP);
+        cudaError_t e1 = cudaMalloc(&X->d_scale, sizeof(uint32_t) * (MAX_NP + 1) * (LOG_MAXM + 1) * MAX_NP);
         cudaError_t e2 = cudaMalloc(&X->d_err, sizeof(int));
         cudaError_t e3 = cudaMalloc(&X->d_ticket, sizeof(unsigned long long));
         if (e1 || e2 || e3) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaMalloc of context state failed");
@@ -318,6 +398,7 @@ static int ctx_create(Ctx **out, gpu_ulong p)
             cudaMemset(X->d_ticket, 0, sizeof(unsigned long long));
         }
     }
+    if (!rc) rc = upload_scales(X);
     if (rc) {
         delete X;
         return rc;
@@ -393,7 +474,7 @@ static void ctx_destroy(Ctx *X)
 struct MulPlan {
     int np;
     int logM;
-    MulShape S;
+    LaunchShape L;
 };
 
 static int ceil_log2_u64(uint64_t x)
@@ -416,16 +497,13 @@ static int plan_mpn(uint64_t an, uint64_t bn, MulPlan *P)
     if (np == 0) return set_error(GPU_FFT_SMALL_ENOPRIMES, "operand length %llu beyond the prime set",
                                   (unsigned long long)mn);
     np = std::max(np, 5);
-    int logM = std::max(ceil_log2_u64(L), 4);
+    int logM = std::max(ceil_log2_u64(L), MIN_LOGM);
     if (logM > LOG_MAXM)
         return set_error(GPU_FFT_SMALL_ETOOBIG, "product of %llu coefficients exceeds 2^%d",
                          (unsigned long long)L, LOG_MAXM);
     P->np = np;
     P->logM = logM;
-    P->S.logC = std::min(logM, 13);
-    P->S.logR = logM - P->S.logC;
-    const int R = 1 << P->S.logR, C = 1 << P->S.logC;
-    P->S.G = std::min(C, std::max(8, (1 << 14) / R));
+    P->L = make_shape(logM);
     return 0;
 }
 
@@ -453,6 +531,38 @@ static int ensure_status(Ctx *X, size_t tiles)
     return 0;
 }
 
+static const uint32_t *scale_ptr(const Ctx *X, int np, int logM)
+{
+    return X->d_scale + ((size_t)np * (LOG_MAXM + 1) + logM) * MAX_NP;
+}
+
+// pointwise scales for every (np, logM), uploaded once per context
+static int upload_scales(Ctx *X)
+{
+    std::vector<uint32_t> tab((size_t)(MAX_NP + 1) * (LOG_MAXM + 1) * MAX_NP, 0);
+    for (int np = 1; np <= MAX_NP; np++)
+        for (int lm = 0; lm <= LOG_MAXM; lm++)
+            fill_scale(X, np, lm, &tab[((size_t)np * (LOG_MAXM + 1) + lm) * MAX_NP], 4);
+    CU(cudaMemcpy(X->d_scale, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    return 0;
+}
+
+static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
+                              uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
+                              uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
+                              TimingRecord *tr)
+{
+    const MulShape &S = L.S;
+    FWD_COLS[S.logR]<<<dim3(L.col_grid, np, sq ? 1 : 2), L.col_threads, L.col_smem, st>>>(
+        X->T, a, an, b, bn, ra, rb, S.logC, S.G);
+    timing_mark(tr, 1, st);
+    ROWS[S.logC]<<<dim3(L.row_grid, np), L.row_threads, L.row_smem, st>>>(
+        X->T, ra, rb, S.logR, L.nv, d_scale, sq ? 1 : 0);
+    timing_mark(tr, 2, st);
+    INV_COLS[S.logR]<<<dim3(L.col_grid, np), L.col_threads, L.col_smem, st>>>(X->T, ra, S.logC, S.G);
+    timing_mark(tr, 3, st);
+}
+
 // Enqueue z = a * b on `st` with device pointers.
 static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
                            const uint64_t *b, uint64_t bn, cudaStream_t st)
@@ -467,13 +577,6 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     rc = grow((void **)&X->d_res, &X->res_cap, res_bytes);
     if (rc) return rc;
     uint32_t *ra = X->d_res, *rb = X->d_res + (size_t)np * M;
-    uint32_t scale[MAX_NP];
-    fill_scale(X, np, logM, scale, 4);
-    CU(cudaMemcpyAsync(X->d_scale, scale, sizeof(uint32_t) * np, cudaMemcpyHostToDevice, st));
-
-    const int R = 1 << P.S.logR, C = 1 << P.S.logC, G = P.S.G;
-    const size_t col_smem = (size_t)R * G * sizeof(uint32_t);
-    const size_t row_smem = (size_t)2 * C * sizeof(uint32_t);
     const uint64_t zn = an + bn;
     constexpr int THREADS = 256, TILE = 4 * THREADS;
     const size_t tiles = (zn + TILE - 1) / TILE;
@@ -486,17 +589,9 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     }
     const CrtConst &K = X->crt[np];
 
-    int launches = 0;
+    int launches = 3;
     TimingRecord *tr = timing_begin(X, st);
-    k_fwd_cols<<<dim3(C / G, np, sq ? 1 : 2), 512, col_smem, st>>>(X->T, a, an, b, bn, ra, rb, P.S);
-    launches++;
-    timing_mark(tr, 1, st);
-    k_rows<<<dim3(R, np), 512, row_smem, st>>>(X->T, ra, rb, P.S, X->d_scale, sq ? 1 : 0);
-    launches++;
-    timing_mark(tr, 2, st);
-    k_inv_cols<<<dim3(C / G, np), 512, col_smem, st>>>(X->T, ra, P.S);
-    launches++;
-    timing_mark(tr, 3, st);
+    launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr);
     if (np == 5)
         k_crt_carry<5, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
                                                           X->d_ticket, X->ticket_base, X->epoch, X->d_err);
@@ -624,8 +719,8 @@ int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev, 
     if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
     int rc = bind_device(X);
     if (rc) return rc;
-    return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn,
-                           stream ? (cudaStream_t)stream : X->stream);
+    // NULL is CUDA's default stream, as everywhere in the runtime API
+    return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn, (cudaStream_t)stream);
 }
 
 int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,

@@ -2,16 +2,16 @@
 //
 // Coefficients are single limbs (64-bit chunks); the cyclic convolution of
 // length M = 2^m = R * C is computed modulo np word-size primes with a
-// four-step transform:
+// four-step transform (C = 2^14 once M > 2^14, R = M / C <= 2^11):
 //
 //   k_fwd_cols   limbs -> residues (split fused into the load), length-R
-//                forward transforms down every column, four-step twist
-//                w_M^(i*k1), write.                     [one pass over HBM]
-//   k_rows       per row: forward transforms of a and b, pointwise product
-//                with the CRT/normalisation scale, inverse transform.
-//                                                        [one pass over HBM]
-//   k_inv_cols   untwist, length-R inverse transforms down every column.
-//                                                        [one pass over HBM]
+//                forward transforms down G columns at a time, four-step twist
+//                w_M^(i*k1) applied in registers, write.  [one pass over HBM]
+//   k_rows       per row: forward transform of b (kept in registers), forward
+//                transform of a, pointwise product with the CRT/normalisation
+//                scale, inverse transform.               [one pass over HBM]
+//   k_inv_cols   untwist in registers, length-R inverse transforms down the
+//                columns.                                 [one pass over HBM]
 //   k_crt_carry  np residues -> exact coefficient (CRT), coefficients ->
 //                limbs with the carry chain resolved by a decoupled
 //                look-back scan across tiles.             [one pass over HBM]
@@ -25,11 +25,11 @@
 
 namespace fb {
 
-constexpr int LOG_MAXM = 25;          // largest cyclic length 2^25
-constexpr int TW_SZ = 8192;           // local twiddle table entries per prime
-constexpr int TH_SZ = 4096;           // twist table: w^(t * 2^13), t < 2^12
-constexpr int TL_SZ = 8192;           // twist table: w^t, t < 2^13
-constexpr int MAX_NP = 7;
+constexpr int LOG_MAXM = 25;              // largest cyclic length 2^25
+constexpr int LOG_MAXC = 14;              // longest row transform
+constexpr int TW_SZ = 1 << LOG_MAXC;      // local twiddle table entries per prime
+constexpr int TH_SZ = 1 << (LOG_MAXM - 13);   // twist table: w^(t 2^13), t < 2^12
+constexpr int TL_SZ = 1 << 13;            // twist table: w^t, t < 2^13
 
 struct DevTables {
     const PrimeInfo* pi;   // [MAX_NP]
@@ -61,130 +61,220 @@ struct MulShape {
     int G;                 // columns per column-pass tile
 };
 
+// columns per tile for a column length 2^logR: 64 KB tiles, at least 8
+// columns (32-byte row segments)
+__host__ __device__ constexpr int cols_per_tile(int logR)
+{
+    return logR >= 11 ? 8 : (1 << (14 - logR));
+}
+
 // ---------------------------------------------------------------------------
 // Column pass, forward: split + length-R transforms + twist.
-// grid = (C / G, np, 2 operands); smem = R * G words.
+// grid = (C / G, np, operands); smem = padw(R * G) words.
+template <int LOGR, int G>
 __global__ void __launch_bounds__(512)
 k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
            const uint64_t* __restrict__ b, uint64_t bn,
-           uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, MulShape S)
+           uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols)
 {
     extern __shared__ uint32_t sm[];
-    const int G = S.G;
-    const int logR = S.logR, logC = S.logC;
-    const int R = 1 << logR, C = 1 << logC;
-    const int logM = logR + logC;
+    constexpr int R = 1 << LOGR;
+    const int C = 1 << logC;
+    const int logM = LOGR + logC;
+    const int GR = G ? G : gcols;          // runtime tile width for short columns
     const int j = blockIdx.y;
-    const int i0 = blockIdx.x * G;
+    const int i0 = blockIdx.x * GR;
     const bool opb = blockIdx.z != 0;
     const uint64_t* __restrict__ x = opb ? b : a;
     const uint64_t xn = opb ? bn : an;
     uint32_t* __restrict__ out = (opb ? rb : ra) + ((size_t)j << logM);
     const PrimeInfo P = T.pi[j];
-    const int tot = R * G;
-
+    const uint32_t p = P.p;
     const uint64_t M = (uint64_t)1 << logM;
+    const int tot = R * GR;
+
     for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-        const int u = f / G, c = f - u * G;
+        const int u = f / GR, c = f - u * GR;
         uint64_t n = (uint64_t)u * C + i0 + c;
         uint32_t r = 0;
         // cyclic fold: an operand longer than M wraps around (x mod X^M - 1)
-        for (; n < xn; n += M) r = add_mod(r, limb_redc(x[n], P.p, P.pneg_inv, P.c32), P.p);
-        sm[swz(u * G + c)] = r;
+        for (; n < xn; n += M) r = add_mod(r, limb_redc(x[n], p, P.pneg_inv, P.c32), p);
+        sm[padw(u * GR) + c] = r;
     }
     __syncthreads();
-    if (logR > 0) {
-        VecLayout V{G, logR, 1, G, true};
-        ntt_forward(sm, V, T.twf + (size_t)j * TW_SZ, P.p);
-    }
     const uint2* __restrict__ th = T.th + (size_t)j * TH_SZ;
     const uint2* __restrict__ tl = T.tl + (size_t)j * TL_SZ;
     const int sh = LOG_MAXM - logM;
-    for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-        const int u = f / G, c = f - u * G;
-        const uint32_t k1 = bitrev_bits(u, logR);
-        const uint32_t e = (((uint32_t)(i0 + c) * k1) & ((1u << logM) - 1)) << sh;
-        const uint32_t v = twist_mul(sm[swz(u * G + c)], e, th, tl, P.p);
-        out[(size_t)u * C + i0 + c] = v;
+    const uint32_t mmask = (uint32_t)(M - 1);
+    if constexpr (LOGR >= 5) {
+        gs_strided_all<LOGR, G>(sm, 1, T.twf + (size_t)j * TW_SZ, p);
+        constexpr int NS = R / 32;
+        for (int f = threadIdx.x; f < G * NS; f += blockDim.x) {
+            const int v = f & (G - 1), s = f / G;
+            const int pb = 33 * G * s + v;
+            uint32_t xr[32];
+#pragma unroll
+            for (int m = 0; m < 32; m++) xr[m] = sm[pb + padw(m * G)];
+            gs_contig<5>(xr, c_w32[j], p);
+            const uint32_t col = (uint32_t)(i0 + v);
+#pragma unroll
+            for (int m = 0; m < 32; m++) {
+                const uint32_t u = 32 * s + m;
+                const uint32_t e = ((col * bitrev_bits(u, LOGR)) & mmask) << sh;
+                out[(size_t)u * C + col] = twist_mul(xr[m], e, th, tl, p);
+            }
+        }
+    } else {
+        // short columns: one thread owns a whole column
+        for (int v = threadIdx.x; v < GR; v += blockDim.x) {
+            uint32_t xr[R];
+#pragma unroll
+            for (int m = 0; m < R; m++) xr[m] = sm[padw(m * GR) + v];
+            if constexpr (LOGR > 0) gs_contig<LOGR>(xr, c_w32[j], p);
+            const uint32_t col = (uint32_t)(i0 + v);
+#pragma unroll
+            for (int m = 0; m < R; m++) {
+                uint32_t val = xr[m];
+                if constexpr (LOGR > 0) {
+                    const uint32_t e = ((col * bitrev_bits(m, LOGR)) & mmask) << sh;
+                    val = twist_mul(val, e, th, tl, p);
+                }
+                out[(size_t)m * C + col] = val;
+            }
+        }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Row pass: forward transforms of a and b rows, pointwise product times
-// scale[j], inverse transform; result overwrites the a row.
-// grid = (R, np); smem = 2 * C words.
+// Row pass: nv rows of length C per CTA.  Forward transform of b (result kept
+// in registers), forward transform of a, pointwise product times scale[j],
+// inverse transform; the result overwrites the a rows.
+// grid = (ceil(R / nv), np); block = nv * C / 32; smem = nv * padw(C) words.
+template <int LOGC>
 __global__ void __launch_bounds__(512)
 k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
-       MulShape S, const uint32_t* __restrict__ scale, int squaring)
+       int logR, int nv, const uint32_t* __restrict__ scale, int squaring)
 {
     extern __shared__ uint32_t sm[];
-    const int logC = S.logC;
-    const int C = 1 << logC;
-    const int logM = S.logR + logC;
-    const int u = blockIdx.x;
+    constexpr int C = 1 << LOGC;
+    constexpr int PC = padw(C);
+    constexpr int NSUB = C / 32;
+    const int R = 1 << logR;
+    const int logM = logR + LOGC;
     const int j = blockIdx.y;
+    const int u0 = blockIdx.x * nv;
     const PrimeInfo P = T.pi[j];
-    uint32_t* __restrict__ arow = ra + ((size_t)j << logM) + (size_t)u * C;
-    const uint32_t* __restrict__ brow = rb + ((size_t)j << logM) + (size_t)u * C;
-    const int nv = squaring ? 1 : 2;
+    const uint32_t p = P.p;
+    const uint2* __restrict__ twf = T.twf + (size_t)j * TW_SZ;
+    const uint2* __restrict__ twi = T.twi + (size_t)j * TW_SZ;
+    uint32_t* __restrict__ abase = ra + ((size_t)j << logM);
+    const uint32_t* __restrict__ bbase = rb + ((size_t)j << logM);
 
-    for (int i = threadIdx.x; i < C; i += blockDim.x) {
-        sm[swz(i)] = arow[i];
-        if (!squaring) sm[swz(C + i)] = brow[i];
+    const int t = threadIdx.x;
+    const int tv = t / NSUB, ts = t & (NSUB - 1);
+    const int pb = tv * PC + 33 * ts;
+
+    uint32_t breg[32];
+    if (!squaring) {
+        for (int f = t; f < nv * C; f += blockDim.x) {
+            const int v = f >> LOGC, i = f & (C - 1);
+            const int u = u0 + v;
+            sm[v * PC + padw(i)] = u < R ? bbase[(size_t)u * C + i] : 0u;
+        }
+        __syncthreads();
+        gs_strided_all<LOGC, 0>(sm, nv, twf, p);
+#pragma unroll
+        for (int m = 0; m < 32; m++) breg[m] = sm[pb + m];
+        gs_contig<5>(breg, c_w32[j], p);
+        __syncthreads();
+    }
+    for (int f = t; f < nv * C; f += blockDim.x) {
+        const int v = f >> LOGC, i = f & (C - 1);
+        const int u = u0 + v;
+        sm[v * PC + padw(i)] = u < R ? abase[(size_t)u * C + i] : 0u;
     }
     __syncthreads();
-    {
-        VecLayout V{nv, logC, C, 1, false};
-        ntt_forward(sm, V, T.twf + (size_t)j * TW_SZ, P.p);
-    }
+    gs_strided_all<LOGC, 0>(sm, nv, twf, p);
+    uint32_t xr[32];
+#pragma unroll
+    for (int m = 0; m < 32; m++) xr[m] = sm[pb + m];
+    gs_contig<5>(xr, c_w32[j], p);
     const uint32_t sc = scale[j];
-    for (int i = threadIdx.x; i < C; i += blockDim.x) {
-        const uint32_t x = sm[swz(i)];
-        const uint32_t y = squaring ? x : sm[swz(C + i)];
-        sm[swz(i)] = mul_mont(mul_mont(x, y, P.p, P.pneg_inv), sc, P.p, P.pneg_inv);
+#pragma unroll
+    for (int m = 0; m < 32; m++) {
+        const uint32_t y = squaring ? xr[m] : breg[m];
+        xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
     }
+    ct_contig<5>(xr, c_w32[j], p);
+#pragma unroll
+    for (int m = 0; m < 32; m++) sm[pb + m] = xr[m];
     __syncthreads();
-    {
-        VecLayout V{1, logC, C, 1, false};
-        ntt_inverse(sm, V, T.twi + (size_t)j * TW_SZ, P.p);
+    ct_strided_all<LOGC, 0>(sm, nv, twi, p);
+    for (int f = t; f < nv * C; f += blockDim.x) {
+        const int v = f >> LOGC, i = f & (C - 1);
+        const int u = u0 + v;
+        if (u < R) abase[(size_t)u * C + i] = sm[v * PC + padw(i)];
     }
-    for (int i = threadIdx.x; i < C; i += blockDim.x) arow[i] = sm[swz(i)];
 }
 
 // ---------------------------------------------------------------------------
-// Column pass, inverse: untwist + length-R inverse transforms, in place.
-// grid = (C / G, np); smem = R * G words.
+// Column pass, inverse: untwist in registers + length-R inverse transforms,
+// in place.  grid = (C / G, np); smem = padw(R * G) words.
+template <int LOGR, int G>
 __global__ void __launch_bounds__(512)
-k_inv_cols(DevTables T, uint32_t* __restrict__ ra, MulShape S)
+k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols)
 {
     extern __shared__ uint32_t sm[];
-    const int G = S.G;
-    const int logR = S.logR, logC = S.logC;
-    const int R = 1 << logR, C = 1 << logC;
-    const int logM = logR + logC;
+    constexpr int R = 1 << LOGR;
+    const int C = 1 << logC;
+    const int logM = LOGR + logC;
+    const int GR = G ? G : gcols;
     const int j = blockIdx.y;
-    const int i0 = blockIdx.x * G;
+    const int i0 = blockIdx.x * GR;
     uint32_t* __restrict__ buf = ra + ((size_t)j << logM);
-    const PrimeInfo P = T.pi[j];
+    const uint32_t p = T.pi[j].p;
     const uint2* __restrict__ th = T.thi + (size_t)j * TH_SZ;
     const uint2* __restrict__ tl = T.tli + (size_t)j * TL_SZ;
     const int sh = LOG_MAXM - logM;
-    const int tot = R * G;
+    const uint32_t mmask = (uint32_t)(((uint64_t)1 << logM) - 1);
 
-    for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-        const int u = f / G, c = f - u * G;
-        const uint32_t k1 = bitrev_bits(u, logR);
-        const uint32_t e = (((uint32_t)(i0 + c) * k1) & ((1u << logM) - 1)) << sh;
-        sm[swz(u * G + c)] = twist_mul(buf[(size_t)u * C + i0 + c], e, th, tl, P.p);
-    }
-    __syncthreads();
-    if (logR > 0) {
-        VecLayout V{G, logR, 1, G, true};
-        ntt_inverse(sm, V, T.twi + (size_t)j * TW_SZ, P.p);
-    }
-    for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-        const int u = f / G, c = f - u * G;
-        buf[(size_t)u * C + i0 + c] = sm[swz(u * G + c)];
+    if constexpr (LOGR >= 5) {
+        constexpr int NS = R / 32;
+        for (int f = threadIdx.x; f < G * NS; f += blockDim.x) {
+            const int v = f & (G - 1), s = f / G;
+            const uint32_t col = (uint32_t)(i0 + v);
+            uint32_t xr[32];
+#pragma unroll
+            for (int m = 0; m < 32; m++) {
+                const uint32_t u = 32 * s + m;
+                const uint32_t e = ((col * bitrev_bits(u, LOGR)) & mmask) << sh;
+                xr[m] = twist_mul(buf[(size_t)u * C + col], e, th, tl, p);
+            }
+            ct_contig<5>(xr, c_w32[j], p);
+            const int pb = 33 * G * s + v;
+#pragma unroll
+            for (int m = 0; m < 32; m++) sm[pb + padw(m * G)] = xr[m];
+        }
+        __syncthreads();
+        ct_strided_all<LOGR, G>(sm, 1, T.twi + (size_t)j * TW_SZ, p);
+        const int tot = R * G;
+        for (int f = threadIdx.x; f < tot; f += blockDim.x) {
+            const int u = f / G, c = f - u * G;
+            buf[(size_t)u * C + i0 + c] = sm[padw(u * G) + c];
+        }
+    } else if constexpr (LOGR > 0) {
+        for (int v = threadIdx.x; v < GR; v += blockDim.x) {
+            const uint32_t col = (uint32_t)(i0 + v);
+            uint32_t xr[R];
+#pragma unroll
+            for (int m = 0; m < R; m++) {
+                const uint32_t e = ((col * bitrev_bits(m, LOGR)) & mmask) << sh;
+                xr[m] = twist_mul(buf[(size_t)m * C + col], e, th, tl, p);
+            }
+            ct_contig<LOGR>(xr, c_w32[j], p);
+#pragma unroll
+            for (int m = 0; m < R; m++) buf[(size_t)m * C + col] = xr[m];
+        }
     }
 }
 

@@ -1,157 +1,264 @@
 // Block-cooperative number-theoretic transforms on vectors held in shared
-// memory.
+// memory (and, for the last forward / first inverse levels, in registers).
 //
 // A forward transform of length L = 2^k is a Gentleman-Sande (decimation in
-// frequency) network: natural-order input, bit-reversed output.  Level with
-// half-size h pairs positions (j, j + h) inside blocks of 2h and computes
-//     (a, b) -> (a + b, (a - b) * w2h^jj),   jj = j mod h, w2h a 2h-th root.
+// frequency) network: natural-order input, bit-reversed output.  The level
+// with half-size h pairs positions (j, j + h) inside blocks of 2h:
+//     (a, b) -> (a + b, (a - b) * w_2h^(j mod h)).
 // The inverse is the transposed Cooley-Tukey (decimation in time) network
 // with inverse twiddles: bit-reversed input, natural output, scaled by L.
 //
-// Both are executed as passes of Q levels: each thread loads E = 2^Q
-// elements that are closed under those levels into registers, runs the
-// butterflies there and writes them back, so shared memory is touched once
-// per Q levels instead of once per level.
+// Execution is split into passes; each thread loads the 2^Q elements of one
+// radix-2^Q sub-transform, runs Q levels in registers and writes back:
+//   * strided passes (levels with half-size >= 32): element stride S >= 32,
+//     consecutive threads take consecutive sub-transforms, per-thread
+//     twiddles w_2h^(jj0 + k S) are read from a table, each distinct one once;
+//   * the contiguous pass (the five levels h = 16..1): each thread owns 32
+//     consecutive positions; its twiddles are powers of w_32, the same for
+//     every thread, and come from constant memory.
+// Shared memory holds one pad word per 32 (physical = a + a/32), which makes
+// both kinds of pass conflict-free and lets every address be a per-thread
+// base plus a compile-time offset.
 //
-// Twiddles come from per-prime tables tw[h + jj] = (w2h^jj, Shoup companion)
-// for h a power of two; one table serves every transform length because the
-// entry for a given (h, jj) does not depend on L.
+// Table layout: tw[h + jj] = (w_2h^jj, Shoup companion) for h a power of two;
+// the entry for (h, jj) does not depend on L, so one table serves all lengths.
 //
 // The reference computes the same transforms with radix-4 double-precision
 // butterflies over 256-point blocks (src/fft_small/sd_fft.c:1230-1274,
-// src/fft_small/sd_ifft.c:1503-1533); the output order here differs, which
-// is harmless because only pointwise products are formed in transform space.
+// src/fft_small/sd_ifft.c:1503-1533); the output order differs, which is
+// harmless because only pointwise products are formed in transform space.
 #pragma once
 #include "modarith.cuh"
 
 namespace fb {
 
-// Bank-conflict-avoiding permutation of shared-memory word addresses: the low
-// five bits (the bank) are XORed with a fold of the higher bits, so that
-// power-of-two strides up to 2^15 words spread over all banks.  It is a
-// bijection that keeps every address inside its aligned 32-word row.
-__device__ __forceinline__ int swz(int a)
-{
-    return a ^ (((a >> 5) ^ (a >> 10)) & 31);
-}
+constexpr int MAX_NP = 7;
 
-struct VecLayout {
-    int nvec;      // number of independent vectors
-    int logL;      // log2 of the vector length
-    int vstride;   // word distance between vectors
-    int estride;   // word distance between consecutive elements of a vector
-    bool vec_fast; // consecutive threads take consecutive vectors
+__host__ __device__ constexpr int padw(int a) { return a + (a >> 5); }
+
+// w_32^k and w_32^-k (k < 16) with Shoup companions, per prime
+struct W32Table {
+    uint2 f[16];
+    uint2 i[16];
 };
+__constant__ W32Table c_w32[MAX_NP];
 
-__device__ __forceinline__ int vl_addr(const VecLayout& V, int v, int j)
-{
-    return swz(v * V.vstride + j * V.estride);
-}
+// ---------------------------------------------------------------------------
+// butterflies on registers
 
-// One Gentleman-Sande pass: levels with half-sizes h, h/2, ..., h/2^(Q-1).
+// Q Gentleman-Sande levels on 2^Q consecutive positions (half-sizes 2^(Q-1)..1)
 template <int Q>
-__device__ __forceinline__ void gs_pass(uint32_t* sm, const VecLayout& V, int h,
-                                        const uint2* __restrict__ tw, uint32_t p)
+__device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table& W, uint32_t p)
 {
     constexpr int E = 1 << Q;
-    const int logS = __ffs(h) - 1 - (Q - 1);   // S = h >> (Q-1)
-    const int S = 1 << logS;
-    const int lognsub = V.logL - Q;
-    const int total = V.nvec << lognsub;
-    for (int f = threadIdx.x; f < total; f += blockDim.x) {
-        int v, s;
-        if (V.vec_fast) { v = f % V.nvec; s = f / V.nvec; }
-        else            { s = f & ((1 << lognsub) - 1); v = f >> lognsub; }
-        const int jj0 = s & (S - 1);
-        const int base = ((s >> logS) << (logS + Q)) + jj0;   // blk * 2h + jj0
-        uint32_t x[E];
 #pragma unroll
-        for (int m = 0; m < E; m++) x[m] = sm[vl_addr(V, v, base + m * S)];
+    for (int t = 0; t < Q; t++) {
+        const int hm = E >> (t + 1);
 #pragma unroll
-        for (int t = 0; t < Q; t++) {
-            const int hm = E >> (t + 1);
-            const int ht = h >> t;
-#pragma unroll
-            for (int m = 0; m < E; m++) {
-                if ((m & hm) == 0) {
-                    const int jj = jj0 + (m & (hm - 1)) * S;
-                    const uint2 w = tw[ht + jj];
-                    const uint32_t a = x[m], b = x[m + hm];
-                    x[m] = add_mod(a, b, p);
+        for (int m = 0; m < E; m++) {
+            if ((m & hm) == 0) {
+                const int k = m & (hm - 1);
+                const uint32_t a = x[m], b = x[m + hm];
+                x[m] = add_mod(a, b, p);
+                if (k == 0) {
+                    x[m + hm] = sub_mod(a, b, p);
+                } else {
+                    const uint2 w = W.f[k * (16 / hm)];
                     x[m + hm] = mul_shoup(a - b + p, w.x, w.y, p);
                 }
             }
         }
-#pragma unroll
-        for (int m = 0; m < E; m++) sm[vl_addr(V, v, base + m * S)] = x[m];
     }
 }
 
-// One Cooley-Tukey pass: levels with half-sizes h, 2h, ..., 2^(Q-1) h.
+// Q Cooley-Tukey levels on 2^Q consecutive positions (half-sizes 1..2^(Q-1))
 template <int Q>
-__device__ __forceinline__ void ct_pass(uint32_t* sm, const VecLayout& V, int h,
-                                        const uint2* __restrict__ twi, uint32_t p)
+__device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table& W, uint32_t p)
 {
     constexpr int E = 1 << Q;
-    const int logh = __ffs(h) - 1;
-    const int lognsub = V.logL - Q;
-    const int total = V.nvec << lognsub;
-    for (int f = threadIdx.x; f < total; f += blockDim.x) {
-        int v, s;
-        if (V.vec_fast) { v = f % V.nvec; s = f / V.nvec; }
-        else            { s = f & ((1 << lognsub) - 1); v = f >> lognsub; }
-        const int jj0 = s & (h - 1);
-        const int base = ((s >> logh) << (logh + Q)) + jj0;
-        uint32_t x[E];
 #pragma unroll
-        for (int m = 0; m < E; m++) x[m] = sm[vl_addr(V, v, base + m * h)];
+    for (int t = 0; t < Q; t++) {
+        const int hm = 1 << t;
 #pragma unroll
-        for (int t = 0; t < Q; t++) {
-            const int hm = 1 << t;
-            const int ht = h << t;
-#pragma unroll
-            for (int m = 0; m < E; m++) {
-                if ((m & hm) == 0) {
-                    const int jj = jj0 + (m & (hm - 1)) * h;
-                    const uint2 w = twi[ht + jj];
-                    const uint32_t a = x[m];
-                    const uint32_t b = mul_shoup(x[m + hm], w.x, w.y, p);
-                    x[m] = add_mod(a, b, p);
-                    x[m + hm] = sub_mod(a, b, p);
+        for (int m = 0; m < E; m++) {
+            if ((m & hm) == 0) {
+                const int k = m & (hm - 1);
+                uint32_t b = x[m + hm];
+                if (k != 0) {
+                    const uint2 w = W.i[k * (16 / hm)];
+                    b = mul_shoup(b, w.x, w.y, p);
                 }
+                const uint32_t a = x[m];
+                x[m] = add_mod(a, b, p);
+                x[m + hm] = sub_mod(a, b, p);
             }
         }
+    }
+}
+
+// Q Gentleman-Sande levels, half-sizes H..H/2^(Q-1), element stride S = H/2^(Q-1)
+template <int Q, int H>
+__device__ __forceinline__ void gs_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
+                                           int jj0, uint32_t p)
+{
+    constexpr int E = 1 << Q;
+    constexpr int S = H >> (Q - 1);
 #pragma unroll
-        for (int m = 0; m < E; m++) sm[vl_addr(V, v, base + m * h)] = x[m];
+    for (int t = 0; t < Q; t++) {
+        constexpr int dummy = 0;
+        (void)dummy;
+        const int hm = E >> (t + 1);
+        const int ht = H >> t;
+        uint2 w[E / 2];
+#pragma unroll
+        for (int k = 0; k < hm; k++) w[k] = tw[ht + jj0 + k * S];
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            if ((m & hm) == 0) {
+                const uint2 ww = w[m & (hm - 1)];
+                const uint32_t a = x[m], b = x[m + hm];
+                x[m] = add_mod(a, b, p);
+                x[m + hm] = mul_shoup(a - b + p, ww.x, ww.y, p);
+            }
+        }
     }
 }
 
-// Full forward transform of every vector (caller synchronises before).
-__device__ __forceinline__ void ntt_forward(uint32_t* sm, const VecLayout& V,
-                                            const uint2* __restrict__ tw, uint32_t p)
+// Q Cooley-Tukey levels, half-sizes H..2^(Q-1) H, element stride S = H
+template <int Q, int H>
+__device__ __forceinline__ void ct_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
+                                           int jj0, uint32_t p)
 {
-    int rem = V.logL;
-    int h = (1 << V.logL) >> 1;
-    while (rem > 0) {
-        if (rem >= 4)      { gs_pass<4>(sm, V, h, tw, p); h >>= 4; rem -= 4; }
-        else if (rem == 3) { gs_pass<3>(sm, V, h, tw, p); h >>= 3; rem -= 3; }
-        else if (rem == 2) { gs_pass<2>(sm, V, h, tw, p); h >>= 2; rem -= 2; }
-        else               { gs_pass<1>(sm, V, h, tw, p); h >>= 1; rem -= 1; }
+    constexpr int E = 1 << Q;
+#pragma unroll
+    for (int t = 0; t < Q; t++) {
+        const int hm = 1 << t;
+        const int ht = H << t;
+        uint2 w[E / 2];
+#pragma unroll
+        for (int k = 0; k < hm; k++) w[k] = twi[ht + jj0 + k * H];
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            if ((m & hm) == 0) {
+                const uint2 ww = w[m & (hm - 1)];
+                const uint32_t b = mul_shoup(x[m + hm], ww.x, ww.y, p);
+                const uint32_t a = x[m];
+                x[m] = add_mod(a, b, p);
+                x[m + hm] = sub_mod(a, b, p);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory layouts.
+//   Rows:    NV vectors of length 2^LOGL, vector v at v * padw(L), element j
+//            at padw(j) inside it.
+//   Columns: G interleaved columns of length 2^LOGL, element j of column v at
+//            padw(j * G) + v (valid because G divides 32 and v < G).
+
+template <int LOGL, int G>
+struct ColLayout {
+    static constexpr int L = 1 << LOGL;
+    __device__ static int addr(int v, int j) { return padw(j * G) + v; }
+};
+
+// One strided GS pass over every sub-transform of the tile.
+// Rows layout (G == 0): NV vectors; columns layout: G columns.
+template <int LOGL, int Q, int H, int G>
+__device__ __forceinline__ void gs_pass_smem(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
+{
+    constexpr int L = 1 << LOGL;
+    constexpr int E = 1 << Q;
+    constexpr int S = H >> (Q - 1);
+    constexpr int NSUB = L / E;
+    const int TOT = (G ? G : nv) * NSUB;
+    static_assert(S * (G ? G : 1) % 32 == 0, "strided pass must step by whole bank rows");
+    constexpr int PSTEP = (S * (G ? G : 1)) / 32 * 33;
+    for (int f = threadIdx.x; f < TOT; f += blockDim.x) {
+        int v, s;
+        if (G) { v = f & (G - 1); s = f / (G ? G : 1); }
+        else   { s = f & (NSUB - 1); v = f / NSUB; }
+        const int jj0 = s & (S - 1);
+        const int base = (s / S) * (2 * H) + jj0;
+        const int pb = G ? padw(base * G) + v : v * padw(L) + padw(base);
+        uint32_t x[E];
+#pragma unroll
+        for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
+        gs_strided<Q, H>(x, tw, jj0, p);
+#pragma unroll
+        for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
+    }
+}
+
+template <int LOGL, int Q, int H, int G>
+__device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* __restrict__ twi, uint32_t p)
+{
+    constexpr int L = 1 << LOGL;
+    constexpr int E = 1 << Q;
+    constexpr int S = H;
+    constexpr int NSUB = L / E;
+    const int TOT = (G ? G : nv) * NSUB;
+    static_assert(S * (G ? G : 1) % 32 == 0, "strided pass must step by whole bank rows");
+    constexpr int PSTEP = (S * (G ? G : 1)) / 32 * 33;
+    for (int f = threadIdx.x; f < TOT; f += blockDim.x) {
+        int v, s;
+        if (G) { v = f & (G - 1); s = f / (G ? G : 1); }
+        else   { s = f & (NSUB - 1); v = f / NSUB; }
+        const int jj0 = s & (S - 1);
+        const int base = (s / S) * (S * E) + jj0;
+        const int pb = G ? padw(base * G) + v : v * padw(L) + padw(base);
+        uint32_t x[E];
+#pragma unroll
+        for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
+        ct_strided<Q, H>(x, twi, jj0, p);
+#pragma unroll
+        for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
+    }
+}
+
+// Strided part of the forward transform: all levels with half-size >= 32,
+// i.e. LOGL - 5 levels, in passes of at most four (the first may be shorter).
+template <int LOGL, int G>
+__device__ __forceinline__ void gs_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
+{
+    constexpr int NS = LOGL - 5;
+    if constexpr (NS > 0) {
+        constexpr int Q0 = NS - 4 * ((NS - 1) / 4);
+        constexpr int H0 = 1 << (LOGL - 1);
+        gs_pass_smem<LOGL, Q0, H0, G>(sm, nv, tw, p);
         __syncthreads();
+        if constexpr (NS > Q0) {
+            constexpr int H1 = H0 >> Q0;
+            gs_pass_smem<LOGL, 4, H1, G>(sm, nv, tw, p);
+            __syncthreads();
+            if constexpr (NS > Q0 + 4) {
+                constexpr int H2 = H1 >> 4;
+                gs_pass_smem<LOGL, 4, H2, G>(sm, nv, tw, p);
+                __syncthreads();
+            }
+        }
     }
 }
 
-// Full inverse transform (times L) of every vector.
-__device__ __forceinline__ void ntt_inverse(uint32_t* sm, const VecLayout& V,
-                                            const uint2* __restrict__ twi, uint32_t p)
+// Strided part of the inverse transform (half-sizes 32 .. L/2), after the
+// contiguous first pass.
+template <int LOGL, int G>
+__device__ __forceinline__ void ct_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ twi, uint32_t p)
 {
-    int rem = V.logL;
-    int h = 1;
-    while (rem > 0) {
-        if (rem >= 4)      { ct_pass<4>(sm, V, h, twi, p); h <<= 4; rem -= 4; }
-        else if (rem == 3) { ct_pass<3>(sm, V, h, twi, p); h <<= 3; rem -= 3; }
-        else if (rem == 2) { ct_pass<2>(sm, V, h, twi, p); h <<= 2; rem -= 2; }
-        else               { ct_pass<1>(sm, V, h, twi, p); h <<= 1; rem -= 1; }
+    constexpr int NS = LOGL - 5;
+    if constexpr (NS > 0) {
+        constexpr int Q0 = NS - 4 * ((NS - 1) / 4);   // the last pass is the short one
+        if constexpr (NS > Q0) {
+            ct_pass_smem<LOGL, 4, 32, G>(sm, nv, twi, p);
+            __syncthreads();
+            if constexpr (NS > Q0 + 4) {
+                ct_pass_smem<LOGL, 4, 512, G>(sm, nv, twi, p);
+                __syncthreads();
+            }
+        }
+        constexpr int HL = 1 << (LOGL - Q0);
+        ct_pass_smem<LOGL, Q0, HL, G>(sm, nv, twi, p);
         __syncthreads();
     }
 }

@@ -95,7 +95,7 @@ GPU_FFT_SMALL_API void _gpu_mpn_ctx_mpn_mul_range(gpu_mpn_ctx_t R, gpu_ulong *z,
                                 const gpu_ulong *b, gpu_ulong bn);
 
 /* Device-pointer twin of gpu_mpn_ctx_mpn_mul: a, b, z are device addresses,
-   the work is queued on `stream` (a cudaStream_t, NULL = the context's own
+   the work is queued on `stream` (a cudaStream_t; NULL is CUDA's default
    stream) and the call returns without synchronising when it succeeds. */
 GPU_FFT_SMALL_API int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev,
                        const uint64_t *a_dev, gpu_ulong an,
