@@ -52,7 +52,7 @@ def test_plan_matches_design():
     assert FB.mpn_mul_plan(1 << 24, 1 << 24) == (5, 25)
     assert FB.mpn_mul_plan(1 << 24, 1 << 20) == (5, 25)
     assert FB.mpn_mul_plan(1 << 16, 1 << 16) == (5, 17)
-    assert FB.mpn_mul_plan(1, 1) == (5, 4)
+    assert FB.mpn_mul_plan(1, 1) == (5, 5)   # smallest transform: 32 points
     with pytest.raises(FB.GpuFftSmallError) as e:
         FB.mpn_mul_plan(1 << 25, 1 << 25)
     assert e.value.code == FB.ETOOBIG
