@@ -148,6 +148,7 @@ static void timing_mark(TimingRecord *r, int k, cudaStream_t st)
 
 struct Ctx {
     int device = -1;
+    int nsm = 148;                        // multiprocessors of the device
     gpu_ulong p0 = 0;
     cudaStream_t stream = nullptr;
     void *d_tables = nullptr;
@@ -295,6 +296,10 @@ static int ctx_build_tables(Ctx *X)
     X->T.tli = (const uint2 *)(base + o_tli);
     // constant memory belongs to the current device's module instance
     CU(cudaMemcpyToSymbol(c_w32, w32tab.data(), sizeof(W32Table) * MAX_NP));
+    const uint32_t one = 1, minus_one = 0xffffffffu;
+    CU(cudaMemcpyToSymbol(c_one, &one, sizeof one));
+    CU(cudaMemcpyToSymbol(c_minus_one, &minus_one, sizeof minus_one));
+    CU(cudaDeviceGetAttribute(&X->nsm, cudaDevAttrMultiProcessorCount, X->device));
     return 0;
 }
 
@@ -303,7 +308,8 @@ static int ctx_build_tables(Ctx *X)
 typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t,
                             uint32_t *, uint32_t *, int, int);
 typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int);
-typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, const uint32_t *, int);
+typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, const uint32_t *,
+                        int);
 
 template <int LOGR>
 constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
@@ -346,8 +352,8 @@ static LaunchShape make_shape(int logM)
     L.col_smem = (size_t)(padw(R * L.S.G) + 32) * sizeof(uint32_t);
     L.nv = std::min(R, std::max(1, 1 << (LOG_MAXC - L.S.logC)));
     L.row_threads = L.nv * C / 32;
-    L.row_grid = (R + L.nv - 1) / L.nv;
-    L.row_smem = (size_t)L.nv * padw(C) * sizeof(uint32_t);
+    L.row_grid = (R + L.nv - 1) / L.nv;                // items per prime; launch clamps
+    L.row_smem = (size_t)2 * L.nv * padw(C) * sizeof(uint32_t);   // b and a buffers
     return L;
 }
 
@@ -368,7 +374,7 @@ static int configure_kernels()
         CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
     for (int c = 5; c <= LOG_MAXC; c++)
-        CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done = true;
     return 0;
 }
@@ -556,8 +562,9 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     FWD_COLS[S.logR]<<<dim3(L.col_grid, np, sq ? 1 : 2), L.col_threads, L.col_smem, st>>>(
         X->T, a, an, b, bn, ra, rb, S.logC, S.G);
     timing_mark(tr, 1, st);
-    ROWS[S.logC]<<<dim3(L.row_grid, np), L.row_threads, L.row_smem, st>>>(
-        X->T, ra, rb, S.logR, L.nv, d_scale, sq ? 1 : 0);
+    const int items = L.row_grid * np;
+    ROWS[S.logC]<<<std::min(items, X->nsm), L.row_threads, L.row_smem, st>>>(
+        X->T, ra, rb, S.logR, L.nv, np, d_scale, sq ? 1 : 0);
     timing_mark(tr, 2, st);
     INV_COLS[S.logR]<<<dim3(L.col_grid, np), L.col_threads, L.col_smem, st>>>(X->T, ra, S.logC, S.G);
     timing_mark(tr, 3, st);

@@ -101,6 +101,71 @@ FB_HD uint32_t limb_redc(uint64_t x, uint32_t p, uint32_t pneg_inv, uint32_t c32
     return redc64(t, p, pneg_inv);
 }
 
+#ifdef __CUDACC__
+// Pipe balancing.  Integer adds, compares and min/max issue to the ALU pipe;
+// IMAD issues to the FMA pipe.  Both run at half the issue rate, and the
+// butterflies below are ALU-heavy, so some additions are written as
+// x * one + y with `one` an opaque constant-memory 1 that the compiler cannot
+// fold, which keeps them on the FMA pipe.
+__constant__ uint32_t c_one;        // 1
+__constant__ uint32_t c_minus_one;  // 0xffffffff
+
+__device__ __forceinline__ uint32_t fadd(uint32_t x, uint32_t y) { return x * c_one + y; }
+__device__ __forceinline__ uint32_t fsub(uint32_t x, uint32_t y) { return y * c_minus_one + x; }
+
+// Gentleman-Sande butterfly, inputs and outputs in [0, p):
+// (a, b) -> (a + b, (a - b) w)
+__device__ __forceinline__ void bfly_gs(uint32_t& a, uint32_t& b, uint32_t w, uint32_t wq, uint32_t p)
+{
+    const uint32_t s = fadd(a, b);          // FMA pipe
+    const uint32_t s1 = a + b - p;          // ALU
+    const uint32_t d = a - b + p;           // ALU, in [1, 2p)
+    const uint32_t q = __umulhi(d, wq);
+    const uint32_t r = d * w - q * p;       // [0, 2p)
+    const uint32_t r1 = fadd(r, 0u - p);
+    a = min(s, s1);
+    b = min(r, r1);
+}
+
+// Gentleman-Sande butterfly with twiddle 1
+__device__ __forceinline__ void bfly_gs1(uint32_t& a, uint32_t& b, uint32_t p)
+{
+    const uint32_t s = fadd(a, b);
+    const uint32_t s1 = a + b - p;
+    const uint32_t d = a - b + p;
+    const uint32_t d1 = fsub(a, b);
+    a = min(s, s1);
+    b = min(d, d1);
+}
+
+// Cooley-Tukey butterfly, inputs and outputs in [0, p):
+// (x, y) -> (x + y w, x - y w)
+__device__ __forceinline__ void bfly_ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p)
+{
+    const uint32_t q = __umulhi(y, wq);
+    uint32_t t = y * w - q * p;             // [0, 2p)
+    t = min(t, fadd(t, 0u - p));
+    const uint32_t s = fadd(x, t);
+    const uint32_t s1 = x + t - p;
+    const uint32_t d = x - t + p;
+    const uint32_t d1 = fsub(x, t);
+    x = min(s, s1);
+    y = min(d, d1);
+}
+
+// Cooley-Tukey butterfly with twiddle 1
+__device__ __forceinline__ void bfly_ct1(uint32_t& x, uint32_t& y, uint32_t p)
+{
+    const uint32_t t = y;
+    const uint32_t s = fadd(x, t);
+    const uint32_t s1 = x + t - p;
+    const uint32_t d = x - t + p;
+    const uint32_t d1 = fsub(x, t);
+    x = min(s, s1);
+    y = min(d, d1);
+}
+#endif
+
 // host-side helpers ---------------------------------------------------------
 static inline uint32_t h_mulmod(uint32_t a, uint32_t b, uint32_t p)
 {

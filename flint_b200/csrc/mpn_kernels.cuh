@@ -146,14 +146,42 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
 }
 
 // ---------------------------------------------------------------------------
-// Row pass: nv rows of length C per CTA.  Forward transform of b (result kept
-// in registers), forward transform of a, pointwise product times scale[j],
-// inverse transform; the result overwrites the a rows.
-// grid = (ceil(R / nv), np); block = nv * C / 32; smem = nv * padw(C) words.
+// Row pass, persistent: each CTA walks over items of nv rows (one prime per
+// item).  For every item: forward transform of b (result kept in registers),
+// forward transform of a, pointwise product times scale[j], inverse
+// transform; the result overwrites the a rows.  Two shared buffers hold b and
+// a; the next item's rows are fetched with cp.async into a buffer as soon as
+// the current item has finished with it, so global loads overlap the
+// transforms.  grid = min(items, SMs); block = nv * C / 32;
+// smem = 2 * nv * padw(C) words.
+__device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src, bool valid)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    const int n = valid ? 4 : 0;   // a zero source size fills the word with zeros
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(src), "r"(n));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 template <int LOGC>
-__global__ void __launch_bounds__(512)
+__device__ __forceinline__ void rows_prefetch(uint32_t* dst, const uint32_t* __restrict__ base,
+                                              int u0, int nv, int R)
+{
+    constexpr int C = 1 << LOGC;
+    constexpr int PC = padw(C);
+    for (int f = threadIdx.x; f < nv * C; f += blockDim.x) {
+        const int v = f >> LOGC, i = f & (C - 1);
+        const int u = u0 + v;
+        cp_async4(&dst[v * PC + padw(i)], base + (size_t)min(u, R - 1) * C + i, u < R);
+    }
+    cp_async_commit();
+}
+
+template <int LOGC>
+__global__ void __launch_bounds__(512, 1)
 k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
-       int logR, int nv, const uint32_t* __restrict__ scale, int squaring)
+       int logR, int nv, int np, const uint32_t* __restrict__ scale, int squaring)
 {
     extern __shared__ uint32_t sm[];
     constexpr int C = 1 << LOGC;
@@ -161,60 +189,71 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     constexpr int NSUB = C / 32;
     const int R = 1 << logR;
     const int logM = logR + LOGC;
-    const int j = blockIdx.y;
-    const int u0 = blockIdx.x * nv;
-    const PrimeInfo P = T.pi[j];
-    const uint32_t p = P.p;
-    const uint2* __restrict__ twf = T.twf + (size_t)j * TW_SZ;
-    const uint2* __restrict__ twi = T.twi + (size_t)j * TW_SZ;
-    uint32_t* __restrict__ abase = ra + ((size_t)j << logM);
-    const uint32_t* __restrict__ bbase = rb + ((size_t)j << logM);
-
+    const int groups = (R + nv - 1) / nv;
+    const int total = groups * np;
+    uint32_t* sb = sm;
+    uint32_t* sa = sm + nv * PC;
     const int t = threadIdx.x;
-    const int tv = t / NSUB, ts = t & (NSUB - 1);
-    const int pb = tv * PC + 33 * ts;
+    const int pb = (t / NSUB) * PC + 33 * (t & (NSUB - 1));
 
-    uint32_t breg[32];
-    if (!squaring) {
+    int g = blockIdx.x;
+    if (g >= total) return;
+    {
+        const int j = g / groups, u0 = (g - j * groups) * nv;
+        if (!squaring) rows_prefetch<LOGC>(sb, rb + ((size_t)j << logM), u0, nv, R);
+        else cp_async_commit();
+        rows_prefetch<LOGC>(sa, ra + ((size_t)j << logM), u0, nv, R);
+    }
+    for (; g < total; g += gridDim.x) {
+        const int j = g / groups, u0 = (g - j * groups) * nv;
+        const int g2 = g + gridDim.x;
+        const int j2 = g2 / groups, u2 = (g2 - j2 * groups) * nv;
+        const PrimeInfo P = T.pi[j];
+        const uint32_t p = P.p;
+        const uint2* __restrict__ twf = T.twf + (size_t)j * TW_SZ;
+        const uint2* __restrict__ twi = T.twi + (size_t)j * TW_SZ;
+
+        uint32_t breg[32];
+        if (!squaring) {
+            cp_async_wait<1>();
+            __syncthreads();
+            gs_strided_all<LOGC, 0>(sb, nv, twf, p);
+#pragma unroll
+            for (int m = 0; m < 32; m++) breg[m] = sb[pb + m];
+            gs_contig<5>(breg, c_w32[j], p);
+            __syncthreads();
+        }
+        if (!squaring && g2 < total) rows_prefetch<LOGC>(sb, rb + ((size_t)j2 << logM), u2, nv, R);
+        else cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        gs_strided_all<LOGC, 0>(sa, nv, twf, p);
+        uint32_t xr[32];
+#pragma unroll
+        for (int m = 0; m < 32; m++) xr[m] = sa[pb + m];
+        gs_contig<5>(xr, c_w32[j], p);
+        const uint32_t sc = scale[j];
+#pragma unroll
+        for (int m = 0; m < 32; m++) {
+            const uint32_t y = squaring ? xr[m] : breg[m];
+            xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
+        }
+        ct_contig<5>(xr, c_w32[j], p);
+#pragma unroll
+        for (int m = 0; m < 32; m++) sa[pb + m] = xr[m];
+        __syncthreads();
+        ct_strided_all<LOGC, 0>(sa, nv, twi, p);
+        uint32_t* __restrict__ abase = ra + ((size_t)j << logM);
         for (int f = t; f < nv * C; f += blockDim.x) {
             const int v = f >> LOGC, i = f & (C - 1);
             const int u = u0 + v;
-            sm[v * PC + padw(i)] = u < R ? bbase[(size_t)u * C + i] : 0u;
+            if (u < R) abase[(size_t)u * C + i] = sa[v * PC + padw(i)];
         }
         __syncthreads();
-        gs_strided_all<LOGC, 0>(sm, nv, twf, p);
-#pragma unroll
-        for (int m = 0; m < 32; m++) breg[m] = sm[pb + m];
-        gs_contig<5>(breg, c_w32[j], p);
-        __syncthreads();
+        if (g2 < total) rows_prefetch<LOGC>(sa, ra + ((size_t)j2 << logM), u2, nv, R);
+        else cp_async_commit();
     }
-    for (int f = t; f < nv * C; f += blockDim.x) {
-        const int v = f >> LOGC, i = f & (C - 1);
-        const int u = u0 + v;
-        sm[v * PC + padw(i)] = u < R ? abase[(size_t)u * C + i] : 0u;
-    }
-    __syncthreads();
-    gs_strided_all<LOGC, 0>(sm, nv, twf, p);
-    uint32_t xr[32];
-#pragma unroll
-    for (int m = 0; m < 32; m++) xr[m] = sm[pb + m];
-    gs_contig<5>(xr, c_w32[j], p);
-    const uint32_t sc = scale[j];
-#pragma unroll
-    for (int m = 0; m < 32; m++) {
-        const uint32_t y = squaring ? xr[m] : breg[m];
-        xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
-    }
-    ct_contig<5>(xr, c_w32[j], p);
-#pragma unroll
-    for (int m = 0; m < 32; m++) sm[pb + m] = xr[m];
-    __syncthreads();
-    ct_strided_all<LOGC, 0>(sm, nv, twi, p);
-    for (int f = t; f < nv * C; f += blockDim.x) {
-        const int v = f >> LOGC, i = f & (C - 1);
-        const int u = u0 + v;
-        if (u < R) abase[(size_t)u * C + i] = sm[v * PC + padw(i)];
-    }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------------------

@@ -58,13 +58,11 @@ __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table&
         for (int m = 0; m < E; m++) {
             if ((m & hm) == 0) {
                 const int k = m & (hm - 1);
-                const uint32_t a = x[m], b = x[m + hm];
-                x[m] = add_mod(a, b, p);
                 if (k == 0) {
-                    x[m + hm] = sub_mod(a, b, p);
+                    bfly_gs1(x[m], x[m + hm], p);
                 } else {
                     const uint2 w = W.f[k * (16 / hm)];
-                    x[m + hm] = mul_shoup(a - b + p, w.x, w.y, p);
+                    bfly_gs(x[m], x[m + hm], w.x, w.y, p);
                 }
             }
         }
@@ -83,71 +81,65 @@ __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table&
         for (int m = 0; m < E; m++) {
             if ((m & hm) == 0) {
                 const int k = m & (hm - 1);
-                uint32_t b = x[m + hm];
-                if (k != 0) {
+                if (k == 0) {
+                    bfly_ct1(x[m], x[m + hm], p);
+                } else {
                     const uint2 w = W.i[k * (16 / hm)];
-                    b = mul_shoup(b, w.x, w.y, p);
+                    bfly_ct(x[m], x[m + hm], w.x, w.y, p);
                 }
-                const uint32_t a = x[m];
-                x[m] = add_mod(a, b, p);
-                x[m + hm] = sub_mod(a, b, p);
             }
         }
     }
 }
 
-// Q Gentleman-Sande levels, half-sizes H..H/2^(Q-1), element stride S = H/2^(Q-1)
+// Q Gentleman-Sande levels, half-sizes H..H/2^(Q-1), element stride S = H/2^(Q-1).
+// Level t is a separate instantiation so every register index is a constant.
+template <int Q, int H, int t>
+__device__ __forceinline__ void gs_strided_level(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
+                                                 int jj0, uint32_t p)
+{
+    constexpr int E = 1 << Q;
+    constexpr int S = H >> (Q - 1);
+    constexpr int hm = E >> (t + 1);
+    constexpr int ht = H >> t;
+    uint2 w[hm];
+#pragma unroll
+    for (int k = 0; k < hm; k++) w[k] = tw[ht + jj0 + k * S];
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        if ((m & hm) == 0) bfly_gs(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
+    if constexpr (t + 1 < Q) gs_strided_level<Q, H, t + 1>(x, tw, jj0, p);
+}
+
 template <int Q, int H>
 __device__ __forceinline__ void gs_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
                                            int jj0, uint32_t p)
 {
-    constexpr int E = 1 << Q;
-    constexpr int S = H >> (Q - 1);
-#pragma unroll
-    for (int t = 0; t < Q; t++) {
-        constexpr int dummy = 0;
-        (void)dummy;
-        const int hm = E >> (t + 1);
-        const int ht = H >> t;
-        uint2 w[E / 2];
-#pragma unroll
-        for (int k = 0; k < hm; k++) w[k] = tw[ht + jj0 + k * S];
-#pragma unroll
-        for (int m = 0; m < E; m++) {
-            if ((m & hm) == 0) {
-                const uint2 ww = w[m & (hm - 1)];
-                const uint32_t a = x[m], b = x[m + hm];
-                x[m] = add_mod(a, b, p);
-                x[m + hm] = mul_shoup(a - b + p, ww.x, ww.y, p);
-            }
-        }
-    }
+    gs_strided_level<Q, H, 0>(x, tw, jj0, p);
 }
 
 // Q Cooley-Tukey levels, half-sizes H..2^(Q-1) H, element stride S = H
+template <int Q, int H, int t>
+__device__ __forceinline__ void ct_strided_level(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
+                                                 int jj0, uint32_t p)
+{
+    constexpr int E = 1 << Q;
+    constexpr int hm = 1 << t;
+    constexpr int ht = H << t;
+    uint2 w[hm];
+#pragma unroll
+    for (int k = 0; k < hm; k++) w[k] = twi[ht + jj0 + k * H];
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        if ((m & hm) == 0) bfly_ct(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
+    if constexpr (t + 1 < Q) ct_strided_level<Q, H, t + 1>(x, twi, jj0, p);
+}
+
 template <int Q, int H>
 __device__ __forceinline__ void ct_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
                                            int jj0, uint32_t p)
 {
-    constexpr int E = 1 << Q;
-#pragma unroll
-    for (int t = 0; t < Q; t++) {
-        const int hm = 1 << t;
-        const int ht = H << t;
-        uint2 w[E / 2];
-#pragma unroll
-        for (int k = 0; k < hm; k++) w[k] = twi[ht + jj0 + k * H];
-#pragma unroll
-        for (int m = 0; m < E; m++) {
-            if ((m & hm) == 0) {
-                const uint2 ww = w[m & (hm - 1)];
-                const uint32_t b = mul_shoup(x[m + hm], ww.x, ww.y, p);
-                const uint32_t a = x[m];
-                x[m] = add_mod(a, b, p);
-                x[m + hm] = sub_mod(a, b, p);
-            }
-        }
-    }
+    ct_strided_level<Q, H, 0>(x, twi, jj0, p);
 }
 
 // ---------------------------------------------------------------------------
