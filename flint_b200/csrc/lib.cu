@@ -559,7 +559,7 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
                               TimingRecord *tr)
 {
     const MulShape &S = L.S;
-    FWD_COLS[S.logR]<<<dim3(L.col_grid, np, sq ? 1 : 2), L.col_threads, L.col_smem, st>>>(
+    FWD_COLS[S.logR]<<<dim3(np, L.col_grid, sq ? 1 : 2), L.col_threads, L.col_smem, st>>>(
         X->T, a, an, b, bn, ra, rb, S.logC, S.G);
     timing_mark(tr, 1, st);
     const int items = L.row_grid * np;

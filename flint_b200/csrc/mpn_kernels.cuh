@@ -68,9 +68,61 @@ __host__ __device__ constexpr int cols_per_tile(int logR)
     return logR >= 11 ? 8 : (1 << (14 - logR));
 }
 
+// w^e for e in units of the largest transform, from the two-level tables
+__device__ __forceinline__ uint32_t table_power(uint32_t e, const uint2* __restrict__ th,
+                                                const uint2* __restrict__ tl, uint32_t p)
+{
+    const uint2 w1 = th[e >> 13];
+    const uint2 w2 = tl[e & 8191];
+    return mul_shoup(w1.x, w2.x, w2.y, p);
+}
+
+// Shoup companion floor(w 2^32 / p) on the device: a double-precision
+// estimate (error well below 1) corrected by one exact remainder test.
+__device__ __forceinline__ uint32_t shoup_companion_dev(uint32_t w, uint32_t p)
+{
+    const double est = (double)w * (4294967296.0 / (double)p);
+    uint32_t q = (uint32_t)est;
+    const int64_t r = (int64_t)((uint64_t)w << 32) - (int64_t)((uint64_t)q * p);
+    if (r >= (int64_t)p) q++;
+    else if (r < 0) q--;
+    return q;
+}
+
+// Four-step twist of the 32 consecutive column positions u = 32 s + m held by
+// one thread: position u gets w_M^(col * bitrev_r(u)).  Since
+// bitrev_r(32 s + m) = bitrev_(r-5)(s) + 2^(r-5) bitrev_5(m), the factors are
+// alpha * beta^k, k = bitrev_5(m), with alpha = w^(col bitrev_(r-5)(s)) and
+// beta = w^(col 2^(r-5)).  They are generated by a Shoup chain in Montgomery
+// form (F_(k+1) = F_k beta) and applied with one Montgomery product each,
+// so no table is read per element.
+template <int LOGR>
+__device__ __forceinline__ void twist32(uint32_t (&x)[32], uint32_t col, int s, int logM,
+                                        const uint2* __restrict__ th, const uint2* __restrict__ tl,
+                                        const PrimeInfo& P)
+{
+    const uint32_t p = P.p;
+    const uint32_t mmask = (1u << logM) - 1;
+    const int sh = LOG_MAXM - logM;
+    const uint32_t e0 = ((col * bitrev_bits((uint32_t)s, LOGR - 5)) & mmask) << sh;
+    const uint32_t e1 = ((col << (LOGR - 5)) & mmask) << sh;
+    const uint32_t alpha = table_power(e0, th, tl, p);
+    const uint32_t beta = table_power(e1, th, tl, p);
+    const uint32_t bq = shoup_companion_dev(beta, p);
+    uint32_t F = mul_mont(alpha, P.r2, p, P.pneg_inv);   // alpha in Montgomery form
+#pragma unroll
+    for (int k = 0; k < 32; k++) {
+        const int m = (int)(__brev((unsigned)k) >> 27);
+        x[m] = mul_mont(x[m], F, p, P.pneg_inv);
+        if (k < 31) F = mul_shoup(F, beta, bq, p);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Column pass, forward: split + length-R transforms + twist.
-// grid = (C / G, np, operands); smem = padw(R * G) words.
+// grid = (np, C / G, operands) -- the prime index varies fastest so that the
+// np tiles that read the same limbs run together and share them through L2;
+// smem = padw(R * G) words.
 template <int LOGR, int G>
 __global__ void __launch_bounds__(512)
 k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
@@ -82,8 +134,8 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     const int C = 1 << logC;
     const int logM = LOGR + logC;
     const int GR = G ? G : gcols;          // runtime tile width for short columns
-    const int j = blockIdx.y;
-    const int i0 = blockIdx.x * GR;
+    const int j = blockIdx.x;
+    const int i0 = blockIdx.y * GR;
     const bool opb = blockIdx.z != 0;
     const uint64_t* __restrict__ x = opb ? b : a;
     const uint64_t xn = opb ? bn : an;
@@ -93,13 +145,21 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     const uint64_t M = (uint64_t)1 << logM;
     const int tot = R * GR;
 
-    for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-        const int u = f / GR, c = f - u * GR;
-        uint64_t n = (uint64_t)u * C + i0 + c;
-        uint32_t r = 0;
+    if (xn <= M) {
+        for (int f = threadIdx.x; f < tot; f += blockDim.x) {
+            const int u = f / GR, c = f - u * GR;
+            const uint64_t n = (uint64_t)u * C + i0 + c;
+            sm[padw(u * GR) + c] = n < xn ? limb_redc(x[n], p, P.pneg_inv, P.c32) : 0u;
+        }
+    } else {
         // cyclic fold: an operand longer than M wraps around (x mod X^M - 1)
-        for (; n < xn; n += M) r = add_mod(r, limb_redc(x[n], p, P.pneg_inv, P.c32), p);
-        sm[padw(u * GR) + c] = r;
+        for (int f = threadIdx.x; f < tot; f += blockDim.x) {
+            const int u = f / GR, c = f - u * GR;
+            uint32_t r = 0;
+            for (uint64_t n = (uint64_t)u * C + i0 + c; n < xn; n += M)
+                r = add_mod(r, limb_redc(x[n], p, P.pneg_inv, P.c32), p);
+            sm[padw(u * GR) + c] = r;
+        }
     }
     __syncthreads();
     const uint2* __restrict__ th = T.th + (size_t)j * TH_SZ;
@@ -117,12 +177,9 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             for (int m = 0; m < 32; m++) xr[m] = sm[pb + padw(m * G)];
             gs_contig<5>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
+            twist32<LOGR>(xr, col, s, logM, th, tl, P);
 #pragma unroll
-            for (int m = 0; m < 32; m++) {
-                const uint32_t u = 32 * s + m;
-                const uint32_t e = ((col * bitrev_bits(u, LOGR)) & mmask) << sh;
-                out[(size_t)u * C + col] = twist_mul(xr[m], e, th, tl, p);
-            }
+            for (int m = 0; m < 32; m++) out[(size_t)(32 * s + m) * C + col] = xr[m];
         }
     } else {
         // short columns: one thread owns a whole column
@@ -271,7 +328,8 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols)
     const int j = blockIdx.y;
     const int i0 = blockIdx.x * GR;
     uint32_t* __restrict__ buf = ra + ((size_t)j << logM);
-    const uint32_t p = T.pi[j].p;
+    const PrimeInfo P = T.pi[j];
+    const uint32_t p = P.p;
     const uint2* __restrict__ th = T.thi + (size_t)j * TH_SZ;
     const uint2* __restrict__ tl = T.tli + (size_t)j * TL_SZ;
     const int sh = LOG_MAXM - logM;
@@ -284,11 +342,8 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols)
             const uint32_t col = (uint32_t)(i0 + v);
             uint32_t xr[32];
 #pragma unroll
-            for (int m = 0; m < 32; m++) {
-                const uint32_t u = 32 * s + m;
-                const uint32_t e = ((col * bitrev_bits(u, LOGR)) & mmask) << sh;
-                xr[m] = twist_mul(buf[(size_t)u * C + col], e, th, tl, p);
-            }
+            for (int m = 0; m < 32; m++) xr[m] = buf[(size_t)(32 * s + m) * C + col];
+            twist32<LOGR>(xr, col, s, logM, th, tl, P);
             ct_contig<5>(xr, c_w32[j], p);
             const int pb = 33 * G * s + v;
 #pragma unroll
@@ -333,14 +388,26 @@ struct CrtConst {
 };
 
 template <int NP>
+__device__ __forceinline__ void crt_values(const uint32_t (&y)[NP], const CrtConst& K, uint64_t& c0,
+                                           uint64_t& c1, uint64_t& c2);
+
+template <int NP>
 __device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ res, int logM, uint64_t n,
                                           const CrtConst& K, uint64_t& c0, uint64_t& c1, uint64_t& c2)
 {
     uint32_t y[NP];
+#pragma unroll
+    for (int jp = 0; jp < NP; jp++) y[jp] = res[((size_t)jp << logM) + n];
+    crt_values<NP>(y, K, c0, c1, c2);
+}
+
+template <int NP>
+__device__ __forceinline__ void crt_values(const uint32_t (&y)[NP], const CrtConst& K, uint64_t& c0,
+                                           uint64_t& c1, uint64_t& c2)
+{
     float fk = 0.0f;
 #pragma unroll
     for (int jp = 0; jp < NP; jp++) {
-        y[jp] = res[((size_t)jp << logM) + n];
         fk = fmaf((float)y[jp], K.finv[jp], fk);
     }
     // P/p_j has NP-1 words (one when NP == 1); the sum has NP words.
@@ -405,13 +472,31 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
     const uint32_t tile = sh_tile;
     const int64_t n0 = (int64_t)tile * TILE;
 
-    // coefficients n0-3 .. n0+TILE-1 into shared memory
-    for (int q = 0; q < PER; q++) {
-        const int idx = threadIdx.x * PER + q;
-        const uint64_t n = (uint64_t)(n0 + idx);
-        uint64_t c0 = 0, c1 = 0, c2 = 0;
-        if (n < L) crt_coeff<NP>(res, logM, n, K, c0, c1, c2);
-        X0[idx + 3] = c0; X1[idx + 3] = c1; X2[idx + 3] = c2;
+    // coefficients n0-3 .. n0+TILE-1 into shared memory; a thread's four
+    // residues per prime are one 16-byte load when they lie inside the array
+    {
+        const uint64_t nb = (uint64_t)(n0 + threadIdx.x * PER);
+        uint32_t y[PER][NP];
+        if (nb + PER <= ((uint64_t)1 << logM)) {
+#pragma unroll
+            for (int jp = 0; jp < NP; jp++) {
+                const uint4 v = *reinterpret_cast<const uint4*>(res + ((size_t)jp << logM) + nb);
+                y[0][jp] = v.x; y[1][jp] = v.y; y[2][jp] = v.z; y[3][jp] = v.w;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < PER; q++)
+#pragma unroll
+                for (int jp = 0; jp < NP; jp++)
+                    y[q][jp] = (nb + q < L) ? res[((size_t)jp << logM) + nb + q] : 0u;
+        }
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int idx = threadIdx.x * PER + q;
+            uint64_t c0 = 0, c1 = 0, c2 = 0;
+            if (nb + q < L) crt_values<NP>(y[q], K, c0, c1, c2);
+            X0[idx + 3] = c0; X1[idx + 3] = c1; X2[idx + 3] = c2;
+        }
     }
     if (threadIdx.x < 3) {
         const int64_t n = n0 - 3 + threadIdx.x;

@@ -210,49 +210,48 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
 }
 
 // Strided part of the forward transform: all levels with half-size >= 32,
-// i.e. LOGL - 5 levels, in passes of at most four (the first may be shorter).
-template <int LOGL, int G>
-__device__ __forceinline__ void gs_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
+// i.e. LOGL - 5 levels, split into as few passes as QMAX allows with their
+// sizes balanced (a one-level pass costs a full shared-memory round trip).
+template <int REM, int QMAX>
+constexpr int balanced_pass()
 {
-    constexpr int NS = LOGL - 5;
-    if constexpr (NS > 0) {
-        constexpr int Q0 = NS - 4 * ((NS - 1) / 4);
-        constexpr int H0 = 1 << (LOGL - 1);
-        gs_pass_smem<LOGL, Q0, H0, G>(sm, nv, tw, p);
+    return (REM + (REM + QMAX - 1) / QMAX - 1) / ((REM + QMAX - 1) / QMAX);
+}
+
+template <int LOGL, int G, int QMAX, int H, int REM>
+__device__ __forceinline__ void gs_passes(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
+{
+    if constexpr (REM > 0) {
+        constexpr int Q = balanced_pass<REM, QMAX>();
+        gs_pass_smem<LOGL, Q, H, G>(sm, nv, tw, p);
         __syncthreads();
-        if constexpr (NS > Q0) {
-            constexpr int H1 = H0 >> Q0;
-            gs_pass_smem<LOGL, 4, H1, G>(sm, nv, tw, p);
-            __syncthreads();
-            if constexpr (NS > Q0 + 4) {
-                constexpr int H2 = H1 >> 4;
-                gs_pass_smem<LOGL, 4, H2, G>(sm, nv, tw, p);
-                __syncthreads();
-            }
-        }
+        gs_passes<LOGL, G, QMAX, (H >> Q), REM - Q>(sm, nv, tw, p);
     }
 }
 
+template <int LOGL, int G, int QMAX = (G ? 4 : 5)>
+__device__ __forceinline__ void gs_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
+{
+    if constexpr (LOGL > 5) gs_passes<LOGL, G, QMAX, (1 << (LOGL - 1)), LOGL - 5>(sm, nv, tw, p);
+}
+
 // Strided part of the inverse transform (half-sizes 32 .. L/2), after the
-// contiguous first pass.
-template <int LOGL, int G>
+// contiguous first pass; the mirror image of the forward schedule.
+template <int LOGL, int G, int QMAX, int H, int REM>
+__device__ __forceinline__ void ct_passes(uint32_t* sm, int nv, const uint2* __restrict__ twi, uint32_t p)
+{
+    if constexpr (REM > 0) {
+        constexpr int Q = balanced_pass<REM, QMAX>();
+        ct_pass_smem<LOGL, Q, H, G>(sm, nv, twi, p);
+        __syncthreads();
+        ct_passes<LOGL, G, QMAX, (H << Q), REM - Q>(sm, nv, twi, p);
+    }
+}
+
+template <int LOGL, int G, int QMAX = (G ? 4 : 5)>
 __device__ __forceinline__ void ct_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ twi, uint32_t p)
 {
-    constexpr int NS = LOGL - 5;
-    if constexpr (NS > 0) {
-        constexpr int Q0 = NS - 4 * ((NS - 1) / 4);   // the last pass is the short one
-        if constexpr (NS > Q0) {
-            ct_pass_smem<LOGL, 4, 32, G>(sm, nv, twi, p);
-            __syncthreads();
-            if constexpr (NS > Q0 + 4) {
-                ct_pass_smem<LOGL, 4, 512, G>(sm, nv, twi, p);
-                __syncthreads();
-            }
-        }
-        constexpr int HL = 1 << (LOGL - Q0);
-        ct_pass_smem<LOGL, Q0, HL, G>(sm, nv, twi, p);
-        __syncthreads();
-    }
+    if constexpr (LOGL > 5) ct_passes<LOGL, G, QMAX, 32, LOGL - 5>(sm, nv, twi, p);
 }
 
 }  // namespace fb
