@@ -145,7 +145,19 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     const uint64_t M = (uint64_t)1 << logM;
     const int tot = R * GR;
 
-    if (xn <= M) {
+    if (LOGR >= 5 && xn <= M) {
+        // blockDim == G R / 32 == 512: thread t loads elements t + 512 k, i.e.
+        // rows u_t + k 512/G of its fixed column; shared offsets are constants
+        const int t = threadIdx.x;
+        const int GG = G ? G : 1;
+        const int u_t = t / GG, c = t & (GG - 1);
+        const uint64_t step = (uint64_t)(512 / GG) * C;
+        uint64_t n = (uint64_t)u_t * C + i0 + c;
+        uint32_t* d = sm + padw(u_t * GG) + c;
+#pragma unroll 8
+        for (int k = 0; k < R * GG / 512; k++, n += step)
+            d[k * 528] = n < xn ? limb_redc(x[n], p, P.pneg_inv, P.c32) : 0u;
+    } else if (xn <= M) {
         for (int f = threadIdx.x; f < tot; f += blockDim.x) {
             const int u = f / GR, c = f - u * GR;
             const uint64_t n = (uint64_t)u * C + i0 + c;
@@ -221,16 +233,32 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
+__device__ __forceinline__ void cp_async4_full(uint32_t* dst, const uint32_t* src)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src));
+}
+
 template <int LOGC>
 __device__ __forceinline__ void rows_prefetch(uint32_t* dst, const uint32_t* __restrict__ base,
                                               int u0, int nv, int R)
 {
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
-    for (int f = threadIdx.x; f < nv * C; f += blockDim.x) {
-        const int v = f >> LOGC, i = f & (C - 1);
-        const int u = u0 + v;
-        cp_async4(&dst[v * PC + padw(i)], base + (size_t)min(u, R - 1) * C + i, u < R);
+    constexpr int NSUB = C / 32;
+    if (nv == 1 && NSUB % 32 == 0) {
+        // one row, blockDim == C / 32: element t + k NSUB, compile-time offsets
+        const int t = threadIdx.x;
+        const uint32_t* src = base + (size_t)u0 * C + t;
+        uint32_t* d = dst + padw(t);
+#pragma unroll
+        for (int k = 0; k < 32; k++) cp_async4_full(d + k * (NSUB / 32 * 33), src + k * NSUB);
+    } else {
+        for (int f = threadIdx.x; f < nv * C; f += blockDim.x) {
+            const int v = f >> LOGC, i = f & (C - 1);
+            const int u = u0 + v;
+            cp_async4(&dst[v * PC + padw(i)], base + (size_t)min(u, R - 1) * C + i, u < R);
+        }
     }
     cp_async_commit();
 }
@@ -301,10 +329,17 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         __syncthreads();
         ct_strided_all<LOGC, 0>(sa, nv, twi, p);
         uint32_t* __restrict__ abase = ra + ((size_t)j << logM);
-        for (int f = t; f < nv * C; f += blockDim.x) {
-            const int v = f >> LOGC, i = f & (C - 1);
-            const int u = u0 + v;
-            if (u < R) abase[(size_t)u * C + i] = sa[v * PC + padw(i)];
+        if (nv == 1 && NSUB % 32 == 0) {
+            uint32_t* dst = abase + (size_t)u0 * C + t;
+            const uint32_t* s_ = sa + padw(t);
+#pragma unroll
+            for (int k = 0; k < 32; k++) dst[k * NSUB] = s_[k * (NSUB / 32 * 33)];
+        } else {
+            for (int f = t; f < nv * C; f += blockDim.x) {
+                const int v = f >> LOGC, i = f & (C - 1);
+                const int u = u0 + v;
+                if (u < R) abase[(size_t)u * C + i] = sa[v * PC + padw(i)];
+            }
         }
         __syncthreads();
         if (g2 < total) rows_prefetch<LOGC>(sa, ra + ((size_t)j2 << logM), u2, nv, R);
@@ -351,11 +386,15 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols)
         }
         __syncthreads();
         ct_strided_all<LOGR, G>(sm, 1, T.twi + (size_t)j * TW_SZ, p);
-        const int tot = R * G;
-        for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-            const int u = f / G, c = f - u * G;
-            buf[(size_t)u * C + i0 + c] = sm[padw(u * G) + c];
-        }
+        // blockDim == G R / 32 == 512: thread t stores rows u_t + k 512/G of
+        // its column (the inverse of the forward pass's load mapping)
+        const int t = threadIdx.x;
+        const int u_t = t / G, c = t & (G - 1);
+        const size_t step = (size_t)(512 / G) * C;
+        uint32_t* dst = buf + (size_t)u_t * C + i0 + c;
+        const uint32_t* s_ = sm + padw(u_t * G) + c;
+#pragma unroll 8
+        for (int k = 0; k < R * G / 512; k++) dst[k * step] = s_[k * 528];
     } else if constexpr (LOGR > 0) {
         for (int v = threadIdx.x; v < GR; v += blockDim.x) {
             const uint32_t col = (uint32_t)(i0 + v);
@@ -401,10 +440,118 @@ __device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ res, int 
     crt_values<NP>(y, K, c0, c1, c2);
 }
 
+// A[0..5] += y * (c0, c1, c2, c3): one PTX carry chain per partial-product row
+__device__ __forceinline__ void mac4(uint32_t (&A)[7], uint32_t y, const uint32_t* c)
+{
+    asm("mad.lo.cc.u32  %0, %7, %8, %0;\n\t"
+        "madc.lo.cc.u32 %1, %7, %9, %1;\n\t"
+        "madc.lo.cc.u32 %2, %7, %10, %2;\n\t"
+        "madc.lo.cc.u32 %3, %7, %11, %3;\n\t"
+        "addc.cc.u32    %4, %4, 0;\n\t"
+        "addc.u32       %5, %5, 0;\n\t"
+        "mad.hi.cc.u32  %1, %7, %8, %1;\n\t"
+        "madc.hi.cc.u32 %2, %7, %9, %2;\n\t"
+        "madc.hi.cc.u32 %3, %7, %10, %3;\n\t"
+        "madc.hi.cc.u32 %4, %7, %11, %4;\n\t"
+        "addc.u32       %5, %5, 0;"
+        : "+r"(A[0]), "+r"(A[1]), "+r"(A[2]), "+r"(A[3]), "+r"(A[4]), "+r"(A[5]), "+r"(A[6])
+        : "r"(y), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]));
+}
+
+// A[0..6] += y * (c0 .. c4)
+__device__ __forceinline__ void mac5(uint32_t (&A)[7], uint32_t y, const uint32_t* c)
+{
+    asm("mad.lo.cc.u32  %0, %7, %8, %0;\n\t"
+        "madc.lo.cc.u32 %1, %7, %9, %1;\n\t"
+        "madc.lo.cc.u32 %2, %7, %10, %2;\n\t"
+        "madc.lo.cc.u32 %3, %7, %11, %3;\n\t"
+        "madc.lo.cc.u32 %4, %7, %12, %4;\n\t"
+        "addc.cc.u32    %5, %5, 0;\n\t"
+        "addc.u32       %6, %6, 0;\n\t"
+        "mad.hi.cc.u32  %1, %7, %8, %1;\n\t"
+        "madc.hi.cc.u32 %2, %7, %9, %2;\n\t"
+        "madc.hi.cc.u32 %3, %7, %10, %3;\n\t"
+        "madc.hi.cc.u32 %4, %7, %11, %4;\n\t"
+        "madc.hi.cc.u32 %5, %7, %12, %5;\n\t"
+        "addc.u32       %6, %6, 0;"
+        : "+r"(A[0]), "+r"(A[1]), "+r"(A[2]), "+r"(A[3]), "+r"(A[4]), "+r"(A[5]), "+r"(A[6])
+        : "r"(y), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]));
+}
+
+// A[0..5] -= k * (P0 .. P4)   (k < 8; the result is non-negative)
+__device__ __forceinline__ void msub5(uint32_t (&A)[7], uint32_t k, const uint32_t* P)
+{
+    asm("{\n\t.reg .u32 t0, t1, t2, t3, t4, t5;\n\t"
+        "mul.lo.u32     t0, %6, %7;\n\t"
+        "mul.lo.u32     t1, %6, %8;\n\t"
+        "mul.lo.u32     t2, %6, %9;\n\t"
+        "mul.lo.u32     t3, %6, %10;\n\t"
+        "mul.lo.u32     t4, %6, %11;\n\t"
+        "mad.hi.cc.u32  t1, %6, %7, t1;\n\t"
+        "madc.hi.cc.u32 t2, %6, %8, t2;\n\t"
+        "madc.hi.cc.u32 t3, %6, %9, t3;\n\t"
+        "madc.hi.cc.u32 t4, %6, %10, t4;\n\t"
+        "madc.hi.u32    t5, %6, %11, 0;\n\t"
+        "sub.cc.u32     %0, %0, t0;\n\t"
+        "subc.cc.u32    %1, %1, t1;\n\t"
+        "subc.cc.u32    %2, %2, t2;\n\t"
+        "subc.cc.u32    %3, %3, t3;\n\t"
+        "subc.cc.u32    %4, %4, t4;\n\t"
+        "subc.u32       %5, %5, t5;\n\t}"
+        : "+r"(A[0]), "+r"(A[1]), "+r"(A[2]), "+r"(A[3]), "+r"(A[4]), "+r"(A[5])
+        : "r"(k), "r"(P[0]), "r"(P[1]), "r"(P[2]), "r"(P[3]), "r"(P[4]));
+}
+
+// A[0..6] -= k * (P0 .. P5)
+__device__ __forceinline__ void msub6(uint32_t (&A)[7], uint32_t k, const uint32_t* P)
+{
+    asm("{\n\t.reg .u32 t0, t1, t2, t3, t4, t5, t6;\n\t"
+        "mul.lo.u32     t0, %7, %8;\n\t"
+        "mul.lo.u32     t1, %7, %9;\n\t"
+        "mul.lo.u32     t2, %7, %10;\n\t"
+        "mul.lo.u32     t3, %7, %11;\n\t"
+        "mul.lo.u32     t4, %7, %12;\n\t"
+        "mul.lo.u32     t5, %7, %13;\n\t"
+        "mad.hi.cc.u32  t1, %7, %8, t1;\n\t"
+        "madc.hi.cc.u32 t2, %7, %9, t2;\n\t"
+        "madc.hi.cc.u32 t3, %7, %10, t3;\n\t"
+        "madc.hi.cc.u32 t4, %7, %11, t4;\n\t"
+        "madc.hi.cc.u32 t5, %7, %12, t5;\n\t"
+        "madc.hi.u32    t6, %7, %13, 0;\n\t"
+        "sub.cc.u32     %0, %0, t0;\n\t"
+        "subc.cc.u32    %1, %1, t1;\n\t"
+        "subc.cc.u32    %2, %2, t2;\n\t"
+        "subc.cc.u32    %3, %3, t3;\n\t"
+        "subc.cc.u32    %4, %4, t4;\n\t"
+        "subc.cc.u32    %5, %5, t5;\n\t"
+        "subc.u32       %6, %6, t6;\n\t}"
+        : "+r"(A[0]), "+r"(A[1]), "+r"(A[2]), "+r"(A[3]), "+r"(A[4]), "+r"(A[5]), "+r"(A[6])
+        : "r"(k), "r"(P[0]), "r"(P[1]), "r"(P[2]), "r"(P[3]), "r"(P[4]), "r"(P[5]));
+}
+
 template <int NP>
 __device__ __forceinline__ void crt_values(const uint32_t (&y)[NP], const CrtConst& K, uint64_t& c0,
                                            uint64_t& c1, uint64_t& c2)
 {
+    if constexpr (NP == 5 || NP == 6) {
+        // carry-chain form: X = sum_j y_j (P/p_j) - k P in 32-bit words
+        float fk = 0.0f;
+#pragma unroll
+        for (int jp = 0; jp < NP; jp++) fk = fmaf((float)y[jp], K.finv[jp], fk);
+        uint32_t A[7] = {0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int jp = 0; jp < NP; jp++) {
+            if constexpr (NP == 5) mac4(A, y[jp], K.cof[jp]);
+            else mac5(A, y[jp], K.cof[jp]);
+        }
+        const uint32_t k = (uint32_t)rintf(fk);
+        if constexpr (NP == 5) msub5(A, k, K.P);
+        else msub6(A, k, K.P);
+        c0 = (uint64_t)A[0] | ((uint64_t)A[1] << 32);
+        c1 = (uint64_t)A[2] | ((uint64_t)A[3] << 32);
+        c2 = (uint64_t)A[4] | (NP == 6 ? ((uint64_t)A[5] << 32) : 0ull);
+        return;
+    }
     float fk = 0.0f;
 #pragma unroll
     for (int jp = 0; jp < NP; jp++) {
