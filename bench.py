@@ -42,6 +42,15 @@ WORKLOADS = {
 }
 NS_LIMB_BITS = 64
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch measured
+# with ncu on the 2^22 x 2^22-limb case (M = 2^23, 5 primes); traffic grows in
+# proportion to the residue points, so a launch on another size scales by
+# M / 2^23.
+NCU_TRAFFIC_2P22 = {
+    "k_rows": 337.362944e6 + 122.715648e6,
+    "k_crt_carry": 167.829760e6 + 40.386304e6,
+}
+
 
 def splitmix_limbs(seed, n):
     """Same generator as the test fixtures (splitmix64), vectorised."""
@@ -305,8 +314,12 @@ def main():
         v["share"] = v["ms_per_launch"] / tot_ms
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
     alg_pipeline = 208 * (an + bn)
+    traffic = None
+    if dom in NCU_TRAFFIC_2P22 and args.workload in ("mpn24", "mpn22"):
+        scale = M / float(1 << 23)                # residue points relative to the capture
+        traffic = NCU_TRAFFIC_2P22[dom] * scale
     roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["GBps"], "peak": peak,
-                "unit": "GB/s", "frac": kern[dom]["GBps"] / peak, "traffic": None,
+                "unit": "GB/s", "frac": kern[dom]["GBps"] / peak, "traffic": traffic,
                 "peak_kind": peak_kind,
                 "pipeline": {"alg_bytes": alg_pipeline,
                              "achieved": alg_pipeline / (ms_step / 1e3) / 1e9,
