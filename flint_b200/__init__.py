@@ -54,6 +54,7 @@ SIGNATURES = {
     "gpu_mpn_ctx_mpn_mul_status": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U]),
     "_gpu_mpn_ctx_mpn_mul_range": (None, [_CTX, _P, _U, _U, _P, _U, _P, _U]),
     "gpu_mpn_mul_device": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, _P]),
+    "gpu_mpn_mul_device_noalloc": (ctypes.c_int, [_P, _P, _U, _P, _U, _P]),
     "_gpu_nmod_poly_mul_mid_mpn_ctx": (None, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_mul_mid_status": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),

@@ -14,6 +14,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -828,6 +829,278 @@ int gpu_mpn_ctx_kernel_times(gpu_mpn_ctx_t R, double *ms, long *count, int max)
         count[k] = X->kernel_count[k];
     }
     return n;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot call cudaMalloc: a host framework that owns every byte
+// of device memory through its own pool and forbids outside allocations (an
+// extra cudaMalloc would fragment or exceed its reservation), or a latency-
+// critical pipeline that cannot afford cudaMalloc's implicit device-wide
+// synchronisation in the middle of a run.  For them gpu_mpn_mul_device_noalloc
+// computes a product from caller-owned device buffers using only storage that
+// is part of this library's device image: the arrays below are allocated when
+// the module is loaded on a device and kept until the process exits, on every
+// GPU that loads the library.
+//
+// Limits: an + bn <= NA_MAX_LIMBS (transforms up to 2^18 points, five primes);
+// larger products are rejected with GPU_FFT_SMALL_ETOOBIG.  All calls share the
+// scratch, which keeps the last call's contents, so calls whose work overlaps on
+// the GPU (different streams, or different host threads) race and must be
+// serialised by the caller.
+constexpr int NA_LOG_MAXM = 18;
+constexpr uint64_t NA_MAX_LIMBS = ((uint64_t)1 << NA_LOG_MAXM) + 1;
+constexpr int NA_NP = 5;
+constexpr size_t NA_RES_WORDS = (size_t)2 * NA_NP << NA_LOG_MAXM;
+constexpr int NA_TILES = (int)((NA_MAX_LIMBS + 1023) / 1024);
+
+// scratch: residues of both operands, look-back status, ticket, error flag
+static __device__ __align__(256) uint32_t na_scratch[NA_RES_WORDS + NA_TILES + 8];
+// constant tables, written once per device by the set-up kernel
+static __device__ __align__(256) uint2 na_twf[NA_NP * TW_SZ];
+static __device__ __align__(256) uint2 na_twi[NA_NP * TW_SZ];
+static __device__ __align__(256) uint2 na_th[NA_NP * TH_SZ];
+static __device__ __align__(256) uint2 na_tl[NA_NP * TL_SZ];
+static __device__ __align__(256) uint2 na_thi[NA_NP * TH_SZ];
+static __device__ __align__(256) uint2 na_tli[NA_NP * TL_SZ];
+static __device__ __align__(256) PrimeInfo na_pi[MAX_NP];
+static __device__ __align__(256) uint32_t na_scale[(NA_LOG_MAXM + 1) * MAX_NP];
+__constant__ uint32_t c_na_primes[NA_NP];
+__constant__ uint2 c_na_roots[NA_NP];   // (w, w^-1), w of order 2^25
+
+__device__ uint32_t na_powmod(uint32_t a, uint32_t e, uint32_t p)
+{
+    uint64_t r = 1, x = a;
+    while (e) {
+        if (e & 1) r = r * x % p;
+        x = x * x % p;
+        e >>= 1;
+    }
+    return (uint32_t)r;
+}
+
+// twiddle and twist tables from the order-2^25 roots w[j] and their inverses
+__global__ void k_na_tables(uint2* twf, uint2* twi, uint2* th, uint2* tl, uint2* thi, uint2* tli)
+{
+    const uint2* roots = c_na_roots;
+    const int total = NA_NP * (TW_SZ + TH_SZ + TL_SZ);
+    for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < total; f += gridDim.x * blockDim.x) {
+        int r = f;
+        int kind, j, t;
+        if (r < NA_NP * TW_SZ) { kind = 0; j = r / TW_SZ; t = r % TW_SZ; }
+        else if ((r -= NA_NP * TW_SZ) < NA_NP * TH_SZ) { kind = 1; j = r / TH_SZ; t = r % TH_SZ; }
+        else { r -= NA_NP * TH_SZ; kind = 2; j = r / TL_SZ; t = r % TL_SZ; }
+        const uint32_t p = c_na_primes[j];
+        uint32_t e;
+        if (kind == 0) {
+            if (t == 0) { twf[r] = make_uint2(1, 0); twi[r] = make_uint2(1, 0); continue; }
+            const int lh = 31 - __clz(t);                 // t = 2^lh + jj
+            e = (uint32_t)(t - (1 << lh)) << (LOG_MAXM - lh - 1);
+        } else if (kind == 1) {
+            e = (uint32_t)t << 13;
+        } else {
+            e = (uint32_t)t;
+        }
+        const uint32_t wf = na_powmod(roots[j].x, e, p), wi = na_powmod(roots[j].y, e, p);
+        const uint2 vf = make_uint2(wf, shoup_companion_dev(wf, p));
+        const uint2 vi = make_uint2(wi, shoup_companion_dev(wi, p));
+        if (kind == 0) { twf[j * TW_SZ + t] = vf; twi[j * TW_SZ + t] = vi; }
+        else if (kind == 1) { th[j * TH_SZ + t] = vf; thi[j * TH_SZ + t] = vi; }
+        else { tl[j * TL_SZ + t] = vf; tli[j * TL_SZ + t] = vi; }
+    }
+}
+
+struct NaDevice {
+    bool ready = false;
+    Ctx ctx;                       // only T and nsm are used by the launches
+    uint32_t *res = nullptr, *status = nullptr, *scale = nullptr;
+    unsigned long long *ticket = nullptr;
+    int *err = nullptr;
+};
+constexpr int NA_MAX_DEVICES = 64;
+static NaDevice g_na[NA_MAX_DEVICES];
+static std::mutex g_na_lock;
+
+// 2^32-word product and cofactors of the first NA_NP primes, fixed-size
+static void na_crt_constants(CrtConst &K, uint32_t *cof_red)
+{
+    uint32_t P[MAX_NP + 1] = {1};
+    int n = 1;
+    for (int j = 0; j < NA_NP; j++) {
+        uint64_t c = 0;
+        for (int w = 0; w < n; w++) {
+            const uint64_t t = (uint64_t)P[w] * PRIMES[j] + c;
+            P[w] = (uint32_t)t;
+            c = t >> 32;
+        }
+        if (c) P[n++] = (uint32_t)c;
+    }
+    memset(&K, 0, sizeof K);
+    K.np = NA_NP;
+    for (int w = 0; w < n && w < MAX_NP; w++) K.P[w] = P[w];
+    for (int j = 0; j < NA_NP; j++) {
+        uint64_t r = 0;
+        for (int w = n - 1; w >= 0; w--) {
+            const uint64_t t = (r << 32) | P[w];
+            K.cof[j][w] = (uint32_t)(t / PRIMES[j]);
+            r = t % PRIMES[j];
+        }
+        uint64_t m = 0;
+        for (int w = n - 1; w >= 0; w--) m = ((m << 32) | K.cof[j][w]) % PRIMES[j];
+        cof_red[j] = (uint32_t)m;
+        K.finv[j] = 1.0f / (float)PRIMES[j];
+    }
+}
+
+// set-up runtime calls: no error message (that would allocate), just the code
+#define NA_CU(call)                                                           \
+    do {                                                                      \
+        if ((call) != cudaSuccess) return GPU_FFT_SMALL_ECUDA;                \
+    } while (0)
+
+static int na_setup(int dev, NaDevice &D)
+{
+    // order-2^25 roots of unity (forward, inverse) per prime
+    uint2 roots[NA_NP];
+    PrimeInfo pi[MAX_NP];
+    W32Table w32[MAX_NP];
+    memset(pi, 0, sizeof pi);
+    memset(w32, 0, sizeof w32);
+    for (int j = 0; j < NA_NP; j++) {
+        const uint32_t p = PRIMES[j];
+        uint32_t m = p - 1, f[16];
+        int nf = 0;
+        for (uint32_t q = 2; (uint64_t)q * q <= m; q++)
+            if (m % q == 0) {
+                f[nf++] = q;
+                while (m % q == 0) m /= q;
+            }
+        if (m > 1) f[nf++] = m;
+        uint32_t g = 2;
+        for (;; g++) {
+            bool ok = true;
+            for (int i = 0; i < nf; i++)
+                if (h_powmod(g, (p - 1) / f[i], p) == 1) { ok = false; break; }
+            if (ok) break;
+        }
+        const uint32_t w = h_powmod(g, (p - 1) >> LOG_MAXM, p), wi = h_invmod(w, p);
+        roots[j] = make_uint2(w, wi);
+        PrimeInfo &P = pi[j];
+        P.p = p;
+        uint32_t inv = 1;
+        for (int it = 0; it < 5; it++) inv *= 2 - p * inv;
+        P.pneg_inv = 0u - inv;
+        P.c32 = (uint32_t)((1ull << 32) % p);
+        P.r2 = h_mulmod(P.c32, P.c32, p);
+        P.finv = 1.0f / (float)p;
+        const uint32_t w32f = h_powmod(w, 1u << (LOG_MAXM - 5), p), w32i = h_invmod(w32f, p);
+        uint32_t x = 1, xi = 1;
+        for (int k = 0; k < 16; k++) {
+            w32[j].f[k] = make_uint2(x, shoup_companion(x, p));
+            w32[j].i[k] = make_uint2(xi, shoup_companion(xi, p));
+            x = h_mulmod(x, w32f, p);
+            xi = h_mulmod(xi, w32i, p);
+        }
+    }
+    // device addresses of the image's arrays, taken with this device current
+    void *scr = nullptr, *twf, *twi, *th, *tl, *thi, *tli, *pip, *sc;
+    NA_CU(cudaGetSymbolAddress(&scr, na_scratch));
+    NA_CU(cudaGetSymbolAddress(&twf, na_twf));
+    NA_CU(cudaGetSymbolAddress(&twi, na_twi));
+    NA_CU(cudaGetSymbolAddress(&th, na_th));
+    NA_CU(cudaGetSymbolAddress(&tl, na_tl));
+    NA_CU(cudaGetSymbolAddress(&thi, na_thi));
+    NA_CU(cudaGetSymbolAddress(&tli, na_tli));
+    NA_CU(cudaGetSymbolAddress(&pip, na_pi));
+    NA_CU(cudaGetSymbolAddress(&sc, na_scale));
+    for (int r = 0; r < 12; r++) {
+        NA_CU(cudaFuncSetAttribute(FWD_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        NA_CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    }
+    for (int c = 5; c <= LOG_MAXC; c++)
+        NA_CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    NA_CU(cudaMemcpyToSymbol(c_na_primes, PRIMES, sizeof(uint32_t) * NA_NP));
+    NA_CU(cudaMemcpyToSymbol(c_na_roots, roots, sizeof roots));
+    NA_CU(cudaMemcpyToSymbol(c_w32, w32, sizeof(W32Table) * MAX_NP));
+    const uint32_t one = 1, minus_one = 0xffffffffu;
+    NA_CU(cudaMemcpyToSymbol(c_one, &one, sizeof one));
+    NA_CU(cudaMemcpyToSymbol(c_minus_one, &minus_one, sizeof minus_one));
+    NA_CU(cudaMemcpyToSymbol(na_pi, pi, sizeof pi));
+    k_na_tables<<<256, 256>>>((uint2 *)twf, (uint2 *)twi, (uint2 *)th, (uint2 *)tl, (uint2 *)thi,
+                              (uint2 *)tli);
+    NA_CU(cudaGetLastError());
+    // pointwise scales for five primes and every transform length
+    CrtConst K;
+    uint32_t cof_red[MAX_NP];
+    na_crt_constants(K, cof_red);
+    uint32_t scales[(NA_LOG_MAXM + 1) * MAX_NP];
+    memset(scales, 0, sizeof scales);
+    for (int lm = 0; lm <= NA_LOG_MAXM; lm++)
+        for (int j = 0; j < NA_NP; j++) {
+            const uint32_t p = PRIMES[j];
+            uint32_t s = h_invmod(h_powmod(2, lm, p), p);
+            s = h_mulmod(s, h_invmod(cof_red[j], p), p);
+            scales[lm * MAX_NP + j] = h_mulmod(s, h_powmod(2, 128, p), p);
+        }
+    NA_CU(cudaMemcpyToSymbol(na_scale, scales, sizeof scales));
+    NA_CU(cudaDeviceSynchronize());
+    D.ctx.device = dev;
+    NA_CU(cudaDeviceGetAttribute(&D.ctx.nsm, cudaDevAttrMultiProcessorCount, dev));
+    D.ctx.T.pi = (const PrimeInfo *)pip;
+    D.ctx.T.twf = (const uint2 *)twf;
+    D.ctx.T.twi = (const uint2 *)twi;
+    D.ctx.T.th = (const uint2 *)th;
+    D.ctx.T.tl = (const uint2 *)tl;
+    D.ctx.T.thi = (const uint2 *)thi;
+    D.ctx.T.tli = (const uint2 *)tli;
+    D.ctx.crt[NA_NP] = K;
+    D.res = (uint32_t *)scr;
+    D.status = D.res + NA_RES_WORDS;
+    D.ticket = (unsigned long long *)(D.status + NA_TILES + (NA_TILES & 1));   // 8-byte aligned
+    D.err = (int *)(D.ticket + 1);
+    D.scale = (uint32_t *)sc;
+    D.ready = true;
+    return 0;
+}
+
+extern "C" {
+
+int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong an,
+                               const uint64_t *b_dev, gpu_ulong bn, void *stream)
+{
+    if (an == 0 || bn == 0 || !z_dev || !a_dev || !b_dev) return GPU_FFT_SMALL_EINVAL;
+    if (an + bn > NA_MAX_LIMBS) return GPU_FFT_SMALL_ETOOBIG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES)
+        return GPU_FFT_SMALL_ECUDA;
+    NaDevice &D = g_na[dev];
+    if (!D.ready) {
+        std::lock_guard<std::mutex> guard(g_na_lock);
+        if (!D.ready && na_setup(dev, D) != 0) return GPU_FFT_SMALL_ECUDA;
+    }
+    const cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t L = an + bn - 1;
+    int logM = MIN_LOGM;
+    while (((uint64_t)1 << logM) < L) logM++;
+    const LaunchShape shape = make_shape(logM);
+    const bool sq = (a_dev == b_dev) && (an == bn);
+    const size_t M = (size_t)1 << logM;
+    uint32_t *ra = D.res, *rb = D.res + (size_t)NA_NP * M;
+    const uint64_t zn = an + bn;
+    constexpr int THREADS = 256, TILE = 4 * THREADS;
+    const size_t tiles = (zn + TILE - 1) / TILE;
+    // the scratch keeps the previous call's contents: clear the look-back
+    // status, the tile ticket and the error flag
+    if (cudaMemsetAsync(D.status, 0, (NA_TILES + 8) * sizeof(uint32_t), st) != cudaSuccess)
+        return GPU_FFT_SMALL_ECUDA;
+    launch_transforms(&D.ctx, shape, NA_NP, a_dev, an, b_dev, bn, ra, rb, sq,
+                      D.scale + (size_t)logM * MAX_NP, st, nullptr);
+    k_crt_carry<NA_NP, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, L, zn, z_dev, D.ctx.crt[NA_NP],
+                                                          D.status, D.ticket, 0ull, 1u, D.err);
+    return cudaGetLastError() == cudaSuccess ? GPU_FFT_SMALL_OK : GPU_FFT_SMALL_ECUDA;
 }
 
 }  // extern "C"

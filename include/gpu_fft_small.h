@@ -101,6 +101,28 @@ GPU_FFT_SMALL_API int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev,
                        const uint64_t *a_dev, gpu_ulong an,
                        const uint64_t *b_dev, gpu_ulong bn, void *stream);
 
+/* Allocation-free product on device pointers (no counterpart in the
+   reference).  For callers that cannot call cudaMalloc: a framework that owns
+   all device memory through its own pool and forbids outside allocations, or
+   a latency-critical pipeline that cannot take cudaMalloc's implicit
+   device-wide synchronisation.  The caller passes device buffers for a, b and
+   z; every other byte used lives in arrays that are part of the library's
+   device image (about 10 MB of scratch plus 2 MB of tables, held on every GPU
+   that loads the library until the process exits).  The call allocates
+   nothing and does not synchronise; the work goes on `stream` (NULL is CUDA's
+   default stream).
+     * Limit: an + bn <= 2^18 + 1 limbs; larger products return
+       GPU_FFT_SMALL_ETOOBIG.  Empty operands return GPU_FFT_SMALL_EINVAL.
+     * The first call on a device does a one-time set-up there (table
+       generation, a device synchronisation); make that first call before
+       any stream capture.
+     * All calls share the scratch, which keeps the last call's contents:
+       calls whose work overlaps on the GPU (other streams, other host
+       threads) race, so the caller must serialise them. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev,
+                                                 gpu_ulong an, const uint64_t *b_dev,
+                                                 gpu_ulong bn, void *stream);
+
 /* --- nmod polynomials ---------------------------------------------------- */
 
 /* z[0, zh-zl) = coefficients [zl, zh) of a * b mod n, inputs reduced mod n.
