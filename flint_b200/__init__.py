@@ -41,6 +41,18 @@ class _Nmod(ctypes.Structure):
     _fields_ = [("n", ctypes.c_ulong), ("ninv", ctypes.c_ulong), ("norm", ctypes.c_ulong)]
 
 
+class MulReq(ctypes.Structure):
+    """gpu_mpn_mul_req: one product z = a * b of a batch (device pointers)."""
+    _fields_ = [("z", ctypes.c_void_p), ("a", ctypes.c_void_p), ("an", ctypes.c_ulong),
+                ("b", ctypes.c_void_p), ("bn", ctypes.c_ulong)]
+
+
+class BatchOptions(ctypes.Structure):
+    """gpu_mpn_batch_options: schedule knobs of a batch."""
+    _fields_ = [("promote_small", ctypes.c_int), ("max_streams", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
+
+
 # symbol -> (restype, argtypes); every symbol include/gpu_fft_small.h declares
 _P = ctypes.c_void_p
 _U = ctypes.c_ulong
@@ -60,6 +72,12 @@ SIGNATURES = {
     "gpu_get_default_mpn_ctx": (_CTX, []),
     "gpu_mpn_mul_default_mpn_ctx": (None, [_P, _P, _S, _P, _S]),
     "_gpu_nmod_poly_mul_mid_default_mpn_ctx": (None, [_P, _S, _S, _P, _S, _P, _S, _Nmod]),
+    "gpu_mpn_batch_init": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, ctypes.c_size_t, _P]),
+    "gpu_mpn_batch_run": (ctypes.c_int, [_P, _P]),
+    "gpu_mpn_batch_check": (ctypes.c_int, [_P, _P]),
+    "gpu_mpn_batch_launches": (ctypes.c_int, [_P]),
+    "gpu_mpn_batch_classes": (ctypes.c_int, [_P]),
+    "gpu_mpn_batch_clear": (None, [_P]),
     "gpu_fft_small_set_throw": (None, [_P]),
     "gpu_fft_small_last_error": (ctypes.c_char_p, []),
     "gpu_mpn_mul_plan": (ctypes.c_int, [_U, _U, ctypes.POINTER(ctypes.c_int),
@@ -189,3 +207,50 @@ class MpnCtx:
         cnt = (ctypes.c_long * 8)()
         n = lib().gpu_mpn_ctx_kernel_times(self.ptr, ms, cnt, 8)
         return {KERNEL_SLOTS[k]: (ms[k], cnt[k]) for k in range(n)}
+
+
+class MpnBatch:
+    """A planned batch of uneven products on device pointers (gpu_mpn_batch_*).
+
+    `reqs` is a sequence of (z_ptr, a_ptr, an, b_ptr, bn) with device
+    pointers as ints.  run() queues every product on `stream` and returns
+    without synchronising; check() waits and raises on a kernel error.
+    """
+
+    def __init__(self, ctx, reqs, promote_small=0, max_streams=4, use_graph=True):
+        arr = (MulReq * len(reqs))(*[MulReq(z, a, an, b, bn) for (z, a, an, b, bn) in reqs])
+        opt = BatchOptions(promote_small, max_streams, 1 if use_graph else 0)
+        self._h = ctypes.c_void_p()
+        _check(lib().gpu_mpn_batch_init(ctypes.byref(self._h), ctx.ptr, arr, len(reqs),
+                                        ctypes.byref(opt)))
+
+    def run(self, stream=None):
+        _check(lib().gpu_mpn_batch_run(self._h, stream))
+
+    def check(self, stream=None):
+        _check(lib().gpu_mpn_batch_check(self._h, stream))
+
+    @property
+    def launches(self):
+        return int(lib().gpu_mpn_batch_launches(self._h))
+
+    @property
+    def classes(self):
+        return int(lib().gpu_mpn_batch_classes(self._h))
+
+    def close(self):
+        if self._h:
+            lib().gpu_mpn_batch_clear(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -307,10 +307,10 @@ static int ctx_build_tables(Ctx *X)
 // ---------------------------------------------------------------------------
 // kernel dispatch by transform shape (column length 2^logR, row length 2^logC)
 typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t,
-                            uint32_t *, uint32_t *, int, int);
-typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int);
+                            uint32_t *, uint32_t *, int, int, const InstDesc *, int);
+typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int, const InstDesc *);
 typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, const uint32_t *,
-                        int);
+                        int, const InstDesc *, int);
 
 template <int LOGR>
 constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
@@ -358,11 +358,12 @@ static LaunchShape make_shape(int logM)
     return L;
 }
 
-// the three transform launches shared by every product type
+// the three transform launches shared by every product type; with a batch
+// descriptor array (ninst products of this shape) a, b, ra, rb are ignored
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
-                              TimingRecord *tr);
+                              TimingRecord *tr, const InstDesc *desc = nullptr, int ninst = 1);
 
 static int upload_scales(Ctx *X);
 
@@ -554,20 +555,40 @@ static int upload_scales(Ctx *X)
     return 0;
 }
 
+// Resident row CTAs per SM for a shape: 1 for long rows (512 threads, ~135 KB
+// of shared memory), several for short ones.  The row shape depends on logC
+// alone (rows shorter than 2^14 only occur with R = 1, one row per item).
+static int rows_per_sm(const LaunchShape &L)
+{
+    static int occ[LOG_MAXC + 1] = {0};
+    const int c = L.S.logC;
+    if (occ[c] == 0) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ROWS[c], L.row_threads, L.row_smem) !=
+                cudaSuccess || n < 1)
+            n = 1;
+        occ[c] = n;
+    }
+    return occ[c];
+}
+
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
-                              TimingRecord *tr)
+                              TimingRecord *tr, const InstDesc *desc, int ninst)
 {
     const MulShape &S = L.S;
-    FWD_COLS[S.logR]<<<dim3(np, L.col_grid, sq ? 1 : 2), L.col_threads, L.col_smem, st>>>(
-        X->T, a, an, b, bn, ra, rb, S.logC, S.G);
+    const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
+    FWD_COLS[S.logR]<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
+        X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np);
     timing_mark(tr, 1, st);
-    const int items = L.row_grid * np;
-    ROWS[S.logC]<<<std::min(items, X->nsm), L.row_threads, L.row_smem, st>>>(
-        X->T, ra, rb, S.logR, L.nv, np, d_scale, sq ? 1 : 0);
+    const int items = L.row_grid * np * (desc ? ninst : 1);
+    ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
+        X->T, ra, rb, S.logR, L.nv, np, d_scale, (sq && !desc) ? 1 : 0, desc, desc ? ninst : 1);
     timing_mark(tr, 2, st);
-    INV_COLS[S.logR]<<<dim3(L.col_grid, np), L.col_threads, L.col_smem, st>>>(X->T, ra, S.logC, S.G);
+    if (S.logR > 0)
+        INV_COLS[S.logR]<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
+            X->T, ra, S.logC, S.G, desc);
     timing_mark(tr, 3, st);
 }
 
@@ -602,10 +623,12 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr);
     if (np == 5)
         k_crt_carry<5, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
-                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err);
+                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err,
+                                                          nullptr, nullptr);
     else
         k_crt_carry<6, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
-                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err);
+                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err,
+                                                          nullptr, nullptr);
     launches++;
     timing_mark(tr, 4, st);
     X->ticket_base += tiles;
@@ -672,6 +695,10 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 // ---------------------------------------------------------------------------
 // nmod polynomials
 #include "nmod_host.inc"
+
+// ---------------------------------------------------------------------------
+// batches of uneven products
+#include "batch_host.inc"
 
 // ---------------------------------------------------------------------------
 // C ABI
@@ -775,6 +802,66 @@ void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gpu_slong zl, gpu_sl
 {
     _gpu_nmod_poly_mul_mid_mpn_ctx(res, (gpu_ulong)zl, (gpu_ulong)zh, a, (gpu_ulong)an, b,
                                    (gpu_ulong)bn, mod, gpu_get_default_mpn_ctx());
+}
+
+struct gpu_mpn_batch_struct {
+    Batch *impl;
+};
+
+int gpu_mpn_batch_init(gpu_mpn_batch_t *out, gpu_mpn_ctx_t R, const gpu_mpn_mul_req *reqs, size_t n,
+                       const gpu_mpn_batch_options *opt)
+{
+    if (!out) return set_error(GPU_FFT_SMALL_EINVAL, "null batch handle");
+    *out = nullptr;
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (n == 0 || !reqs) return set_error(GPU_FFT_SMALL_EINVAL, "empty batch");
+    if (opt && (opt->promote_small < 0 || opt->max_streams < 0))
+        return set_error(GPU_FFT_SMALL_EINVAL, "negative batch option");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    Batch *B = new Batch();
+    B->X = X;
+    rc = batch_plan(B, reqs, n, opt);
+    if (rc) {
+        batch_destroy(B);
+        return rc;
+    }
+    *out = new gpu_mpn_batch_struct{B};
+    return 0;
+}
+
+int gpu_mpn_batch_run(gpu_mpn_batch_t B, void *stream)
+{
+    if (!B || !B->impl) return set_error(GPU_FFT_SMALL_EINVAL, "batch not initialised");
+    return batch_run(B->impl, (cudaStream_t)stream);
+}
+
+int gpu_mpn_batch_check(gpu_mpn_batch_t B, void *stream)
+{
+    if (!B || !B->impl) return set_error(GPU_FFT_SMALL_EINVAL, "batch not initialised");
+    Ctx *X = B->impl->X;
+    int rc = bind_device(X);
+    if (rc) return rc;
+    CU(cudaStreamSynchronize((cudaStream_t)stream));
+    return check_device_error(X);
+}
+
+int gpu_mpn_batch_launches(gpu_mpn_batch_t B)
+{
+    return (B && B->impl) ? B->impl->launches : 0;
+}
+
+int gpu_mpn_batch_classes(gpu_mpn_batch_t B)
+{
+    return (B && B->impl) ? (int)B->impl->cls.size() : 0;
+}
+
+void gpu_mpn_batch_clear(gpu_mpn_batch_t B)
+{
+    if (!B) return;
+    batch_destroy(B->impl);
+    delete B;
 }
 
 void gpu_fft_small_set_throw(void (*handler)(int code, const char *msg))
@@ -1099,7 +1186,8 @@ int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong
     launch_transforms(&D.ctx, shape, NA_NP, a_dev, an, b_dev, bn, ra, rb, sq,
                       D.scale + (size_t)logM * MAX_NP, st, nullptr);
     k_crt_carry<NA_NP, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, L, zn, z_dev, D.ctx.crt[NA_NP],
-                                                          D.status, D.ticket, 0ull, 1u, D.err);
+                                                          D.status, D.ticket, 0ull, 1u, D.err,
+                                                          nullptr, nullptr);
     return cudaGetLastError() == cudaSuccess ? GPU_FFT_SMALL_OK : GPU_FFT_SMALL_ECUDA;
 }
 

@@ -118,16 +118,29 @@ __device__ __forceinline__ void twist32(uint32_t (&x)[32], uint32_t col, int s, 
     }
 }
 
+// One product of a batch: operands, result, its residue scratch (a's np
+// transforms at ra, b's at ra + np M) and its first CRT tile within the launch.
+struct InstDesc {
+    const uint64_t* a;
+    const uint64_t* b;
+    uint64_t* z;
+    uint32_t* ra;
+    uint64_t an, bn;
+    uint32_t tile0, ntiles;
+};
+
 // ---------------------------------------------------------------------------
 // Column pass, forward: split + length-R transforms + twist.
 // grid = (np, C / G, operands) -- the prime index varies fastest so that the
 // np tiles that read the same limbs run together and share them through L2;
+// with a batch descriptor, grid.z = 2 * instance + operand.
 // smem = padw(R * G) words.
 template <int LOGR, int G>
 __global__ void __launch_bounds__(512)
 k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
            const uint64_t* __restrict__ b, uint64_t bn,
-           uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols)
+           uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols,
+           const InstDesc* __restrict__ desc, int np)
 {
     extern __shared__ uint32_t sm[];
     constexpr int R = 1 << LOGR;
@@ -136,7 +149,13 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     const int GR = G ? G : gcols;          // runtime tile width for short columns
     const int j = blockIdx.x;
     const int i0 = blockIdx.y * GR;
-    const bool opb = blockIdx.z != 0;
+    const bool opb = (blockIdx.z & 1) != 0;
+    if (desc) {
+        const InstDesc& D = desc[blockIdx.z >> 1];
+        a = D.a; b = D.b; an = D.an; bn = D.bn;
+        ra = D.ra;
+        rb = D.ra + ((size_t)np << logM);
+    }
     const uint64_t* __restrict__ x = opb ? b : a;
     const uint64_t xn = opb ? bn : an;
     uint32_t* __restrict__ out = (opb ? rb : ra) + ((size_t)j << logM);
@@ -266,7 +285,8 @@ __device__ __forceinline__ void rows_prefetch(uint32_t* dst, const uint32_t* __r
 template <int LOGC>
 __global__ void __launch_bounds__(512, 1)
 k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
-       int logR, int nv, int np, const uint32_t* __restrict__ scale, int squaring)
+       int logR, int nv, int np, const uint32_t* __restrict__ scale, int squaring,
+       const InstDesc* __restrict__ desc, int ninst)
 {
     extern __shared__ uint32_t sm[];
     constexpr int C = 1 << LOGC;
@@ -275,24 +295,40 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     const int R = 1 << logR;
     const int logM = logR + LOGC;
     const int groups = (R + nv - 1) / nv;
-    const int total = groups * np;
+    const int per = groups * np;           // items of one product
+    const int total = per * ninst;
     uint32_t* sb = sm;
     uint32_t* sa = sm + nv * PC;
     const int t = threadIdx.x;
     const int pb = (t / NSUB) * PC + 33 * (t & (NSUB - 1));
+    // item -> (prime, first row, residue base of a, of b)
+    auto decode = [&](int gg, int& jj, int& uu, uint32_t*& A, const uint32_t*& B) {
+        const int inst = gg / per;
+        const int r = gg - inst * per;
+        jj = r / groups;
+        uu = (r - jj * groups) * nv;
+        if (desc) { A = desc[inst].ra; B = A + ((size_t)np << logM); }
+        else { A = ra; B = rb; }
+    };
 
     int g = blockIdx.x;
     if (g >= total) return;
     {
-        const int j = g / groups, u0 = (g - j * groups) * nv;
-        if (!squaring) rows_prefetch<LOGC>(sb, rb + ((size_t)j << logM), u0, nv, R);
+        int j, u0;
+        uint32_t* A;
+        const uint32_t* B;
+        decode(g, j, u0, A, B);
+        if (!squaring) rows_prefetch<LOGC>(sb, B + ((size_t)j << logM), u0, nv, R);
         else cp_async_commit();
-        rows_prefetch<LOGC>(sa, ra + ((size_t)j << logM), u0, nv, R);
+        rows_prefetch<LOGC>(sa, A + ((size_t)j << logM), u0, nv, R);
     }
     for (; g < total; g += gridDim.x) {
-        const int j = g / groups, u0 = (g - j * groups) * nv;
+        int j, u0, j2 = 0, u2 = 0;
+        uint32_t *A, *A2 = nullptr;
+        const uint32_t *B, *B2 = nullptr;
+        decode(g, j, u0, A, B);
         const int g2 = g + gridDim.x;
-        const int j2 = g2 / groups, u2 = (g2 - j2 * groups) * nv;
+        if (g2 < total) decode(g2, j2, u2, A2, B2);
         const PrimeInfo P = T.pi[j];
         const uint32_t p = P.p;
         const uint2* __restrict__ twf = T.twf + (size_t)j * TW_SZ;
@@ -308,7 +344,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
             gs_contig<5>(breg, c_w32[j], p);
             __syncthreads();
         }
-        if (!squaring && g2 < total) rows_prefetch<LOGC>(sb, rb + ((size_t)j2 << logM), u2, nv, R);
+        if (!squaring && g2 < total) rows_prefetch<LOGC>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
         else cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
@@ -328,7 +364,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         for (int m = 0; m < 32; m++) sa[pb + m] = xr[m];
         __syncthreads();
         ct_strided_all<LOGC, 0>(sa, nv, twi, p);
-        uint32_t* __restrict__ abase = ra + ((size_t)j << logM);
+        uint32_t* __restrict__ abase = A + ((size_t)j << logM);
         if (nv == 1 && NSUB % 32 == 0) {
             uint32_t* dst = abase + (size_t)u0 * C + t;
             const uint32_t* s_ = sa + padw(t);
@@ -342,7 +378,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
             }
         }
         __syncthreads();
-        if (g2 < total) rows_prefetch<LOGC>(sa, ra + ((size_t)j2 << logM), u2, nv, R);
+        if (g2 < total) rows_prefetch<LOGC>(sa, A2 + ((size_t)j2 << logM), u2, nv, R);
         else cp_async_commit();
     }
     cp_async_wait<0>();
@@ -350,10 +386,11 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
 
 // ---------------------------------------------------------------------------
 // Column pass, inverse: untwist in registers + length-R inverse transforms,
-// in place.  grid = (C / G, np); smem = padw(R * G) words.
+// in place.  grid = (C / G, np, instances); smem = padw(R * G) words.
 template <int LOGR, int G>
 __global__ void __launch_bounds__(512)
-k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols)
+k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
+           const InstDesc* __restrict__ desc)
 {
     extern __shared__ uint32_t sm[];
     constexpr int R = 1 << LOGR;
@@ -362,6 +399,7 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols)
     const int GR = G ? G : gcols;
     const int j = blockIdx.y;
     const int i0 = blockIdx.x * GR;
+    if (desc) ra = desc[blockIdx.z].ra;
     uint32_t* __restrict__ buf = ra + ((size_t)j << logM);
     const PrimeInfo P = T.pi[j];
     const uint32_t p = P.p;
@@ -605,7 +643,8 @@ __global__ void __launch_bounds__(THREADS)
 k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
             uint64_t* __restrict__ z, CrtConst K, uint32_t* __restrict__ status,
             unsigned long long* __restrict__ ticket, unsigned long long ticket_base,
-            uint32_t epoch, int* __restrict__ err)
+            uint32_t epoch, int* __restrict__ err,
+            const InstDesc* __restrict__ desc, const uint32_t* __restrict__ tile_inst)
 {
     constexpr int PER = 4;
     constexpr int TILE = PER * THREADS;
@@ -616,7 +655,20 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
 
     if (threadIdx.x == 0) sh_tile = (uint32_t)(atomicAdd(ticket, 1ull) - ticket_base);
     __syncthreads();
-    const uint32_t tile = sh_tile;
+    // `gtile` numbers tiles across the launch (status words, look-back order);
+    // `tile` is the tile inside its product: a batch launch runs the tiles of
+    // all its products back to back, and each product's first tile starts a
+    // fresh carry chain, so look-backs never cross into the previous product.
+    const uint32_t gtile = sh_tile;
+    uint32_t tile = gtile;
+    if (desc) {
+        const InstDesc& D = desc[tile_inst[gtile]];
+        tile = gtile - D.tile0;
+        res = D.ra;
+        L = D.an + D.bn - 1;
+        zn = D.an + D.bn;
+        z = D.z;
+    }
     const int64_t n0 = (int64_t)tile * TILE;
 
     // coefficients n0-3 .. n0+TILE-1 into shared memory; a thread's four
@@ -714,11 +766,11 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
         uint32_t cin = 0;
         if (tile == 0) {
             __threadfence();
-            atomicExch(&status[0], (epoch << 4) | ST_INC | (Gtile << 1));
+            atomicExch(&status[gtile], (epoch << 4) | ST_INC | (Gtile << 1));
         } else {
-            atomicExch(&status[tile], (epoch << 4) | ST_AGG | (Gtile << 1) | Ptile);
+            atomicExch(&status[gtile], (epoch << 4) | ST_AGG | (Gtile << 1) | Ptile);
             uint32_t Gr = 0, Pr = 1;
-            int64_t k = (int64_t)tile - 1;
+            int64_t k = (int64_t)gtile - 1;
             long spins = 0;
             while (true) {
                 const uint32_t st = *(volatile uint32_t*)&status[k];
@@ -736,7 +788,7 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
                 if (k < 0) { cin = Gr; break; }
             }
             const uint32_t cout = Gtile | (Ptile & cin);
-            atomicExch(&status[tile], (epoch << 4) | ST_INC | (cout << 1));
+            atomicExch(&status[gtile], (epoch << 4) | ST_INC | (cout << 1));
         }
         sh_carry_in = cin;
     }

@@ -154,6 +154,54 @@ GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gp
                                             const gpu_ulong *b, gpu_slong bn,
                                             gpu_nmod_t mod);
 
+/* --- batches of uneven products (no counterpart in the reference, which
+       multiplies one product per mpn_ctx_mpn_mul call, src/fft_small.h:433) */
+
+/* One product of a batch: z[0 .. an+bn) = a * b, all device pointers.  The
+   same rules as gpu_mpn_mul_device hold per product (no aliasing of z with
+   a or b; distinct products write disjoint z). */
+typedef struct {
+    gpu_ulong *z;
+    const gpu_ulong *a;
+    gpu_ulong an;
+    const gpu_ulong *b;
+    gpu_ulong bn;
+} gpu_mpn_mul_req;
+
+/* Schedule of a batch.  promote_small: products whose (primes, transform
+   length) class holds fewer than this many products are run at the next
+   longer length together with that class (0 = off).  max_streams: classes run
+   concurrently on up to this many streams (0 = 4).  use_graph: record the
+   first run as a CUDA graph and replay it afterwards. */
+typedef struct {
+    int promote_small;
+    int max_streams;
+    int use_graph;
+} gpu_mpn_batch_options;
+
+typedef struct gpu_mpn_batch_struct *gpu_mpn_batch_t;
+
+/* Plans a batch of n products over the context's device: groups them into
+   classes, allocates their residue scratch and descriptors.  opt == NULL
+   selects {0, 4, 1}.  The requests' pointers are captured; the operands may
+   change between runs, the pointers may not.  Returns 0 on success. */
+GPU_FFT_SMALL_API int gpu_mpn_batch_init(gpu_mpn_batch_t *B, gpu_mpn_ctx_t R,
+                                         const gpu_mpn_mul_req *reqs, size_t n,
+                                         const gpu_mpn_batch_options *opt);
+/* Queues every product of the batch on `stream` (NULL = CUDA's default
+   stream) and returns without synchronising.  Runs of one batch must not
+   overlap.  Kernel errors (a carry look-back that gave up) are reported by
+   gpu_mpn_batch_check. */
+GPU_FFT_SMALL_API int gpu_mpn_batch_run(gpu_mpn_batch_t B, void *stream);
+/* Waits for `stream` and returns GPU_FFT_SMALL_ETIMEOUT if any kernel of the
+   context recorded an error since the last check, else 0. */
+GPU_FFT_SMALL_API int gpu_mpn_batch_check(gpu_mpn_batch_t B, void *stream);
+/* Kernel launches of one run, and the number of (primes, length) classes. */
+GPU_FFT_SMALL_API int gpu_mpn_batch_launches(gpu_mpn_batch_t B);
+GPU_FFT_SMALL_API int gpu_mpn_batch_classes(gpu_mpn_batch_t B);
+/* Waits for pending runs and frees the batch. */
+GPU_FFT_SMALL_API void gpu_mpn_batch_clear(gpu_mpn_batch_t B);
+
 /* --- error handling ------------------------------------------------------ */
 
 /* Handler called by the void entry points on failure (the analogue of
