@@ -172,6 +172,117 @@ def cpu_baseline_run(an, bn, steps, warmup, max_seconds=60.0):
             "ms_per_step": med * 1e3, "steps_timed": len(times)}
 
 
+BATCH_N, BATCH_SEED = 4096, 4096
+
+
+def time_on_stream(torch, stream, fn, steps, warmup):
+    """Mean milliseconds of fn() over `steps` calls, CUDA events on `stream`."""
+    for _ in range(max(warmup, 3)):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds):
+    """4096 uneven products (an = round(2^U), U ~ U[10,18]; bn = an / 2^V,
+    V ~ U[0,4]): the per-instance device entry point in a loop against one
+    planned batch.  Returns the `batch` object of the JSON line."""
+    from flint_b200.workload import batch_operands, uneven_batch
+    sizes = uneven_batch(BATCH_SEED, BATCH_N)
+    host, spans = batch_operands(7, sizes)
+    total = int(sum(a + b for a, b in sizes))
+    d_in = torch.from_numpy(host.view(np.int64)).to(dev)
+    d_out = torch.empty(total, dtype=torch.int64, device=dev)
+    d_ref = torch.empty(total, dtype=torch.int64, device=dev)
+    reqs, zoffs, off = [], [], 0
+    for (ao, an, bo, bn) in spans:
+        reqs.append((d_out.data_ptr() + 8 * off, d_in.data_ptr() + 8 * ao, an,
+                     d_in.data_ptr() + 8 * bo, bn))
+        zoffs.append(off)
+        off += an + bn
+    delta = d_ref.data_ptr() - d_out.data_ptr()
+    s = stream.cuda_stream
+
+    def per_instance():
+        for (z, a, an, b, bn) in reqs:
+            ctx.mpn_mul_device(z + delta, a, an, b, bn, s)
+
+    bits = NS_LIMB_BITS * total
+    k_plain = max(2, steps // 3)
+    ms_plain = time_on_stream(torch, stream, per_instance, k_plain, 3)
+    B = FB.MpnBatch(ctx, reqs)
+    ms_batch = time_on_stream(torch, stream, lambda: B.run(s), steps, warmup)
+    B.check(s)
+    exact = bool(torch.equal(d_out, d_ref))
+    # residue fingerprints of a subsample (Python integers)
+    out = d_out.cpu().numpy().view(np.uint64)
+    q = 2305843009213693951
+    fp_ok = True
+    for k in range(0, BATCH_N, 97):
+        ao, an, bo, bn = spans[k]
+        zo = zoffs[k]
+        fp_ok &= (to_int(host[ao:ao + an]) % q) * (to_int(host[bo:bo + bn]) % q) % q == \
+            to_int(out[zo:zo + an + bn]) % q
+
+    # end to end: pinned host operands in, products out, copies inside the timed region
+    h_in = torch.from_numpy(host.view(np.int64)).pin_memory()
+    h_out = torch.empty(total, dtype=torch.int64).pin_memory()
+
+    def e2e():
+        d_in.copy_(h_in, non_blocking=True)
+        B.run(s)
+        h_out.copy_(d_out, non_blocking=True)
+
+    ms_e2e = time_on_stream(torch, stream, e2e, max(3, steps // 2), 2)
+    B.check(s)
+    e2e_ok = bool(np.array_equal(h_out.numpy().view(np.uint64), out))
+    res = {
+        "workload": "%d uneven products, an = round(2^U), U~U[10,18], bn = max(1, round(an/2^V)), "
+                    "V~U[0,4], seed %d" % (BATCH_N, BATCH_SEED),
+        "limbs": total, "classes": B.classes, "launches_per_step": B.launches,
+        "value": bits / ms_batch / 1e6, "unit": "Gbit/s", "ms_per_step": ms_batch,
+        "per_instance": {"value": bits / ms_plain / 1e6, "ms_per_step": ms_plain,
+                         "launches_per_step": 4 * BATCH_N},
+        "speedup_vs_per_instance": ms_plain / ms_batch,
+        "e2e": {"value": bits / ms_e2e / 1e6, "unit": "Gbit/s", "ms_per_step": ms_e2e,
+                "h2d_bytes_per_step": 8 * total, "d2h_bytes_per_step": 8 * total},
+        "exact_vs_per_instance": exact, "fingerprints_ok": bool(fp_ok), "e2e_matches": e2e_ok,
+        "roofline": {"bound": "hbm", "alg_bytes": 208 * total,
+                     "achieved": 208 * total / ms_batch / 1e6},
+    }
+    B.close()
+    if cpu_seconds > 0:
+        res["cpu_baseline"] = batch_cpu_baseline(sizes, host, spans, cpu_seconds)
+    return res
+
+
+def batch_cpu_baseline(sizes, host, spans, seconds):
+    """The reference's fft_small, one product at a time over the batch in
+    order (all host threads), until `seconds` have passed."""
+    import oracle
+    L, kind, nthreads = ref_library()
+    if L is None:
+        return None
+    t0 = time.perf_counter()
+    done_limbs, k = 0, 0
+    while k < len(spans) and time.perf_counter() - t0 < seconds:
+        ao, an, bo, bn = spans[k]
+        oracle.ref_mpn_mul(host[ao:ao + an], host[bo:bo + bn])
+        done_limbs += an + bn
+        k += 1
+    dt = time.perf_counter() - t0
+    return {"value": NS_LIMB_BITS * done_limbs / dt / 1e9, "unit": "Gbit/s",
+            "cores": min(nthreads, 8), "kind": kind,
+            "sample": "first %d of the %d products, one mpn_ctx_mpn_mul each" % (k, len(spans))}
+
+
 def kernel_bytes(name, an, bn, np_, M, L):
     """Algorithmic bytes each kernel must move in the four-pass design:
     residues are 4-byte words, np primes, M-point transforms."""
@@ -192,12 +303,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mpn24", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the 4096-product uneven batch")
     args = ap.parse_args()
     an, bn, desc = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    config = {"workload": desc + " (configs[1])" if args.workload == "mpn24" else desc,
+    config = {"workload": desc,
               "an": an, "bn": bn}
 
     if args.impl == "reference":
@@ -298,6 +411,10 @@ def main():
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
+    batch = None
+    if not args.no_batch:
+        batch = bench_batch(torch, FB, ctx, dev, stream, args.steps, args.warmup,
+                            cpu_seconds=0.0 if (world > 1 or args.no_cpu_baseline) else 10.0)
     clk = clocks.stop()
     e2e_ok = bool(np.array_equal(hz.numpy().view(np.uint64), z))
 
@@ -346,9 +463,11 @@ def main():
                 "h2d_bytes_per_step": 8 * (an + bn), "d2h_bytes_per_step": 8 * (an + bn),
                 "ms_per_step": e2e_s * 1e3},
         "gpu_launches": 4 * args.steps,
+        "gpu_launches_note": "headline product only; the batch object counts its own",
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk,
+        "batch": batch,
     }
     print(json.dumps(line), flush=True)
     if dist:

@@ -8,6 +8,8 @@ functions (src/fft_small.h):
     MpnCtx.mpn_mul(a, b)           mpn_ctx_mpn_mul
     MpnCtx.mpn_mul_range(..)       _mpn_ctx_mpn_mul_range
     MpnCtx.nmod_poly_mul_mid(..)   _nmod_poly_mul_mid_mpn_ctx
+    MpnCtx.fmpz_poly_mul_mid(..)   _fmpz_poly_mul_mid_mpn_ctx (raw coefficient rows)
+    MpnBatch(ctx, reqs)            batches of uneven products (no counterpart)
     MpnCtx.mpn_mul_device(..)      device-pointer twin (no host copies)
 
 There is no CPU fallback: if the library or a GPU is missing, every call
@@ -72,6 +74,12 @@ SIGNATURES = {
     "gpu_get_default_mpn_ctx": (_CTX, []),
     "gpu_mpn_mul_default_mpn_ctx": (None, [_P, _P, _S, _P, _S]),
     "_gpu_nmod_poly_mul_mid_default_mpn_ctx": (None, [_P, _S, _S, _P, _S, _P, _S, _Nmod]),
+    "_gpu_fmpz_poly_mul_mid_mpn_ctx": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _CTX]),
+    "_gpu_fmpz_poly_mul_mid_default_mpn_ctx": (ctypes.c_int, [_P, _S, _S, _P, _S, _P, _S]),
+    "gpu_fmpz_set_signed_hook": (None, [_P]),
+    "_gpu_fmpz_poly_mul_mid_raw": (ctypes.c_int, [_P, _U, _U, _U, _P, _U, _U, _P, _U, _U, _CTX]),
+    "gpu_fmpz_poly_mul_mid_device": (ctypes.c_int, [_CTX, _P, _U, _U, _U, _P, _U, _U, _P, _U,
+                                                    _U, _P]),
     "gpu_mpn_batch_init": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, ctypes.c_size_t, _P]),
     "gpu_mpn_batch_run": (ctypes.c_int, [_P, _P]),
     "gpu_mpn_batch_check": (ctypes.c_int, [_P, _P]),
@@ -129,6 +137,28 @@ def mpn_mul_plan(an, bn):
 
 def prime(i):
     return int(lib().gpu_fft_small_prime(i))
+
+
+def _raw_bits(x):
+    """Largest magnitude bit count over the rows of a two's complement array."""
+    if x.size == 0:
+        return 0
+    w = x.shape[1]
+    neg = (x[:, -1] >> np.uint64(63)).astype(bool)
+    best = 0
+    for row, s in zip(x, neg):
+        v = int.from_bytes(row.tobytes(), "little")
+        if s:
+            v = (1 << (64 * w)) - v
+        best = max(best, v.bit_length())
+    return best
+
+
+def fmpz_result_width(a, b):
+    """Limbs per coefficient that hold every coefficient of a * b."""
+    mn = min(len(a), len(b))
+    bits = _raw_bits(a) + _raw_bits(b) + (mn - 1).bit_length() + 1
+    return max(1, (bits + 63) // 64)
 
 
 class MpnCtx:
@@ -192,6 +222,25 @@ class MpnCtx:
                                                    b.ctypes.data, len(b), _Nmod(n, 0, 0),
                                                    self.ptr))
         return z
+
+    def fmpz_poly_mul_mid(self, zl, zh, a, b, zw=None):
+        """coefficients [zl, zh) of a * b for integer polynomials given as
+        (n, w) uint64 arrays of two's complement coefficients (raw form of
+        _fmpz_poly_mul_mid_mpn_ctx); returns a (zh - zl, zw) array."""
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = a if b is a else np.ascontiguousarray(b, dtype=np.uint64)
+        (an, aw), (bn, bw) = a.shape, b.shape
+        if zw is None:
+            zw = fmpz_result_width(a, b)
+        z = np.empty((max(zh - zl, 0), zw), dtype=np.uint64)
+        _check(lib()._gpu_fmpz_poly_mul_mid_raw(z.ctypes.data, zw, zl, zh, a.ctypes.data, aw, an,
+                                                b.ctypes.data, bw, bn, self.ptr))
+        return z
+
+    def fmpz_poly_mul_device(self, z_ptr, zw, zl, zh, a_ptr, aw, an, b_ptr, bw, bn, stream=None):
+        """Queue the raw-form window product on device pointers."""
+        _check(lib().gpu_fmpz_poly_mul_mid_device(self.ptr, z_ptr, zw, zl, zh, a_ptr, aw, an,
+                                                  b_ptr, bw, bn, stream))
 
     @property
     def last_launches(self):

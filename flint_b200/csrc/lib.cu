@@ -6,6 +6,7 @@
 #include "../../include/gpu_fft_small.h"
 #include "mpn_kernels.cuh"
 #include "nmod_kernels.cuh"
+#include "fmpz_kernels.cuh"
 
 #include <cuda_runtime.h>
 #include <math.h>
@@ -307,7 +308,7 @@ static int ctx_build_tables(Ctx *X)
 // ---------------------------------------------------------------------------
 // kernel dispatch by transform shape (column length 2^logR, row length 2^logC)
 typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t,
-                            uint32_t *, uint32_t *, int, int, const InstDesc *, int);
+                            uint32_t *, uint32_t *, int, int, const InstDesc *, int, FzShape);
 typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int, const InstDesc *);
 typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, const uint32_t *,
                         int, const InstDesc *, int);
@@ -315,11 +316,14 @@ typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, 
 template <int LOGR>
 constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
 
-#define FB_COLS(X) X<0, tmpl_cols<0>()>, X<1, tmpl_cols<1>()>, X<2, tmpl_cols<2>()>,      \
-                   X<3, tmpl_cols<3>()>, X<4, tmpl_cols<4>()>, X<5, tmpl_cols<5>()>,      \
-                   X<6, tmpl_cols<6>()>, X<7, tmpl_cols<7>()>, X<8, tmpl_cols<8>()>,      \
-                   X<9, tmpl_cols<9>()>, X<10, tmpl_cols<10>()>, X<11, tmpl_cols<11>()>
-static const fwd_cols_fn FWD_COLS[12] = {FB_COLS(k_fwd_cols)};
+#define FB_COLS(X, ...) X<0, tmpl_cols<0>() __VA_ARGS__>, X<1, tmpl_cols<1>() __VA_ARGS__>,        \
+                        X<2, tmpl_cols<2>() __VA_ARGS__>, X<3, tmpl_cols<3>() __VA_ARGS__>,        \
+                        X<4, tmpl_cols<4>() __VA_ARGS__>, X<5, tmpl_cols<5>() __VA_ARGS__>,        \
+                        X<6, tmpl_cols<6>() __VA_ARGS__>, X<7, tmpl_cols<7>() __VA_ARGS__>,        \
+                        X<8, tmpl_cols<8>() __VA_ARGS__>, X<9, tmpl_cols<9>() __VA_ARGS__>,        \
+                        X<10, tmpl_cols<10>() __VA_ARGS__>, X<11, tmpl_cols<11>() __VA_ARGS__>
+static const fwd_cols_fn FWD_COLS[12] = {FB_COLS(k_fwd_cols, , false)};
+static const fwd_cols_fn FWD_COLS_FZ[12] = {FB_COLS(k_fwd_cols, , true)};
 static const inv_cols_fn INV_COLS[12] = {FB_COLS(k_inv_cols)};
 static const rows_fn ROWS[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                                  k_rows<5>, k_rows<6>, k_rows<7>, k_rows<8>, k_rows<9>,
@@ -359,11 +363,13 @@ static LaunchShape make_shape(int logM)
 }
 
 // the three transform launches shared by every product type; with a batch
-// descriptor array (ninst products of this shape) a, b, ra, rb are ignored
+// descriptor array (ninst products of this shape) a, b, ra, rb are ignored;
+// with fz the operands are integer polynomials (an, bn coefficients)
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
-                              TimingRecord *tr, const InstDesc *desc = nullptr, int ninst = 1);
+                              TimingRecord *tr, const InstDesc *desc = nullptr, int ninst = 1,
+                              const FzShape *fz = nullptr);
 
 static int upload_scales(Ctx *X);
 
@@ -373,6 +379,7 @@ static int configure_kernels()
     if (done) return 0;
     for (int r = 0; r < 12; r++) {
         CU(cudaFuncSetAttribute(FWD_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(FWD_COLS_FZ[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
         CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
     for (int c = 5; c <= LOG_MAXC; c++)
@@ -575,12 +582,13 @@ static int rows_per_sm(const LaunchShape &L)
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
-                              TimingRecord *tr, const InstDesc *desc, int ninst)
+                              TimingRecord *tr, const InstDesc *desc, int ninst, const FzShape *fz)
 {
     const MulShape &S = L.S;
     const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
-    FWD_COLS[S.logR]<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
-        X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np);
+    const FzShape shape = fz ? *fz : FzShape{1, 1, 1};
+    (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
+        X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np, shape);
     timing_mark(tr, 1, st);
     const int items = L.row_grid * np * (desc ? ninst : 1);
     ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
@@ -701,6 +709,10 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 #include "batch_host.inc"
 
 // ---------------------------------------------------------------------------
+// integer polynomials
+#include "fmpz_host.inc"
+
+// ---------------------------------------------------------------------------
 // C ABI
 extern "C" {
 
@@ -802,6 +814,59 @@ void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gpu_slong zl, gpu_sl
 {
     _gpu_nmod_poly_mul_mid_mpn_ctx(res, (gpu_ulong)zl, (gpu_ulong)zh, a, (gpu_ulong)an, b,
                                    (gpu_ulong)bn, mod, gpu_get_default_mpn_ctx());
+}
+
+int _gpu_fmpz_poly_mul_mid_raw(gpu_ulong *z, gpu_ulong zw, gpu_ulong zl, gpu_ulong zh,
+                               const gpu_ulong *a, gpu_ulong aw, gpu_ulong an,
+                               const gpu_ulong *b, gpu_ulong bw, gpu_ulong bn, gpu_mpn_ctx_t R)
+{
+    return fmpz_mul_mid_host(get_ctx(R), z, zw, zl, zh, a, aw, an, b, bw, bn);
+}
+
+int gpu_fmpz_poly_mul_mid_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zw, gpu_ulong zl,
+                                 gpu_ulong zh, const uint64_t *a_dev, gpu_ulong aw, gpu_ulong an,
+                                 const uint64_t *b_dev, gpu_ulong bw, gpu_ulong bn, void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = fmpz_check_args(zw, aw, an, bw, bn);
+    if (rc) return rc;
+    if (zl >= zh) return 0;
+    rc = bind_device(X);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const gpu_ulong zn = an + bn - 1;
+    if (zh > zn) {
+        const gpu_ulong from = std::max(zl, zn);
+        CU(cudaMemsetAsync(z_dev + (from - zl) * zw, 0, (zh - from) * zw * 8, st));
+        if (zl >= zn) return 0;
+        zh = zn;
+    }
+    return fmpz_mul_mid_enqueue(X, z_dev, zw, zl, zh, a_dev, aw, an, b_dev, bw, bn, st);
+}
+
+int _gpu_fmpz_poly_mul_mid_mpn_ctx(gpu_slong *z, gpu_ulong zl, gpu_ulong zh, const gpu_slong *a,
+                                   gpu_ulong an, const gpu_slong *b, gpu_ulong bn, gpu_mpn_ctx_t R)
+{
+    const int rc = fmpz_poly_mul_mid_fmpz(get_ctx(R), z, zl, zh, a, an, b, bn);
+    if (rc < 0) {
+        raise_error(-rc);
+        return 0;
+    }
+    return rc;
+}
+
+int _gpu_fmpz_poly_mul_mid_default_mpn_ctx(gpu_slong *z, gpu_slong zl, gpu_slong zh,
+                                           const gpu_slong *a, gpu_slong an, const gpu_slong *b,
+                                           gpu_slong bn)
+{
+    return _gpu_fmpz_poly_mul_mid_mpn_ctx(z, (gpu_ulong)zl, (gpu_ulong)zh, a, (gpu_ulong)an, b,
+                                          (gpu_ulong)bn, gpu_get_default_mpn_ctx());
+}
+
+void gpu_fmpz_set_signed_hook(void (*set_signed)(gpu_slong *f, const gpu_ulong *limbs, gpu_slong n))
+{
+    g_fmpz_set_signed = set_signed;
 }
 
 struct gpu_mpn_batch_struct {

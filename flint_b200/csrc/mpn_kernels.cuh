@@ -129,18 +129,49 @@ struct InstDesc {
     uint32_t tile0, ntiles;
 };
 
+// Integer-polynomial operands: coefficient i of an operand is w 64-bit limbs
+// in two's complement (the top limb signed), chunk k of it is placed at
+// position i S + k of a polynomial in y (S = wa + wb - 1, so the chunk
+// products of different output coefficients never share a position).
+struct FzShape {
+    uint32_t S;       // slot stride in y
+    uint32_t wa, wb;  // limbs per coefficient of a and of b
+};
+
+// Residue (times 2^-32) of operand element n.  Limb source: limb n of an
+// xn-limb integer.  Coefficient source: chunk (n mod S) of coefficient n / S
+// of an xn-coefficient polynomial with w limbs per coefficient.
+template <bool FZ>
+__device__ __forceinline__ uint32_t load_residue(const uint64_t* __restrict__ x, uint64_t n, uint64_t xn,
+                                                 uint32_t S, uint32_t w, const PrimeInfo& P)
+{
+    if constexpr (!FZ) {
+        return n < xn ? limb_redc(x[n], P.p, P.pneg_inv, P.c32) : 0u;
+    } else {
+        const uint32_t nn = (uint32_t)n;      // y-lengths stay below 2^32
+        const uint32_t i = nn / S, k = nn - i * S;
+        if (k >= w || i >= xn) return 0u;
+        const uint64_t v = x[(size_t)i * w + k];
+        uint32_t r = limb_redc(v, P.p, P.pneg_inv, P.c32);
+        // a negative top limb stands for v - 2^64, and 2^64 2^-32 = 2^32
+        if (k == w - 1 && (int64_t)v < 0) r = sub_mod(r, P.c32, P.p);
+        return r;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Column pass, forward: split + length-R transforms + twist.
 // grid = (np, C / G, operands) -- the prime index varies fastest so that the
 // np tiles that read the same limbs run together and share them through L2;
-// with a batch descriptor, grid.z = 2 * instance + operand.
+// with a batch descriptor, grid.z = 2 * instance + operand.  FZ selects the
+// integer-polynomial source (an, bn count coefficients, shape in fz).
 // smem = padw(R * G) words.
-template <int LOGR, int G>
+template <int LOGR, int G, bool FZ>
 __global__ void __launch_bounds__(512)
 k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
            const uint64_t* __restrict__ b, uint64_t bn,
            uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols,
-           const InstDesc* __restrict__ desc, int np)
+           const InstDesc* __restrict__ desc, int np, FzShape fz)
 {
     extern __shared__ uint32_t sm[];
     constexpr int R = 1 << LOGR;
@@ -158,13 +189,14 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     }
     const uint64_t* __restrict__ x = opb ? b : a;
     const uint64_t xn = opb ? bn : an;
+    const uint32_t xw = opb ? fz.wb : fz.wa;
     uint32_t* __restrict__ out = (opb ? rb : ra) + ((size_t)j << logM);
     const PrimeInfo P = T.pi[j];
     const uint32_t p = P.p;
     const uint64_t M = (uint64_t)1 << logM;
     const int tot = R * GR;
 
-    if (LOGR >= 5 && xn <= M) {
+    if (LOGR >= 5 && (FZ || xn <= M)) {
         // blockDim == G R / 32 == 512: thread t loads elements t + 512 k, i.e.
         // rows u_t + k 512/G of its fixed column; shared offsets are constants
         const int t = threadIdx.x;
@@ -175,12 +207,12 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
         uint32_t* d = sm + padw(u_t * GG) + c;
 #pragma unroll 8
         for (int k = 0; k < R * GG / 512; k++, n += step)
-            d[k * 528] = n < xn ? limb_redc(x[n], p, P.pneg_inv, P.c32) : 0u;
-    } else if (xn <= M) {
+            d[k * 528] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
+    } else if (FZ || xn <= M) {
         for (int f = threadIdx.x; f < tot; f += blockDim.x) {
             const int u = f / GR, c = f - u * GR;
             const uint64_t n = (uint64_t)u * C + i0 + c;
-            sm[padw(u * GR) + c] = n < xn ? limb_redc(x[n], p, P.pneg_inv, P.c32) : 0u;
+            sm[padw(u * GR) + c] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
         }
     } else {
         // cyclic fold: an operand longer than M wraps around (x mod X^M - 1)
@@ -206,7 +238,7 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             uint32_t xr[32];
 #pragma unroll
             for (int m = 0; m < 32; m++) xr[m] = sm[pb + padw(m * G)];
-            gs_contig<5>(xr, c_w32[j], p);
+            gs_contig<5, false>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
             twist32<LOGR>(xr, col, s, logM, th, tl, P);
 #pragma unroll
@@ -218,7 +250,7 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             uint32_t xr[R];
 #pragma unroll
             for (int m = 0; m < R; m++) xr[m] = sm[padw(m * GR) + v];
-            if constexpr (LOGR > 0) gs_contig<LOGR>(xr, c_w32[j], p);
+            if constexpr (LOGR > 0) gs_contig<LOGR, false>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
 #pragma unroll
             for (int m = 0; m < R; m++) {
@@ -417,7 +449,7 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
 #pragma unroll
             for (int m = 0; m < 32; m++) xr[m] = buf[(size_t)(32 * s + m) * C + col];
             twist32<LOGR>(xr, col, s, logM, th, tl, P);
-            ct_contig<5>(xr, c_w32[j], p);
+            ct_contig<5, false>(xr, c_w32[j], p);
             const int pb = 33 * G * s + v;
 #pragma unroll
             for (int m = 0; m < 32; m++) sm[pb + padw(m * G)] = xr[m];
@@ -442,7 +474,7 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
                 const uint32_t e = ((col * bitrev_bits(m, LOGR)) & mmask) << sh;
                 xr[m] = twist_mul(buf[(size_t)m * C + col], e, th, tl, p);
             }
-            ct_contig<LOGR>(xr, c_w32[j], p);
+            ct_contig<LOGR, false>(xr, c_w32[j], p);
 #pragma unroll
             for (int m = 0; m < R; m++) buf[(size_t)m * C + col] = xr[m];
         }

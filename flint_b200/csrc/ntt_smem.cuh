@@ -16,6 +16,8 @@
 //   * the contiguous pass (the five levels h = 16..1): each thread owns 32
 //     consecutive positions; its twiddles are powers of w_32, the same for
 //     every thread, and come from constant memory.
+// Row passes (G == 0) route two additions per butterfly to the FMA pipe,
+// column passes one (see bfly_gs).
 // Shared memory holds one pad word per 32 (physical = a + a/32), which makes
 // both kinds of pass conflict-free and lets every address be a per-thread
 // base plus a compile-time offset.
@@ -47,7 +49,7 @@ __constant__ W32Table c_w32[MAX_NP];
 // butterflies on registers
 
 // Q Gentleman-Sande levels on 2^Q consecutive positions (half-sizes 2^(Q-1)..1)
-template <int Q>
+template <int Q, bool F = true>
 __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table& W, uint32_t p)
 {
     constexpr int E = 1 << Q;
@@ -62,7 +64,7 @@ __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table&
                     bfly_gs1(x[m], x[m + hm], p);
                 } else {
                     const uint2 w = W.f[k * (16 / hm)];
-                    bfly_gs(x[m], x[m + hm], w.x, w.y, p);
+                    bfly_gs<F>(x[m], x[m + hm], w.x, w.y, p);
                 }
             }
         }
@@ -70,7 +72,7 @@ __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table&
 }
 
 // Q Cooley-Tukey levels on 2^Q consecutive positions (half-sizes 1..2^(Q-1))
-template <int Q>
+template <int Q, bool F = true>
 __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table& W, uint32_t p)
 {
     constexpr int E = 1 << Q;
@@ -85,7 +87,7 @@ __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table&
                     bfly_ct1(x[m], x[m + hm], p);
                 } else {
                     const uint2 w = W.i[k * (16 / hm)];
-                    bfly_ct(x[m], x[m + hm], w.x, w.y, p);
+                    bfly_ct<F>(x[m], x[m + hm], w.x, w.y, p);
                 }
             }
         }
@@ -94,7 +96,7 @@ __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table&
 
 // Q Gentleman-Sande levels, half-sizes H..H/2^(Q-1), element stride S = H/2^(Q-1).
 // Level t is a separate instantiation so every register index is a constant.
-template <int Q, int H, int t>
+template <int Q, int H, int t, bool F>
 __device__ __forceinline__ void gs_strided_level(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
                                                  int jj0, uint32_t p)
 {
@@ -107,19 +109,19 @@ __device__ __forceinline__ void gs_strided_level(uint32_t (&x)[1 << Q], const ui
     for (int k = 0; k < hm; k++) w[k] = tw[ht + jj0 + k * S];
 #pragma unroll
     for (int m = 0; m < E; m++)
-        if ((m & hm) == 0) bfly_gs(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
-    if constexpr (t + 1 < Q) gs_strided_level<Q, H, t + 1>(x, tw, jj0, p);
+        if ((m & hm) == 0) bfly_gs<F>(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
+    if constexpr (t + 1 < Q) gs_strided_level<Q, H, t + 1, F>(x, tw, jj0, p);
 }
 
-template <int Q, int H>
+template <int Q, int H, bool F>
 __device__ __forceinline__ void gs_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
                                            int jj0, uint32_t p)
 {
-    gs_strided_level<Q, H, 0>(x, tw, jj0, p);
+    gs_strided_level<Q, H, 0, F>(x, tw, jj0, p);
 }
 
 // Q Cooley-Tukey levels, half-sizes H..2^(Q-1) H, element stride S = H
-template <int Q, int H, int t>
+template <int Q, int H, int t, bool F>
 __device__ __forceinline__ void ct_strided_level(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
                                                  int jj0, uint32_t p)
 {
@@ -131,15 +133,15 @@ __device__ __forceinline__ void ct_strided_level(uint32_t (&x)[1 << Q], const ui
     for (int k = 0; k < hm; k++) w[k] = twi[ht + jj0 + k * H];
 #pragma unroll
     for (int m = 0; m < E; m++)
-        if ((m & hm) == 0) bfly_ct(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
-    if constexpr (t + 1 < Q) ct_strided_level<Q, H, t + 1>(x, twi, jj0, p);
+        if ((m & hm) == 0) bfly_ct<F>(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
+    if constexpr (t + 1 < Q) ct_strided_level<Q, H, t + 1, F>(x, twi, jj0, p);
 }
 
-template <int Q, int H>
+template <int Q, int H, bool F>
 __device__ __forceinline__ void ct_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
                                            int jj0, uint32_t p)
 {
-    ct_strided_level<Q, H, 0>(x, twi, jj0, p);
+    ct_strided_level<Q, H, 0, F>(x, twi, jj0, p);
 }
 
 // ---------------------------------------------------------------------------
@@ -177,7 +179,7 @@ __device__ __forceinline__ void gs_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
-        gs_strided<Q, H>(x, tw, jj0, p);
+        gs_strided<Q, H, (G == 0)>(x, tw, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
     }
@@ -203,7 +205,7 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
-        ct_strided<Q, H>(x, twi, jj0, p);
+        ct_strided<Q, H, (G == 0)>(x, twi, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
     }

@@ -154,6 +154,54 @@ GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gp
                                             const gpu_ulong *b, gpu_slong bn,
                                             gpu_nmod_t mod);
 
+/* --- integer polynomials ---------------------------------------------------
+
+   Coefficients [zl, zh) of the product of integer polynomials a (an
+   coefficients) and b (bn).  Beyond an + bn - 1 the window is zero-filled.
+   Any coefficient size is handled (chunked Kronecker layout on 64-bit limbs);
+   the limits are a chunk-product length (an + bn - 1)(wa + wb - 1) <= 2^25 and
+   min(an,bn) min(wa,wb) < 2^53. */
+
+/* Same signature as _fmpz_poly_mul_mid_mpn_ctx (src/fft_small.h:856-860).
+   fmpz is FLINT's tagged word (src/flint.h.in:467-477); inputs may hold
+   inline values or mpz pointers.  Output coefficients are written through
+   the setter registered with gpu_fmpz_set_signed_hook (FLINT's
+   fmpz_set_signed_ui_array, src/fmpz.h:239, is the intended one); without a
+   setter only inline results into inline entries are possible and anything
+   else is an error.  Returns 1 on success and 0 when the product is beyond
+   the prime set or the transform length (the caller falls back, as
+   _fmpz_poly_mul does in src/fmpz_poly/mul.c:122-126); other failures go to
+   the throw handler. */
+GPU_FFT_SMALL_API int _gpu_fmpz_poly_mul_mid_mpn_ctx(gpu_slong *z, gpu_ulong zl, gpu_ulong zh,
+                                                     const gpu_slong *a, gpu_ulong an,
+                                                     const gpu_slong *b, gpu_ulong bn,
+                                                     gpu_mpn_ctx_t R);
+/* Same signature as _fmpz_poly_mul_mid_default_mpn_ctx (src/fft_small.h:862-865). */
+GPU_FFT_SMALL_API int _gpu_fmpz_poly_mul_mid_default_mpn_ctx(gpu_slong *z, gpu_slong zl, gpu_slong zh,
+                                                             const gpu_slong *a, gpu_slong an,
+                                                             const gpu_slong *b, gpu_slong bn);
+/* Output setter for the fmpz entry points: set *f to the n-limb two's
+   complement value at limbs (NULL unregisters). */
+GPU_FFT_SMALL_API void gpu_fmpz_set_signed_hook(void (*set_signed)(gpu_slong *f, const gpu_ulong *limbs,
+                                                                   gpu_slong n));
+
+/* Raw form (no counterpart in the reference; the fmpz entry points run on
+   it): each coefficient is a fixed number of 64-bit limbs in two's
+   complement -- aw for a, bw for b, zw for the result (zw must hold every
+   result coefficient: zw >= (bits(a) + bits(b) + ceil(log2 min(an,bn)) + 1)
+   / 64 rounded up; wider is sign-extended).  Host pointers; returns 0 or a
+   GPU_FFT_SMALL_E* code (ENOPRIMES / ETOOBIG beyond the limits above). */
+GPU_FFT_SMALL_API int _gpu_fmpz_poly_mul_mid_raw(gpu_ulong *z, gpu_ulong zw, gpu_ulong zl, gpu_ulong zh,
+                                                 const gpu_ulong *a, gpu_ulong aw, gpu_ulong an,
+                                                 const gpu_ulong *b, gpu_ulong bw, gpu_ulong bn,
+                                                 gpu_mpn_ctx_t R);
+/* Device-pointer twin of the raw form, queued on `stream`. */
+GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zw,
+                                                   gpu_ulong zl, gpu_ulong zh,
+                                                   const uint64_t *a_dev, gpu_ulong aw, gpu_ulong an,
+                                                   const uint64_t *b_dev, gpu_ulong bw, gpu_ulong bn,
+                                                   void *stream);
+
 /* --- batches of uneven products (no counterpart in the reference, which
        multiplies one product per mpn_ctx_mpn_mul call, src/fft_small.h:433) */
 

@@ -216,3 +216,156 @@ def digest(z):
     import hashlib
     return hashlib.blake2b(np.ascontiguousarray(z, dtype=np.uint64).tobytes(),
                            digest_size=16).hexdigest()
+
+
+# ---------------------------------------------------------------- integer polynomials
+# Coefficients travel as fixed-width two's complement limb rows (w limbs per
+# coefficient), the raw form of the GPU library; fmpz vectors of the
+# reference are built and read with its own fmpz_set_signed_ui_array /
+# fmpz_get_signed_ui_array (src/fmpz.h:238-239).
+
+def rand_fmpz_raw(seed, n, bits, w=None):
+    """n signed coefficients uniform in (-2^bits, 2^bits) as an (n, w) uint64
+    two's complement array, w = ceil((bits + 1) / 64) unless given."""
+    wm = (bits + 63) // 64
+    w = w or (bits + 1 + 63) // 64
+    mag = rand_limbs(seed, n * wm, top_nonzero=False).reshape(n, wm)
+    if bits % 64:
+        mag[:, -1] &= np.uint64((1 << (bits % 64)) - 1)
+    out = np.zeros((n, w), dtype=np.uint64)
+    out[:, :wm] = mag
+    neg = (rand_limbs(seed ^ 0x5DEECE66D, n, top_nonzero=False) & np.uint64(1)).astype(bool)
+    rows = out[neg]
+    rows = ~rows
+    carry = np.ones(len(rows), dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        for k in range(w):
+            v = rows[:, k] + carry
+            carry = ((v == 0) & (carry == 1)).astype(np.uint64)
+            rows[:, k] = v
+    out[neg] = rows
+    return out
+
+
+def fmpz_width(bits_a, bits_b, mn):
+    """Limbs per product coefficient for factors below 2^bits_a, 2^bits_b in
+    magnitude, at most mn terms per coefficient, plus a sign bit."""
+    return (bits_a + bits_b + (mn - 1).bit_length() + 1 + 63) // 64
+
+
+def raw_to_ints(raw):
+    """Signed integers of an (n, w) two's complement limb array."""
+    raw = np.ascontiguousarray(raw, dtype=np.uint64)
+    w = raw.shape[1]
+    top = 1 << (64 * w)
+    res = []
+    for row in raw:
+        v = int.from_bytes(row.tobytes(), "little")
+        res.append(v - top if v >> (64 * w - 1) else v)
+    return res
+
+
+def ints_to_raw(vals, w):
+    out = np.zeros((len(vals), w), dtype=np.uint64)
+    mod = 1 << (64 * w)
+    for i, v in enumerate(vals):
+        out[i] = np.frombuffer((v % mod).to_bytes(8 * w, "little"), dtype=np.uint64)
+    return out
+
+
+def fmpz_poly_mul_python(a, b):
+    """Exact product of integer polynomials (lists of ints) by Kronecker
+    substitution in Python integers; for test sizes."""
+    if not a or not b:
+        return []
+    ma = max(abs(x) for x in a)
+    mb = max(abs(x) for x in b)
+    k = ma.bit_length() + mb.bit_length() + min(len(a), len(b)).bit_length() + 2
+
+    def pack(p):
+        v = 0
+        for x in reversed(p):
+            v = (v << k) + x
+        return v
+
+    c = pack(a) * pack(b)
+    out = []
+    half, full = 1 << (k - 1), 1 << k
+    for _ in range(len(a) + len(b) - 1):
+        d = c & (full - 1)
+        if d >= half:
+            d -= full
+        out.append(d)
+        c = (c - d) >> k
+    assert c == 0
+    return out
+
+
+def _ref_fmpz():
+    L = ref()
+    if not getattr(L, "_fmpz_ready", False):
+        P, S = ctypes.c_void_p, ctypes.c_long
+        L._fmpz_vec_init.argtypes = [S]
+        L._fmpz_vec_init.restype = P
+        L._fmpz_vec_clear.argtypes = [P, S]
+        L._fmpz_vec_clear.restype = None
+        L.fmpz_set_signed_ui_array.argtypes = [P, P, S]
+        L.fmpz_set_signed_ui_array.restype = None
+        L.fmpz_get_signed_ui_array.argtypes = [P, S, P]
+        L.fmpz_get_signed_ui_array.restype = None
+        L._fmpz_poly_mul.argtypes = [P, P, S, P, S]
+        L._fmpz_poly_mul.restype = None
+        L._fmpz_poly_mul_mid_mpn_ctx.argtypes = [P, ctypes.c_ulong, ctypes.c_ulong, P,
+                                                 ctypes.c_ulong, P, ctypes.c_ulong, P]
+        L._fmpz_poly_mul_mid_mpn_ctx.restype = ctypes.c_int
+        L._fmpz_vec_equal.argtypes = [P, P, S]
+        L._fmpz_vec_equal.restype = ctypes.c_int
+        L._fmpz_ready = True
+    return L
+
+
+class RefFmpzVec:
+    """An fmpz vector allocated by the reference library."""
+
+    def __init__(self, n):
+        self.L = _ref_fmpz()
+        self.n = n
+        self.ptr = self.L._fmpz_vec_init(max(n, 1))
+
+    def set_raw(self, raw):
+        raw = np.ascontiguousarray(raw, dtype=np.uint64)
+        w = raw.shape[1]
+        for i in range(self.n):
+            self.L.fmpz_set_signed_ui_array(self.ptr + 8 * i, raw[i].ctypes.data, w)
+        return self
+
+    def get_raw(self, w):
+        out = np.zeros((self.n, w), dtype=np.uint64)
+        for i in range(self.n):
+            self.L.fmpz_get_signed_ui_array(out[i].ctypes.data, w, self.ptr + 8 * i)
+        return out
+
+    def close(self):
+        if self.ptr:
+            self.L._fmpz_vec_clear(self.ptr, max(self.n, 1))
+            self.ptr = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def ref_fmpz_poly_mul_raw(a_raw, b_raw, zw):
+    """The reference's _fmpz_poly_mul (src/fmpz_poly/mul.c:100-186) on raw
+    coefficient rows; returns the (an + bn - 1, zw) raw product."""
+    an, bn = len(a_raw), len(b_raw)
+    if an < bn:
+        a_raw, b_raw, an, bn = b_raw, a_raw, bn, an
+    L = _ref_fmpz()
+    with RefFmpzVec(an) as A, RefFmpzVec(bn) as B, RefFmpzVec(an + bn - 1) as Z:
+        A.set_raw(a_raw)
+        B.set_raw(b_raw)
+        L._fmpz_poly_mul(Z.ptr, A.ptr, an, B.ptr, bn)
+        return Z.get_raw(zw)

@@ -3,7 +3,8 @@
 
 Runs in the development container only (it needs oracle/_ref/libflint_ref.so,
 built from the reference tree by oracle/build_ref.py).  Every case names its
-inputs by generator and seed (oracle.rand_limbs / oracle.rand_below), so the
+inputs by generator and seed (oracle.rand_limbs / oracle.rand_below /
+oracle.rand_fmpz_raw), so the
 fixture stores no input data; outputs are stored in full when short and as a
 blake2b-128 digest otherwise.  The GPU tests recompute the inputs and compare.
 
@@ -83,13 +84,37 @@ NMOD_CASES = [
 ]
 
 
+FMPZ_CASES = [
+    dict(name="fmpz_1x1", an=1, bn=1, bits_a=64, bits_b=64, seed_a=51, seed_b=52),
+    dict(name="fmpz_40x33_signed", an=40, bn=33, bits_a=100, bits_b=20, seed_a=53, seed_b=54),
+    dict(name="fmpz_300x17_wide", an=300, bn=17, bits_a=500, bits_b=9, seed_a=55, seed_b=56),
+    dict(name="fmpz_1000x999_130", an=1000, bn=999, bits_a=130, bits_b=130, seed_a=57, seed_b=58),
+    dict(name="fmpz_2048x100_1000x4096", an=2048, bn=100, bits_a=1000, bits_b=4096, seed_a=59,
+         seed_b=60),
+    dict(name="fmpz_square_777_300", an=777, bn=777, bits_a=300, bits_b=300, seed_a=61,
+         square=True),
+    dict(name="fmpz_window_500x400", an=500, bn=400, bits_a=64, bits_b=64, seed_a=62, seed_b=63,
+         zl=200, zh=700),
+    dict(name="fmpz_2^16x2^16_4096", an=1 << 16, bn=1 << 16, bits_a=4096, bits_b=4096, seed_a=64,
+         seed_b=65, large=True),
+]
+
+
+def fmpz_inputs(case):
+    a = O.rand_fmpz_raw(case["seed_a"], case["an"], case["bits_a"])
+    b = a if case.get("square") else O.rand_fmpz_raw(case["seed_b"], case["bn"], case["bits_b"])
+    zw = O.fmpz_width(case["bits_a"], case["bits_b"], min(case["an"], case["bn"]))
+    zn = case["an"] + case["bn"] - 1
+    return a, b, zw, case.get("zl", 0), case.get("zh", zn)
+
+
 def main():
     if not O.have_ref():
         raise SystemExit("oracle/_ref/libflint_ref.so missing: run python oracle/build_ref.py")
     O.ref().flint_set_num_threads(os.cpu_count() or 1)
     out = {"generator": "oracle.rand_limbs / oracle.rand_below (splitmix64)",
            "source": "reference fft_small (oracle/_ref/libflint_ref.so)",
-           "mpn": [], "nmod": []}
+           "mpn": [], "nmod": [], "fmpz": []}
     for case in MPN_CASES:
         t = time.time()
         a, b = mpn_inputs(case)
@@ -101,6 +126,12 @@ def main():
         n, a, b = nmod_inputs(case)
         z = O.ref_nmod_mul_mid(case["zl"], case["zh"], a, b, n)
         out["nmod"].append(dict(case, modulus="%x" % n, **record(z)))
+        print("%-28s %.2fs" % (case["name"], time.time() - t))
+    for case in FMPZ_CASES:
+        t = time.time()
+        a, b, zw, zl, zh = fmpz_inputs(case)
+        z = O.ref_fmpz_poly_mul_raw(a, b, zw)[zl:zh]
+        out["fmpz"].append(dict(case, zw=zw, **record(z.reshape(-1))))
         print("%-28s %.2fs" % (case["name"], time.time() - t))
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
     with open(path, "w") as f:
