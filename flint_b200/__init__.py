@@ -49,6 +49,21 @@ class MulReq(ctypes.Structure):
                 ("b", ctypes.c_void_p), ("bn", ctypes.c_ulong)]
 
 
+class MulConfig(ctypes.Structure):
+    """gpu_mul_config: route, prime count, log2 transform length, log2 row length."""
+    _fields_ = [("route", ctypes.c_int), ("np", ctypes.c_int), ("logM", ctypes.c_int),
+                ("logC", ctypes.c_int)]
+
+    def key(self):
+        return (self.route, self.np, self.logM, self.logC)
+
+    def __repr__(self):
+        return "MulConfig(route=%d, np=%d, logM=%d, logC=%d)" % self.key()
+
+
+ROUTE_NTT, ROUTE_BASECASE = 0, 1
+
+
 class BatchOptions(ctypes.Structure):
     """gpu_mpn_batch_options: schedule knobs of a batch."""
     _fields_ = [("promote_small", ctypes.c_int), ("max_streams", ctypes.c_int),
@@ -80,6 +95,25 @@ SIGNATURES = {
     "_gpu_fmpz_poly_mul_mid_raw": (ctypes.c_int, [_P, _U, _U, _U, _P, _U, _U, _P, _U, _U, _CTX]),
     "gpu_fmpz_poly_mul_mid_device": (ctypes.c_int, [_CTX, _P, _U, _U, _U, _P, _U, _U, _P, _U,
                                                     _U, _P]),
+    "gpu_mpn_mul_config_resolve": (ctypes.c_int, [_U, _U, ctypes.POINTER(MulConfig)]),
+    "gpu_mpn_mul_device_config": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U,
+                                                 ctypes.POINTER(MulConfig), _P]),
+    "gpu_fmpz_poly_mul_config_resolve": (ctypes.c_int, [_U, _U, _U, _U, ctypes.POINTER(MulConfig)]),
+    "gpu_fmpz_poly_mul_mid_device_config": (ctypes.c_int, [_CTX, _P, _U, _U, _U, _P, _U, _U, _P, _U,
+                                                           _U, ctypes.POINTER(MulConfig), _P]),
+    "gpu_mul_time_config": (ctypes.c_int, [_CTX, ctypes.c_int, _U, _U, _U, _U,
+                                           ctypes.POINTER(MulConfig), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)]),
+    "gpu_mlp_init": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.c_ulonglong]),
+    "gpu_mlp_nparams": (ctypes.c_int, [_P]),
+    "gpu_mlp_get_params": (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
+    "gpu_mlp_set_params": (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
+    "gpu_mlp_predict": (ctypes.c_int, [_P, _P, ctypes.c_int, _P]),
+    "gpu_mlp_predict_device": (ctypes.c_int, [_P, _P, ctypes.c_int, _P, _P]),
+    "gpu_mlp_gradient": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, _P, _P]),
+    "gpu_mlp_train": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_float, ctypes.c_ulonglong, _P]),
+    "gpu_mlp_clear": (None, [_P]),
     "gpu_mpn_batch_init": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, ctypes.c_size_t, _P]),
     "gpu_mpn_batch_run": (ctypes.c_int, [_P, _P]),
     "gpu_mpn_batch_check": (ctypes.c_int, [_P, _P]),
@@ -137,6 +171,71 @@ def mpn_mul_plan(an, bn):
 
 def prime(i):
     return int(lib().gpu_fft_small_prime(i))
+
+
+def resolve_config(kind, an, bn, cfg=None, aw=1, bw=1):
+    """The full configuration (defaults filled in) for a product, or raises
+    GpuFftSmallError if cfg is invalid for it."""
+    c = MulConfig(*(cfg.key() if cfg is not None else (0, 0, 0, 0)))
+    if kind == 0:
+        _check(lib().gpu_mpn_mul_config_resolve(an, bn, ctypes.byref(c)))
+    else:
+        _check(lib().gpu_fmpz_poly_mul_config_resolve(an, aw, bn, bw, ctypes.byref(c)))
+    return c
+
+
+class Mlp:
+    """The cost model's network (gpu_mlp_*): n_in -> 3 x 64 ReLU -> 1, fp32,
+    trained and evaluated by the library's CUDA kernels."""
+
+    def __init__(self, n_in, seed=1):
+        self.n_in = n_in
+        self._h = ctypes.c_void_p()
+        _check(lib().gpu_mlp_init(ctypes.byref(self._h), n_in, seed))
+        self.nparams = int(lib().gpu_mlp_nparams(self._h))
+
+    def params(self):
+        p = np.empty(self.nparams, dtype=np.float32)
+        _check(lib().gpu_mlp_get_params(self._h, p.ctypes.data, self.nparams))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        _check(lib().gpu_mlp_set_params(self._h, p.ctypes.data, len(p)))
+
+    def predict(self, X):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        y = np.empty(len(X), dtype=np.float32)
+        _check(lib().gpu_mlp_predict(self._h, X.ctypes.data, len(X), y.ctypes.data))
+        return y
+
+    def gradient(self, X, t):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        g = np.empty(self.nparams, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().gpu_mlp_gradient(self._h, X.ctypes.data, t.ctypes.data, len(X), g.ctypes.data,
+                                      ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, X, t, epochs=200, batch=256, lr=1e-3, seed=7):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        t = np.ascontiguousarray(t, dtype=np.float32)
+        loss = ctypes.c_float()
+        _check(lib().gpu_mlp_train(self._h, X.ctypes.data, t.ctypes.data, len(X), epochs, batch, lr,
+                                   seed, ctypes.byref(loss)))
+        return loss.value
+
+    def close(self):
+        if self._h:
+            lib().gpu_mlp_clear(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _raw_bits(x):
@@ -241,6 +340,25 @@ class MpnCtx:
         """Queue the raw-form window product on device pointers."""
         _check(lib().gpu_fmpz_poly_mul_mid_device(self.ptr, z_ptr, zw, zl, zh, a_ptr, aw, an,
                                                   b_ptr, bw, bn, stream))
+
+    def mpn_mul_device_config(self, z_ptr, a_ptr, an, b_ptr, bn, cfg, stream=None):
+        """mpn_mul_device under an explicit MulConfig."""
+        _check(lib().gpu_mpn_mul_device_config(self.ptr, z_ptr, a_ptr, an, b_ptr, bn,
+                                               ctypes.byref(cfg), stream))
+
+    def fmpz_poly_mul_device_config(self, z_ptr, zw, zl, zh, a_ptr, aw, an, b_ptr, bw, bn, cfg,
+                                    stream=None):
+        _check(lib().gpu_fmpz_poly_mul_mid_device_config(self.ptr, z_ptr, zw, zl, zh, a_ptr, aw,
+                                                         an, b_ptr, bw, bn, ctypes.byref(cfg),
+                                                         stream))
+
+    def time_config(self, kind, an, bn, cfg=None, aw=1, bw=1, reps=3):
+        """Median device milliseconds of a product under cfg (autotuner probe)."""
+        ms = ctypes.c_double()
+        _check(lib().gpu_mul_time_config(self.ptr, kind, an, aw, bn, bw,
+                                         ctypes.byref(cfg) if cfg is not None else None, reps,
+                                         ctypes.byref(ms)))
+        return ms.value
 
     @property
     def last_launches(self):

@@ -7,6 +7,8 @@
 #include "mpn_kernels.cuh"
 #include "nmod_kernels.cuh"
 #include "fmpz_kernels.cuh"
+#include "basecase_kernels.cuh"
+#include "mlp_kernels.cuh"
 
 #include <cuda_runtime.h>
 #include <math.h>
@@ -340,10 +342,20 @@ struct LaunchShape {
     size_t row_smem;
 };
 
-static LaunchShape make_shape(int logM)
+// Four-step split of a 2^logM transform: rows of 2^logC, columns of
+// 2^(logM - logC); logC < 0 takes the longest rows (2^14), which leaves the
+// shortest columns.
+constexpr int LOG_MAXR = 11;
+static int default_logC(int logM) { return std::min(logM, LOG_MAXC); }
+static bool valid_logC(int logM, int logC)
+{
+    return logC >= std::max(MIN_LOGM, logM - LOG_MAXR) && logC <= std::min(logM, LOG_MAXC);
+}
+
+static LaunchShape make_shape(int logM, int logC = -1)
 {
     LaunchShape L;
-    L.S.logC = std::min(logM, LOG_MAXC);
+    L.S.logC = logC < 0 ? default_logC(logM) : logC;
     L.S.logR = logM - L.S.logC;
     const int R = 1 << L.S.logR, C = 1 << L.S.logC;
     if (L.S.logR >= 5) {
@@ -490,6 +502,7 @@ struct MulPlan {
     int np;
     int logM;
     LaunchShape L;
+    int route;   // GPU_MUL_ROUTE_*
 };
 
 static int ceil_log2_u64(uint64_t x)
@@ -497,6 +510,44 @@ static int ceil_log2_u64(uint64_t x)
     int l = 0;
     while (((uint64_t)1 << l) < x) l++;
     return l;
+}
+
+// Plan under an explicit configuration (zero fields take the defaults of
+// plan_mpn); every choice is checked against the exactness bound and the
+// kernels' shape limits.
+static int plan_mpn(uint64_t an, uint64_t bn, MulPlan *P);
+static int plan_mpn_cfg(uint64_t an, uint64_t bn, const gpu_mul_config *cfg, MulPlan *P)
+{
+    int rc = plan_mpn(an, bn, P);
+    if (rc || !cfg) return rc;
+    if (cfg->route == GPU_MUL_ROUTE_BASECASE) {
+        if (std::min(an, bn) > (uint64_t)BASECASE_MAX)
+            return set_error(GPU_FFT_SMALL_EINVAL, "basecase route needs an operand of at most %d limbs",
+                             BASECASE_MAX);
+        if (cfg->np || cfg->logM || cfg->logC)
+            return set_error(GPU_FFT_SMALL_EINVAL, "basecase route takes no transform parameters");
+        P->route = GPU_MUL_ROUTE_BASECASE;
+        P->np = 0;
+        P->logM = std::max(ceil_log2_u64(an + bn - 1), MIN_LOGM);
+        return 0;
+    }
+    if (cfg->route != GPU_MUL_ROUTE_NTT) return set_error(GPU_FFT_SMALL_EINVAL, "unknown route %d", cfg->route);
+    if (cfg->np) {
+        if (cfg->np < P->np || cfg->np > 6)
+            return set_error(GPU_FFT_SMALL_EINVAL, "prime count %d outside [%d, 6]", cfg->np, P->np);
+        P->np = cfg->np;
+    }
+    if (cfg->logM) {
+        if (cfg->logM < P->logM || cfg->logM > LOG_MAXM)
+            return set_error(GPU_FFT_SMALL_EINVAL, "transform length 2^%d outside [2^%d, 2^%d]", cfg->logM,
+                             P->logM, LOG_MAXM);
+        P->logM = cfg->logM;
+    }
+    const int logC = cfg->logC ? cfg->logC : default_logC(P->logM);
+    if (!valid_logC(P->logM, logC))
+        return set_error(GPU_FFT_SMALL_EINVAL, "row length 2^%d invalid for a 2^%d transform", logC, P->logM);
+    P->L = make_shape(P->logM, logC);
+    return 0;
 }
 
 static int plan_mpn(uint64_t an, uint64_t bn, MulPlan *P)
@@ -519,6 +570,7 @@ static int plan_mpn(uint64_t an, uint64_t bn, MulPlan *P)
     P->np = np;
     P->logM = logM;
     P->L = make_shape(logM);
+    P->route = GPU_MUL_ROUTE_NTT;
     return 0;
 }
 
@@ -563,20 +615,20 @@ static int upload_scales(Ctx *X)
 }
 
 // Resident row CTAs per SM for a shape: 1 for long rows (512 threads, ~135 KB
-// of shared memory), several for short ones.  The row shape depends on logC
-// alone (rows shorter than 2^14 only occur with R = 1, one row per item).
+// of shared memory), several for short ones.  The row launch depends on the
+// row length and the rows per item.
 static int rows_per_sm(const LaunchShape &L)
 {
-    static int occ[LOG_MAXC + 1] = {0};
-    const int c = L.S.logC;
-    if (occ[c] == 0) {
+    static int occ[LOG_MAXC + 1][LOG_MAXC + 1] = {{0}};
+    const int c = L.S.logC, v = __builtin_ctz((unsigned)L.nv);
+    if (occ[c][v] == 0) {
         int n = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ROWS[c], L.row_threads, L.row_smem) !=
                 cudaSuccess || n < 1)
             n = 1;
-        occ[c] = n;
+        occ[c][v] = n;
     }
-    return occ[c];
+    return occ[c][v];
 }
 
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
@@ -600,13 +652,52 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     timing_mark(tr, 3, st);
 }
 
-// Enqueue z = a * b on `st` with device pointers.
+// Schoolbook route: column sums, then the carry kernel's direct mode.
+static int mpn_mul_basecase_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
+                                    const uint64_t *b, uint64_t bn, int logM, cudaStream_t st)
+{
+    const uint64_t *x = a, *y = b;
+    uint64_t xn = an, yn = bn;
+    if (yn > xn) { std::swap(x, y); std::swap(xn, yn); }
+    const uint64_t L = an + bn - 1, zn = an + bn;
+    const size_t plane = (size_t)1 << logM;
+    int rc = grow((void **)&X->d_res, &X->res_cap, 3 * plane * sizeof(uint64_t));
+    if (rc) return rc;
+    uint64_t *sums = (uint64_t *)X->d_res;
+    constexpr int THREADS = 256, TILE = 4 * THREADS;
+    const size_t tiles = (zn + TILE - 1) / TILE;
+    rc = ensure_status(X, tiles);
+    if (rc) return rc;
+    X->epoch = (X->epoch + 1) & 0x0fffffffu;
+    if (X->epoch == 0) {
+        CU(cudaMemsetAsync(X->d_status, 0, X->status_cap * sizeof(uint32_t), st));
+        X->epoch = 1;
+    }
+    TimingRecord *tr = timing_begin(X, st);
+    k_basecase_sums<<<(unsigned)((L + BASECASE_THREADS - 1) / BASECASE_THREADS), BASECASE_THREADS, 0, st>>>(
+        x, xn, y, (uint32_t)yn, sums, plane);
+    timing_mark(tr, 1, st);
+    timing_mark(tr, 2, st);
+    timing_mark(tr, 3, st);
+    k_crt_carry<0, THREADS><<<tiles, THREADS, 0, st>>>((const uint32_t *)sums, logM, L, zn, z, X->crt[5],
+                                                       X->d_status, X->d_ticket, X->ticket_base, X->epoch,
+                                                       X->d_err, nullptr, nullptr);
+    timing_mark(tr, 4, st);
+    X->ticket_base += tiles;
+    X->last_launches = 2;
+    CU(cudaGetLastError());
+    return 0;
+}
+
+// Enqueue z = a * b on `st` with device pointers (cfg NULL: default plan).
 static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
-                           const uint64_t *b, uint64_t bn, cudaStream_t st)
+                           const uint64_t *b, uint64_t bn, cudaStream_t st,
+                           const gpu_mul_config *cfg = nullptr)
 {
     MulPlan P;
-    int rc = plan_mpn(an, bn, &P);
+    int rc = plan_mpn_cfg(an, bn, cfg, &P);
     if (rc) return rc;
+    if (P.route == GPU_MUL_ROUTE_BASECASE) return mpn_mul_basecase_enqueue(X, z, a, an, b, bn, P.logM, st);
     const bool sq = (a == b) && (an == bn);
     const int np = P.np, logM = P.logM;
     const size_t M = (size_t)1 << logM;
@@ -713,6 +804,10 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 #include "fmpz_host.inc"
 
 // ---------------------------------------------------------------------------
+// cost model of the learned schedule
+#include "mlp_host.inc"
+
+// ---------------------------------------------------------------------------
 // C ABI
 extern "C" {
 
@@ -768,6 +863,31 @@ int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev, 
     if (rc) return rc;
     // NULL is CUDA's default stream, as everywhere in the runtime API
     return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn, (cudaStream_t)stream);
+}
+
+int gpu_mpn_mul_config_resolve(gpu_ulong an, gpu_ulong bn, gpu_mul_config *cfg)
+{
+    if (!cfg) return set_error(GPU_FFT_SMALL_EINVAL, "null configuration");
+    MulPlan P;
+    int rc = plan_mpn_cfg(an, bn, cfg, &P);
+    if (rc) return rc;
+    if (P.route == GPU_MUL_ROUTE_NTT) {
+        cfg->np = P.np;
+        cfg->logM = P.logM;
+        cfg->logC = P.L.S.logC;
+    }
+    return 0;
+}
+
+int gpu_mpn_mul_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong an,
+                              const uint64_t *b_dev, gpu_ulong bn, const gpu_mul_config *cfg,
+                              void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn, (cudaStream_t)stream, cfg);
 }
 
 int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
@@ -843,6 +963,96 @@ int gpu_fmpz_poly_mul_mid_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zw,
         zh = zn;
     }
     return fmpz_mul_mid_enqueue(X, z_dev, zw, zl, zh, a_dev, aw, an, b_dev, bw, bn, st);
+}
+
+int gpu_fmpz_poly_mul_config_resolve(gpu_ulong an, gpu_ulong aw, gpu_ulong bn, gpu_ulong bw,
+                                     gpu_mul_config *cfg)
+{
+    if (!cfg) return set_error(GPU_FFT_SMALL_EINVAL, "null configuration");
+    FmpzPlan P;
+    int rc = plan_fmpz_cfg(an, aw, bn, bw, cfg, &P);
+    if (rc) return rc;
+    cfg->np = P.np;
+    cfg->logM = P.logM;
+    cfg->logC = P.L.S.logC;
+    return 0;
+}
+
+int gpu_fmpz_poly_mul_mid_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zw, gpu_ulong zl,
+                                        gpu_ulong zh, const uint64_t *a_dev, gpu_ulong aw, gpu_ulong an,
+                                        const uint64_t *b_dev, gpu_ulong bw, gpu_ulong bn,
+                                        const gpu_mul_config *cfg, void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = fmpz_check_args(zw, aw, an, bw, bn);
+    if (rc) return rc;
+    if (zl >= zh || zh > an + bn - 1)
+        return set_error(GPU_FFT_SMALL_EINVAL, "window must lie inside the product");
+    rc = bind_device(X);
+    if (rc) return rc;
+    return fmpz_mul_mid_enqueue(X, z_dev, zw, zl, zh, a_dev, aw, an, b_dev, bw, bn, (cudaStream_t)stream,
+                                cfg);
+}
+
+// device-side operand filler for the timing entry point (splitmix64)
+__global__ void k_fill_limbs(uint64_t *p, uint64_t n, uint64_t seed)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + (i + 1) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        p[i] = (z ^ (z >> 31)) | (i + 1 == n ? 1ull : 0ull);
+    }
+}
+
+int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw, gpu_ulong bn, gpu_ulong bw,
+                        const gpu_mul_config *cfg, int reps, double *ms)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (reps < 1 || !ms || (kind != 0 && kind != 1)) return set_error(GPU_FFT_SMALL_EINVAL, "bad timing request");
+    if (kind == 0) aw = bw = 1;
+    int rc = bind_device(X);
+    if (rc) return rc;
+    // validate the configuration before allocating
+    gpu_mul_config c = cfg ? *cfg : gpu_mul_config{0, 0, 0, 0};
+    rc = kind == 0 ? gpu_mpn_mul_config_resolve(an, bn, &c) : gpu_fmpz_poly_mul_config_resolve(an, aw, bn, bw, &c);
+    if (rc) return rc;
+    const uint64_t zn = an + bn, zw = kind == 0 ? 1 : aw + bw + 1;
+    const size_t na = an * aw, nb = bn * bw, nz = zn * zw;
+    uint64_t *buf = nullptr;
+    CU(cudaMalloc(&buf, (na + nb + nz) * sizeof(uint64_t)));
+    uint64_t *da = buf, *db = buf + na, *dz = buf + na + nb;
+    cudaStream_t st = X->stream;
+    k_fill_limbs<<<X->nsm * 4, 256, 0, st>>>(da, na, 0x1234567ull + an);
+    k_fill_limbs<<<X->nsm * 4, 256, 0, st>>>(db, nb, 0x7654321ull + bn);
+    auto call = [&]() -> int {
+        return kind == 0 ? mpn_mul_enqueue(X, dz, da, an, db, bn, st, cfg)
+                         : fmpz_mul_mid_enqueue(X, dz, zw, 0, an + bn - 1, da, aw, an, db, bw, bn, st, cfg);
+    };
+    std::vector<float> t(reps);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    rc = call();   // warm-up (allocations, first launch)
+    if (!rc && cudaEventCreate(&e0) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
+    if (!rc && cudaEventCreate(&e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
+    for (int r = 0; r < reps && !rc; r++) {
+        cudaEventRecord(e0, st);
+        rc = call();
+        cudaEventRecord(e1, st);
+        if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "timing sync");
+        if (!rc) cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    if (!rc) rc = check_device_error(X);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (rc) return rc;
+    std::sort(t.begin(), t.end());
+    *ms = t[reps / 2];
+    return 0;
 }
 
 int _gpu_fmpz_poly_mul_mid_mpn_ctx(gpu_slong *z, gpu_ulong zl, gpu_ulong zh, const gpu_slong *a,

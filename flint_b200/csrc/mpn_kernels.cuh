@@ -504,10 +504,17 @@ template <int NP>
 __device__ __forceinline__ void crt_coeff(const uint32_t* __restrict__ res, int logM, uint64_t n,
                                           const CrtConst& K, uint64_t& c0, uint64_t& c1, uint64_t& c2)
 {
-    uint32_t y[NP];
+    if constexpr (NP == 0) {
+        // direct values: three word planes of L words each (L = 2^logM here)
+        const uint64_t* v = reinterpret_cast<const uint64_t*>(res);
+        const size_t L = (size_t)1 << logM;
+        c0 = v[n]; c1 = v[L + n]; c2 = v[2 * L + n];
+    } else {
+        uint32_t y[NP];
 #pragma unroll
-    for (int jp = 0; jp < NP; jp++) y[jp] = res[((size_t)jp << logM) + n];
-    crt_values<NP>(y, K, c0, c1, c2);
+        for (int jp = 0; jp < NP; jp++) y[jp] = res[((size_t)jp << logM) + n];
+        crt_values<NP>(y, K, c0, c1, c2);
+    }
 }
 
 // A[0..5] += y * (c0, c1, c2, c3): one PTX carry chain per partial-product row
@@ -670,6 +677,8 @@ __device__ __forceinline__ void crt_values(const uint32_t (&y)[NP], const CrtCon
 constexpr uint32_t ST_AGG = 1u << 2, ST_INC = 2u << 2;
 constexpr long LOOKBACK_SPIN_LIMIT = 1L << 22;
 
+// NP == 0 is the direct mode: the coefficient values are precomputed (the
+// basecase kernel's column sums) instead of recombined from residues.
 template <int NP, int THREADS>
 __global__ void __launch_bounds__(THREADS)
 k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
@@ -705,7 +714,18 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
 
     // coefficients n0-3 .. n0+TILE-1 into shared memory; a thread's four
     // residues per prime are one 16-byte load when they lie inside the array
-    {
+    if constexpr (NP == 0) {
+        // direct mode: the coefficient values are given as three planes of
+        // 2^logM 64-bit words (low, middle, high word of each coefficient)
+#pragma unroll
+        for (int q = 0; q < PER; q++) {
+            const int idx = threadIdx.x * PER + q;
+            const uint64_t n = (uint64_t)(n0 + idx);
+            uint64_t c0 = 0, c1 = 0, c2 = 0;
+            if (n < L) crt_coeff<0>(res, logM, n, K, c0, c1, c2);
+            X0[idx + 3] = c0; X1[idx + 3] = c1; X2[idx + 3] = c2;
+        }
+    } else {
         const uint64_t nb = (uint64_t)(n0 + threadIdx.x * PER);
         uint32_t y[PER][NP];
         if (nb + PER <= ((uint64_t)1 << logM)) {

@@ -45,3 +45,25 @@ def batch_operands(seed, sizes):
         spans.append((off, an, off + an, bn))
         off += an + bn
     return buf, spans
+
+
+def request_stream(seed, n, mpn_log=(6.0, 22.0), mpn_ratio_log=(0.0, 6.0), fmpz_len_log=(8.0, 16.0),
+                   fmpz_bits=(64, 4096)):
+    """n requests (kind, an, bn, aw, bw), half mpn products (an log-uniform
+    in 2^mpn_log, ratio an/bn log-uniform in 2^mpn_ratio_log) and half integer
+    polynomial products (lengths log-uniform in 2^fmpz_len_log, one coefficient
+    bit size per request uniform in fmpz_bits, aw = bw = ceil((bits + 1) / 64))."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        if rng.random() < 0.5:
+            an = int(round(2.0 ** rng.uniform(*mpn_log)))
+            bn = max(1, int(round(an / 2.0 ** rng.uniform(*mpn_ratio_log))))
+            out.append((0, an, bn, 1, 1))
+        else:
+            an = int(round(2.0 ** rng.uniform(*fmpz_len_log)))
+            bn = int(round(2.0 ** rng.uniform(*fmpz_len_log)))
+            bits = int(rng.integers(fmpz_bits[0], fmpz_bits[1] + 1))
+            w = (bits + 1 + 63) // 64
+            out.append((1, an, bn, w, w))
+    return out

@@ -154,6 +154,84 @@ GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gp
                                             const gpu_ulong *b, gpu_slong bn,
                                             gpu_nmod_t mod);
 
+/* --- explicit schedules (no counterpart in the reference; its counterpart
+       is the profile choice of mpn_ctx_best_profile, src/fft_small/mpn_mul.c:
+       1248-1340, which is internal) --------------------------------------- */
+
+#define GPU_MUL_ROUTE_NTT       0   /* number-theoretic transform */
+#define GPU_MUL_ROUTE_BASECASE  1   /* schoolbook; shorter operand <= 1024 limbs */
+
+/* How one product is computed.  Zero fields take the default: the fewest
+   primes that hold the coefficient bound, the shortest transform that holds
+   the product, rows of min(2^logM, 2^14).  Any valid choice gives the same
+   (exact) product; only the time differs. */
+typedef struct {
+    int route;   /* GPU_MUL_ROUTE_* */
+    int np;      /* primes, minimal .. 6 */
+    int logM;    /* transform length 2^logM, minimal .. 2^25 */
+    int logC;    /* four-step row length 2^logC, max(5, logM - 11) .. min(logM, 14) */
+} gpu_mul_config;
+
+/* Fills the zero fields of cfg with the defaults for an an x bn product and
+   checks the rest; returns 0 or GPU_FFT_SMALL_EINVAL naming the bad field. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_config_resolve(gpu_ulong an, gpu_ulong bn, gpu_mul_config *cfg);
+/* gpu_mpn_mul_device under an explicit configuration (NULL = default). */
+GPU_FFT_SMALL_API int gpu_mpn_mul_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev,
+                                                gpu_ulong an, const uint64_t *b_dev, gpu_ulong bn,
+                                                const gpu_mul_config *cfg, void *stream);
+
+/* Integer-polynomial counterparts (raw coefficient rows, transform route;
+   the window must lie inside the product). */
+GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_config_resolve(gpu_ulong an, gpu_ulong aw, gpu_ulong bn,
+                                                       gpu_ulong bw, gpu_mul_config *cfg);
+GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zw,
+                                                          gpu_ulong zl, gpu_ulong zh,
+                                                          const uint64_t *a_dev, gpu_ulong aw,
+                                                          gpu_ulong an, const uint64_t *b_dev,
+                                                          gpu_ulong bw, gpu_ulong bn,
+                                                          const gpu_mul_config *cfg, void *stream);
+
+/* Autotuner measurement: median device time (CUDA events on the context's
+   stream, after one warm-up call) of `reps` products under cfg, on operands
+   filled on the device from a fixed seed.  kind 0: an x bn-limb mpn product
+   (aw, bw ignored); kind 1: integer polynomials of an and bn coefficients of
+   aw and bw limbs (full product).  Returns 0 and *ms, or an error code. */
+GPU_FFT_SMALL_API int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw,
+                                          gpu_ulong bn, gpu_ulong bw, const gpu_mul_config *cfg,
+                                          int reps, double *ms);
+
+/* --- cost model of the learned schedule (no counterpart in the reference) --
+
+   A fully connected network n_in -> 64 -> 64 -> 64 -> 1 (ReLU, fp32) that
+   predicts log device time from request features and a candidate
+   gpu_mul_config; trained and evaluated by the library's own CUDA kernels on
+   the current device.  Host-pointer arguments unless named _dev.  The
+   parameter vector is W1[n_in][64], b1[64], W2[64][64], b2[64], W3[64][64],
+   b3[64], W4[64], b4. */
+typedef struct gpu_mlp_struct *gpu_mlp_t;
+
+/* He-uniform weights from a splitmix64 stream seeded with `seed`, zero
+   biases; 1 <= n_in <= 32. */
+GPU_FFT_SMALL_API int gpu_mlp_init(gpu_mlp_t *M, int n_in, unsigned long long seed);
+GPU_FFT_SMALL_API int gpu_mlp_nparams(gpu_mlp_t M);
+GPU_FFT_SMALL_API int gpu_mlp_get_params(gpu_mlp_t M, float *params, size_t n);
+/* Replaces the parameters and resets the optimiser state. */
+GPU_FFT_SMALL_API int gpu_mlp_set_params(gpu_mlp_t M, const float *params, size_t n);
+/* y[s] = network(X[s][0 .. n_in)) for s < n. */
+GPU_FFT_SMALL_API int gpu_mlp_predict(gpu_mlp_t M, const float *X, int n, float *y);
+GPU_FFT_SMALL_API int gpu_mlp_predict_device(gpu_mlp_t M, const float *X_dev, int n, float *y_dev,
+                                             void *stream);
+/* Gradient of the mean squared error (1/n) sum (y_s - t_s)^2 with respect to
+   the parameters (deterministic summation order), and the loss. */
+GPU_FFT_SMALL_API int gpu_mlp_gradient(gpu_mlp_t M, const float *X, const float *t, int n,
+                                       float *grad, float *loss);
+/* Adam (lr, 0.9, 0.999, 1e-8) on minibatches of `batch` samples, reshuffled
+   every epoch from a splitmix64 stream seeded with `seed`; final_loss (may be
+   NULL) receives the full-batch loss after training. */
+GPU_FFT_SMALL_API int gpu_mlp_train(gpu_mlp_t M, const float *X, const float *t, int n, int epochs,
+                                    int batch, float lr, unsigned long long seed, float *final_loss);
+GPU_FFT_SMALL_API void gpu_mlp_clear(gpu_mlp_t M);
+
 /* --- integer polynomials ---------------------------------------------------
 
    Coefficients [zl, zh) of the product of integer polynomials a (an

@@ -137,3 +137,24 @@ def test_python_fmpz_vs_compiled_reference(seed):
     zw = O.fmpz_width(ba, bb, min(an, bn))
     want = O.raw_to_ints(O.ref_fmpz_poly_mul_raw(a, b, zw))
     assert O.fmpz_poly_mul_python(O.raw_to_ints(a), O.raw_to_ints(b)) == want
+
+
+# ---------------------------------------------------------------- cost model network
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """Pins the NumPy network (the checker of the CUDA kernels) by central
+    differences of its own loss in float64."""
+    from oracle import mlp_ref
+    rng = np.random.default_rng(3)
+    n_in, n = 16, 40
+    P = rng.normal(0, 0.3, mlp_ref.offsets(n_in)["total"])
+    X = rng.normal(0, 1, (n, n_in))
+    t = rng.normal(0, 1, n)
+    g = mlp_ref.gradient(P, X, t)
+    idx = rng.choice(len(P), 60, replace=False)
+    h = 1e-6
+    for k in idx:
+        Pp, Pm = P.copy(), P.copy()
+        Pp[k] += h
+        Pm[k] -= h
+        fd = (mlp_ref.loss(Pp, X, t) - mlp_ref.loss(Pm, X, t)) / (2 * h)
+        assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(fd), (k, fd, g[k])

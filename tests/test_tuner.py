@@ -1,0 +1,61 @@
+"""Host logic of the autotuner and the learned schedule (no GPU needed):
+candidate enumeration, configuration validation, feature encoding and the
+request-stream generator."""
+import math
+
+import numpy as np
+import pytest
+
+import flint_b200 as FB
+from flint_b200 import tuner
+from flint_b200.workload import request_stream
+
+
+REQS = [(0, 1, 1), (0, 64, 64), (0, 1000, 3), (0, 1 << 20, 1 << 14), (0, 1 << 22, 1 << 22),
+        (1, 256, 300, 2, 2), (1, 1 << 16, 1 << 16, 65, 65), (1, 5000, 40, 10, 3)]
+
+
+@pytest.mark.parametrize("r", REQS)
+def test_candidates_are_valid_and_include_default(r):
+    cs = tuner.candidates(r)
+    keys = [c.key() for c in cs]
+    assert len(set(keys)) == len(keys)
+    assert tuner.default_config(r).key() in keys
+    kind, an, bn = r[:3]
+    has_bc = any(c.route == FB.ROUTE_BASECASE for c in cs)
+    assert has_bc == (kind == 0 and min(an, bn) <= tuner.BASECASE_MAX)
+    for c in cs:
+        if c.route == FB.ROUTE_NTT:
+            assert max(5, c.logM - 11) <= c.logC <= min(c.logM, 14)
+        f = tuner.features(r, c)
+        assert f.shape == (tuner.N_FEATURES,) and np.isfinite(f).all()
+
+
+def test_invalid_configs_are_rejected():
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.resolve_config(0, 5000, 5000, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0))   # > 1024
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.resolve_config(0, 100, 100, FB.MulConfig(FB.ROUTE_NTT, 4, 0, 0))          # too few primes
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.resolve_config(0, 100, 100, FB.MulConfig(FB.ROUTE_NTT, 0, 7, 0))          # too short
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.resolve_config(0, 1 << 20, 1, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 8))        # rows too short
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.resolve_config(1, 10, 10, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0), 2, 2)
+    c = FB.resolve_config(0, 1 << 20, 1 << 20)
+    assert c.key() == (FB.ROUTE_NTT, 5, 21, 14)
+
+
+def test_request_stream_shape():
+    rs = request_stream(11, 4000)
+    mpn = [r for r in rs if r[0] == 0]
+    fz = [r for r in rs if r[0] == 1]
+    assert abs(len(mpn) - len(fz)) < 300
+    la = np.log2([r[1] for r in mpn])
+    assert 6 - 1e-9 <= la.min() and la.max() <= 22 + 1e-9
+    # bn = round(an / 2^V) >= 1: rounding moves the ratio by at most a factor 1.5
+    ratios = np.log2([r[1] / r[2] for r in mpn])
+    assert ratios.min() >= -0.6 and ratios.max() <= 6.6
+    ws = [r[3] for r in fz]
+    assert min(ws) >= 2 and max(ws) <= 65
+    assert all(2 ** 8 - 1 <= r[1] <= 2 ** 16 + 1 and 2 ** 8 - 1 <= r[2] <= 2 ** 16 + 1 for r in fz)
