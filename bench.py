@@ -217,10 +217,34 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds):
     bits = NS_LIMB_BITS * total
     k_plain = max(2, steps // 3)
     ms_plain = time_on_stream(torch, stream, per_instance, k_plain, 3)
-    B = FB.MpnBatch(ctx, reqs)
+    B0 = FB.MpnBatch(ctx, reqs)
+    ms_default = time_on_stream(torch, stream, lambda: B0.run(s), steps, warmup)
+    B0.check(s)
+    exact_default = bool(torch.equal(d_out, d_ref))
+    B0.close()
+    # learned schedule: autotuner timings (batched marginal cost) of a training
+    # sample from the same distribution, the cost model trained on them by the
+    # library's CUDA kernels, then one configuration per request of the batch
+    from flint_b200 import tuner
+    t0 = time.perf_counter()
+    train = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 1, 160)]
+    tun = tuner.Autotuner(ctx, reps=3, batched=True)
+    X, tt = tuner.dataset(tun, train)
+    t_tune = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    model = tuner.CostModel(seed=11)
+    fit_loss = model.fit(X, tt, epochs=400)
+    t_fit = time.perf_counter() - t0
+    held = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 2, 48)]
+    reg = tuner.regret(tun, held, model.choose(held))
+    t0 = time.perf_counter()
+    configs = model.choose([(0, a, b) for a, b in sizes])
+    t_choose = time.perf_counter() - t0
+    B = FB.MpnBatch(ctx, reqs, configs=configs)
+    d_out.fill_(0)
     ms_batch = time_on_stream(torch, stream, lambda: B.run(s), steps, warmup)
     B.check(s)
-    exact = bool(torch.equal(d_out, d_ref))
+    exact = bool(torch.equal(d_out, d_ref)) and exact_default
     # residue fingerprints of a subsample (Python integers)
     out = d_out.cpu().numpy().view(np.uint64)
     q = 2305843009213693951
@@ -247,10 +271,20 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds):
         "workload": "%d uneven products, an = round(2^U), U~U[10,18], bn = max(1, round(an/2^V)), "
                     "V~U[0,4], seed %d" % (BATCH_N, BATCH_SEED),
         "limbs": total, "classes": B.classes, "launches_per_step": B.launches,
+        "schedule": "learned (cost model per request, batched by configuration)",
         "value": bits / ms_batch / 1e6, "unit": "Gbit/s", "ms_per_step": ms_batch,
         "per_instance": {"value": bits / ms_plain / 1e6, "ms_per_step": ms_plain,
                          "launches_per_step": 4 * BATCH_N},
+        "plain_batched": {"value": bits / ms_default / 1e6, "ms_per_step": ms_default,
+                          "schedule": "default configuration for every request"},
         "speedup_vs_per_instance": ms_plain / ms_batch,
+        "speedup_vs_plain_batched": ms_default / ms_batch,
+        "learned": {"train_requests": len(train), "train_rows": int(len(X)),
+                    "tuning_s": t_tune, "fit_s": t_fit, "fit_mse_log_ms": fit_loss,
+                    "choose_s_4096": t_choose,
+                    "routes": {"transform": sum(c.route == 0 for c in configs),
+                               "basecase": sum(c.route == 1 for c in configs)},
+                    "held_out_regret_vs_exhaustive": reg},
         "e2e": {"value": bits / ms_e2e / 1e6, "unit": "Gbit/s", "ms_per_step": ms_e2e,
                 "h2d_bytes_per_step": 8 * total, "d2h_bytes_per_step": 8 * total},
         "exact_vs_per_instance": exact, "fingerprints_ok": bool(fp_ok), "e2e_matches": e2e_ok,

@@ -104,6 +104,8 @@ SIGNATURES = {
     "gpu_mul_time_config": (ctypes.c_int, [_CTX, ctypes.c_int, _U, _U, _U, _U,
                                            ctypes.POINTER(MulConfig), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double)]),
+    "gpu_mpn_mul_time_batched": (ctypes.c_int, [_CTX, _U, _U, ctypes.POINTER(MulConfig), ctypes.c_int,
+                                                ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "gpu_mlp_init": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.c_ulonglong]),
     "gpu_mlp_nparams": (ctypes.c_int, [_P]),
     "gpu_mlp_get_params": (ctypes.c_int, [_P, _P, ctypes.c_size_t]),
@@ -115,6 +117,8 @@ SIGNATURES = {
                                      ctypes.c_float, ctypes.c_ulonglong, _P]),
     "gpu_mlp_clear": (None, [_P]),
     "gpu_mpn_batch_init": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, ctypes.c_size_t, _P]),
+    "gpu_mpn_batch_init_config": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, _P, ctypes.c_size_t,
+                                                 _P]),
     "gpu_mpn_batch_run": (ctypes.c_int, [_P, _P]),
     "gpu_mpn_batch_check": (ctypes.c_int, [_P, _P]),
     "gpu_mpn_batch_launches": (ctypes.c_int, [_P]),
@@ -360,6 +364,15 @@ class MpnCtx:
                                          ctypes.byref(ms)))
         return ms.value
 
+    def time_batched(self, an, bn, cfg=None, copies=16, reps=3):
+        """Marginal device milliseconds of an an x bn product inside a batch of
+        `copies` such products under cfg (autotuner probe)."""
+        ms = ctypes.c_double()
+        _check(lib().gpu_mpn_mul_time_batched(self.ptr, an, bn,
+                                              ctypes.byref(cfg) if cfg is not None else None,
+                                              copies, reps, ctypes.byref(ms)))
+        return ms.value
+
     @property
     def last_launches(self):
         return int(lib().gpu_mpn_ctx_last_launches(self.ptr))
@@ -384,12 +397,17 @@ class MpnBatch:
     without synchronising; check() waits and raises on a kernel error.
     """
 
-    def __init__(self, ctx, reqs, promote_small=0, max_streams=4, use_graph=True):
+    def __init__(self, ctx, reqs, promote_small=0, max_streams=4, use_graph=True, configs=None):
         arr = (MulReq * len(reqs))(*[MulReq(z, a, an, b, bn) for (z, a, an, b, bn) in reqs])
         opt = BatchOptions(promote_small, max_streams, 1 if use_graph else 0)
+        cfg = None
+        if configs is not None:
+            if len(configs) != len(reqs):
+                raise ValueError("one configuration per request")
+            cfg = (MulConfig * len(reqs))(*[MulConfig(*c.key()) for c in configs])
         self._h = ctypes.c_void_p()
-        _check(lib().gpu_mpn_batch_init(ctypes.byref(self._h), ctx.ptr, arr, len(reqs),
-                                        ctypes.byref(opt)))
+        _check(lib().gpu_mpn_batch_init_config(ctypes.byref(self._h), ctx.ptr, arr, cfg, len(reqs),
+                                               ctypes.byref(opt)))
 
     def run(self, stream=None):
         _check(lib().gpu_mpn_batch_run(self._h, stream))

@@ -12,11 +12,14 @@
 // through flint_mpn_mul's size thresholds (src/mpn_extras/mul.c:52-75).
 #pragma once
 #include <stdint.h>
+#include "mpn_kernels.cuh"
 
 namespace fb {
 
 constexpr int BASECASE_MAX = 1024;
 constexpr int BASECASE_THREADS = 256;
+constexpr int BASECASE_PER = 4;                                  // positions per thread
+constexpr int BASECASE_TILE = BASECASE_THREADS * BASECASE_PER;   // = the carry kernel's tile
 
 __device__ __forceinline__ void mac192(uint64_t& a0, uint64_t& a1, uint64_t& a2, uint64_t x, uint64_t y)
 {
@@ -28,33 +31,63 @@ __device__ __forceinline__ void mac192(uint64_t& a0, uint64_t& a1, uint64_t& a2,
         : "l"(lo), "l"(hi));
 }
 
-// grid = ceil((xn + yn - 1) / THREADS); thread k0 + t computes s_(k0+t).
-// planes: s[k], s[P + k], s[2 P + k] with plane stride P >= xn + yn - 1.
+// One tile of 1024 positions per block; thread t computes positions
+// k0 + 4t .. k0 + 4t + 3 with a sliding window of four x values (one shared
+// load and four multiply-accumulates per y limb).  Planes: s[k], s[P + k],
+// s[2P + k] with P = 2^logM.  With a batch descriptor the block's instance
+// comes from tile_inst (the same tile map as the carry kernel) and x, y, s
+// from the instance (s = its residue scratch).
 __global__ void __launch_bounds__(BASECASE_THREADS)
 k_basecase_sums(const uint64_t* __restrict__ x, uint64_t xn, const uint64_t* __restrict__ y,
-                uint32_t yn, uint64_t* __restrict__ s, uint64_t P)
+                uint64_t yn, uint64_t* __restrict__ s, int logM,
+                const InstDesc* __restrict__ desc, const uint32_t* __restrict__ tile_inst)
 {
     __shared__ uint64_t sy[BASECASE_MAX];
-    __shared__ uint64_t sx[BASECASE_THREADS + BASECASE_MAX];
-    const uint64_t k0 = (uint64_t)blockIdx.x * BASECASE_THREADS;
+    __shared__ uint64_t sx[BASECASE_TILE + BASECASE_MAX];
+    uint32_t tile = blockIdx.x;
+    if (desc) {
+        const InstDesc& D = desc[tile_inst[blockIdx.x]];
+        tile = blockIdx.x - D.tile0;
+        x = D.a; xn = D.an; y = D.b; yn = D.bn;
+        if (yn > xn) {
+            const uint64_t* t = x; x = y; y = t;
+            const uint64_t tn = xn; xn = yn; yn = tn;
+        }
+        s = reinterpret_cast<uint64_t*>(D.ra);
+    }
+    const uint64_t L = xn + yn - 1;
+    const uint64_t k0 = (uint64_t)tile * BASECASE_TILE;
     for (uint32_t i = threadIdx.x; i < yn; i += BASECASE_THREADS) sy[i] = y[i];
-    // x window k0 - (yn - 1) .. k0 + THREADS - 1, zero outside [0, xn)
+    // x window k0 - (yn - 1) .. k0 + TILE - 1, zero outside [0, xn)
     const int64_t xb = (int64_t)k0 - (int64_t)(yn - 1);
-    for (uint32_t i = threadIdx.x; i < BASECASE_THREADS + yn - 1; i += BASECASE_THREADS) {
+    for (uint32_t i = threadIdx.x; i < BASECASE_TILE + yn - 1; i += BASECASE_THREADS) {
         const int64_t xi = xb + (int64_t)i;
         sx[i] = (xi >= 0 && (uint64_t)xi < xn) ? x[xi] : 0ull;
     }
     __syncthreads();
-    const uint64_t k = k0 + threadIdx.x;
-    const uint64_t L = xn + yn - 1;
-    uint64_t a0 = 0, a1 = 0, a2 = 0;
-    const uint64_t* px = sx + threadIdx.x + (yn - 1);   // px[-j] = x[k - j]
-#pragma unroll 4
-    for (uint32_t j = 0; j < yn; j++) mac192(a0, a1, a2, px[-(int)j], sy[j]);
-    if (k < L) {
-        s[k] = a0;
-        s[P + k] = a1;
-        s[2 * P + k] = a2;
+    // position k0 + 4t + q reads x[k0 + 4t + q - j] = sx[4t + q + yn - 1 - j]
+    const uint64_t* px = sx + BASECASE_PER * threadIdx.x + (yn - 1);
+    uint64_t w0 = px[0], w1 = px[1], w2 = px[2], w3 = px[3];
+    uint64_t a[BASECASE_PER][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (uint32_t j = 0; j < yn; j++) {
+        const uint64_t yj = sy[j];
+        mac192(a[0][0], a[0][1], a[0][2], w0, yj);
+        mac192(a[1][0], a[1][1], a[1][2], w1, yj);
+        mac192(a[2][0], a[2][1], a[2][2], w2, yj);
+        mac192(a[3][0], a[3][1], a[3][2], w3, yj);
+        // slide: the next j needs x one position lower for every q
+        w3 = w2; w2 = w1; w1 = w0;
+        w0 = (j + 1 < yn) ? px[-(int64_t)(j + 1)] : 0ull;
+    }
+    const size_t P = (size_t)1 << logM;
+#pragma unroll
+    for (int q = 0; q < BASECASE_PER; q++) {
+        const uint64_t k = k0 + BASECASE_PER * threadIdx.x + q;
+        if (k < L) {
+            s[k] = a[q][0];
+            s[P + k] = a[q][1];
+            s[2 * P + k] = a[q][2];
+        }
     }
 }
 

@@ -674,8 +674,7 @@ static int mpn_mul_basecase_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint
         X->epoch = 1;
     }
     TimingRecord *tr = timing_begin(X, st);
-    k_basecase_sums<<<(unsigned)((L + BASECASE_THREADS - 1) / BASECASE_THREADS), BASECASE_THREADS, 0, st>>>(
-        x, xn, y, (uint32_t)yn, sums, plane);
+    k_basecase_sums<<<(unsigned)tiles, BASECASE_THREADS, 0, st>>>(x, xn, y, yn, sums, logM, nullptr, nullptr);
     timing_mark(tr, 1, st);
     timing_mark(tr, 2, st);
     timing_mark(tr, 3, st);
@@ -1055,6 +1054,56 @@ int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw, g
     return 0;
 }
 
+int gpu_mpn_mul_time_batched(gpu_mpn_ctx_t R, gpu_ulong an, gpu_ulong bn, const gpu_mul_config *cfg,
+                             int copies, int reps, double *ms_per_product)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (reps < 1 || copies < 1 || !ms_per_product) return set_error(GPU_FFT_SMALL_EINVAL, "bad timing request");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    gpu_mul_config c = cfg ? *cfg : gpu_mul_config{0, 0, 0, 0};
+    rc = gpu_mpn_mul_config_resolve(an, bn, &c);
+    if (rc) return rc;
+    const size_t per = an + bn + (an + bn);
+    uint64_t *buf = nullptr;
+    CU(cudaMalloc(&buf, per * copies * sizeof(uint64_t)));
+    cudaStream_t st = X->stream;
+    std::vector<gpu_mpn_mul_req> reqs(copies);
+    std::vector<gpu_mul_config> cfgs(copies, cfg ? *cfg : gpu_mul_config{0, 0, 0, 0});
+    for (int k = 0; k < copies; k++) {
+        uint64_t *base = buf + per * k;
+        k_fill_limbs<<<X->nsm, 256, 0, st>>>(base, an + bn, 0x9999ull + 77 * k);
+        reqs[k] = gpu_mpn_mul_req{base + an + bn, base, an, base + an, bn};
+    }
+    Batch *B = new Batch();
+    B->X = X;
+    gpu_mpn_batch_options opt = {0, 4, 1};
+    rc = batch_plan(B, reqs.data(), cfgs.data(), copies, &opt);
+    std::vector<float> t(reps);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (!rc) rc = batch_run(B, st);   // warm-up and graph capture
+    if (!rc && cudaEventCreate(&e0) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
+    if (!rc && cudaEventCreate(&e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
+    for (int r = 0; r < reps && !rc; r++) {
+        cudaEventRecord(e0, st);
+        rc = batch_run(B, st);
+        cudaEventRecord(e1, st);
+        if (!rc && cudaEventSynchronize(e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "timing sync");
+        if (!rc) cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    if (!rc) rc = check_device_error(X);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    batch_destroy(B);
+    cudaFree(buf);
+    if (rc) return rc;
+    std::sort(t.begin(), t.end());
+    *ms_per_product = t[reps / 2] / copies;
+    return 0;
+}
+
 int _gpu_fmpz_poly_mul_mid_mpn_ctx(gpu_slong *z, gpu_ulong zl, gpu_ulong zh, const gpu_slong *a,
                                    gpu_ulong an, const gpu_slong *b, gpu_ulong bn, gpu_mpn_ctx_t R)
 {
@@ -1086,6 +1135,12 @@ struct gpu_mpn_batch_struct {
 int gpu_mpn_batch_init(gpu_mpn_batch_t *out, gpu_mpn_ctx_t R, const gpu_mpn_mul_req *reqs, size_t n,
                        const gpu_mpn_batch_options *opt)
 {
+    return gpu_mpn_batch_init_config(out, R, reqs, nullptr, n, opt);
+}
+
+int gpu_mpn_batch_init_config(gpu_mpn_batch_t *out, gpu_mpn_ctx_t R, const gpu_mpn_mul_req *reqs,
+                              const gpu_mul_config *cfgs, size_t n, const gpu_mpn_batch_options *opt)
+{
     if (!out) return set_error(GPU_FFT_SMALL_EINVAL, "null batch handle");
     *out = nullptr;
     Ctx *X = get_ctx(R);
@@ -1097,7 +1152,7 @@ int gpu_mpn_batch_init(gpu_mpn_batch_t *out, gpu_mpn_ctx_t R, const gpu_mpn_mul_
     if (rc) return rc;
     Batch *B = new Batch();
     B->X = X;
-    rc = batch_plan(B, reqs, n, opt);
+    rc = batch_plan(B, reqs, cfgs, n, opt);
     if (rc) {
         batch_destroy(B);
         return rc;

@@ -98,19 +98,34 @@ def features(r, cfg):
     return f
 
 
-class Autotuner:
-    """Exhaustive measurement of a request's candidates on the device."""
+def batch_copies(an, bn):
+    """Products per timing batch in batched mode: about 2^22 limbs of operands,
+    between 1 and 64 products."""
+    return max(1, min(64, (1 << 22) // (an + bn)))
 
-    def __init__(self, ctx, reps=3):
+
+class Autotuner:
+    """Exhaustive measurement of a request's candidates on the device.
+
+    batched=False times a product alone (gpu_mul_time_config); batched=True
+    times mpn products as the marginal cost inside a batch of identical
+    products (gpu_mpn_mul_time_batched), the cost that matters when requests
+    are executed as planned batches."""
+
+    def __init__(self, ctx, reps=3, batched=False):
         self.ctx = ctx
         self.reps = reps
+        self.batched = batched
         self.cache = {}
 
     def time(self, r, cfg):
         kind, an, bn, aw, bw = _req(r)
         key = (kind, an, bn, aw, bw, cfg.key())
         if key not in self.cache:
-            self.cache[key] = self.ctx.time_config(kind, an, bn, cfg, aw, bw, self.reps)
+            if self.batched and kind == 0:
+                self.cache[key] = self.ctx.time_batched(an, bn, cfg, batch_copies(an, bn), self.reps)
+            else:
+                self.cache[key] = self.ctx.time_config(kind, an, bn, cfg, aw, bw, self.reps)
         return self.cache[key]
 
     def table(self, r):

@@ -200,6 +200,14 @@ GPU_FFT_SMALL_API int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong a
                                           gpu_ulong bn, gpu_ulong bw, const gpu_mul_config *cfg,
                                           int reps, double *ms);
 
+/* The same for products inside a batch: `copies` an x bn products of one
+   configuration run as one planned batch (gpu_mpn_batch_*, graph replay);
+   *ms_per_product = median batch time / copies, the marginal cost of a
+   product in batched execution. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_time_batched(gpu_mpn_ctx_t R, gpu_ulong an, gpu_ulong bn,
+                                               const gpu_mul_config *cfg, int copies, int reps,
+                                               double *ms_per_product);
+
 /* --- cost model of the learned schedule (no counterpart in the reference) --
 
    A fully connected network n_in -> 64 -> 64 -> 64 -> 1 (ReLU, fp32) that
@@ -314,6 +322,12 @@ typedef struct gpu_mpn_batch_struct *gpu_mpn_batch_t;
 GPU_FFT_SMALL_API int gpu_mpn_batch_init(gpu_mpn_batch_t *B, gpu_mpn_ctx_t R,
                                          const gpu_mpn_mul_req *reqs, size_t n,
                                          const gpu_mpn_batch_options *opt);
+/* gpu_mpn_batch_init with a configuration per request (cfgs[i] for reqs[i],
+   see gpu_mul_config; NULL = defaults): products sharing a configuration run
+   in the same launches. */
+GPU_FFT_SMALL_API int gpu_mpn_batch_init_config(gpu_mpn_batch_t *B, gpu_mpn_ctx_t R,
+                                                const gpu_mpn_mul_req *reqs, const gpu_mul_config *cfgs,
+                                                size_t n, const gpu_mpn_batch_options *opt);
 /* Queues every product of the batch on `stream` (NULL = CUDA's default
    stream) and returns without synchronising.  Runs of one batch must not
    overlap.  Kernel errors (a carry look-back that gave up) are reported by

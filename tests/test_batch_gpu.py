@@ -132,3 +132,36 @@ def test_batch_rejects_bad_requests(ctx):
     with pytest.raises(FB.GpuFftSmallError) as e:
         FB.MpnBatch(ctx, [])
     assert e.value.code == FB.EINVAL
+
+
+def test_configured_batch_with_basecase_classes(ctx):
+    """Per-request configurations: basecase, shorter rows, a longer transform
+    and an extra prime, mixed in one batch; every product exact."""
+    torch = pytest.importorskip("torch")
+    from flint_b200 import tuner
+    sizes = uneven_batch(77, 90, log_lo=0.0, log_hi=14.0) + [(5000, 1024), (1024, 1024), (1, 1),
+                                                             (70000, 3), (3, 70000)]
+    host, spans, d_in, d_out, reqs, zoff = _device_batch(torch, sizes, 5)
+    configs = []
+    for k, (an, bn) in enumerate(sizes):
+        cs = tuner.candidates((0, an, bn))
+        configs.append(cs[k % len(cs)])
+    assert any(c.route == FB.ROUTE_BASECASE for c in configs)
+    stream = torch.cuda.current_stream()
+    with FB.MpnBatch(ctx, reqs, configs=configs, promote_small=3) as B:
+        B.run(stream.cuda_stream)
+        B.check(stream.cuda_stream)
+        out = d_out.cpu().numpy().view(np.uint64)
+        _check_vs_gmp(host, spans, out, zoff)
+        d_out.fill_(-1)
+        B.run(stream.cuda_stream)   # graph replay
+        B.check(stream.cuda_stream)
+    _check_vs_gmp(host, spans, d_out.cpu().numpy().view(np.uint64), zoff)
+
+
+def test_time_batched_is_positive(ctx):
+    from flint_b200 import tuner
+    for an, bn in [(100, 100), (3000, 700), (1 << 16, 1 << 12)]:
+        for c in tuner.candidates((0, an, bn))[:4]:
+            ms = ctx.time_batched(an, bn, c, copies=tuner.batch_copies(an, bn), reps=2)
+            assert 0.0 < ms < 100.0
