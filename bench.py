@@ -190,10 +190,112 @@ def time_on_stream(torch, stream, fn, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds):
+def train_cost_model(ctx):
+    """The learned schedule used by the batch and stream legs: exhaustive
+    autotuner timings of a training sample (mpn products timed as the marginal
+    cost inside a batch, integer-polynomial products alone), then the MLP cost
+    model trained on them by the library's CUDA kernels."""
+    from flint_b200 import tuner
+    from flint_b200.workload import request_stream, uneven_batch
+    t0 = time.perf_counter()
+    train = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 1, 160)]
+    train += request_stream(STREAM_SEED + 1, 96)
+    tun = tuner.Autotuner(ctx, reps=3, batched=True)
+    X, t = tuner.dataset(tun, train)
+    t_tune = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    model = tuner.CostModel(seed=11)
+    loss = model.fit(X, t, epochs=400)
+    info = {"train_requests": len(train), "train_rows": int(len(X)), "tuning_s": t_tune,
+            "fit_s": time.perf_counter() - t0, "fit_mse_log_ms": loss,
+            "network": "16 -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels"}
+    return model, tun, info
+
+
+STREAM_SEED = 5005
+
+
+def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds):
+    """The mixed request stream (half mpn products, an log-uniform in
+    [2^6, 2^22], ratio log-uniform in [1, 64]; half integer-polynomial
+    products, lengths log-uniform in [2^8, 2^16], coefficient bits uniform in
+    [64, 4096]) under the learned schedule and under the fixed rule."""
+    from flint_b200 import tuner
+    from flint_b200.stream import run_stream
+    from flint_b200.workload import request_stream
+    reqs = request_stream(STREAM_SEED, n_req)
+    t0 = time.perf_counter()
+    learned = model.choose(reqs)
+    t_choose = time.perf_counter() - t0
+    default = [tuner.default_config(r) for r in reqs]
+    keep = set(range(0, n_req, max(1, n_req // 24)))
+    rl = run_stream(ctx, torch, reqs, learned, 17, stream, dev, keep=keep, check_against=default)
+    rd = run_stream(ctx, torch, reqs, default, 17, stream, dev)
+    held = request_stream(STREAM_SEED + 2, 32)
+    reg = tuner.regret(tun, held, model.choose(held))
+    bits_mpn = NS_LIMB_BITS * rl["mpn_limbs"]
+    res = {
+        "workload": "%d requests: half mpn_mul (an log-uniform [2^6, 2^22], an/bn log-uniform "
+                    "[1, 64]), half fmpz_poly_mul (lengths log-uniform [2^8, 2^16], coefficient "
+                    "bits uniform [64, 4096]), seed %d; mpn products in planned batches, "
+                    "integer polynomials one call each" % (n_req, STREAM_SEED),
+        "requests": n_req, "mpn_requests": rl["mpn_requests"], "fmpz_requests": rl["fmpz_requests"],
+        "learned": {"total_ms": rl["total_ms"], "mpn_ms": rl["mpn_ms"], "fmpz_ms": rl["fmpz_ms"],
+                    "mpn_Gbit_s": bits_mpn / rl["mpn_ms"] / 1e6},
+        "default_rule": {"total_ms": rd["total_ms"], "mpn_ms": rd["mpn_ms"], "fmpz_ms": rd["fmpz_ms"],
+                         "mpn_Gbit_s": bits_mpn / rd["mpn_ms"] / 1e6},
+        "gain_over_default_rule": rd["total_ms"] / rl["total_ms"],
+        "choose_s": t_choose,
+        "routes": {"transform": sum(c.route == 0 for c in learned),
+                   "basecase": sum(c.route == 1 for c in learned)},
+        "identical_to_default_rule": rl["identical"],
+        "held_out_regret_vs_exhaustive": reg,
+    }
+    if cpu_seconds > 0:
+        res["cpu_baseline"] = stream_cpu_check(reqs, rl["kept"], cpu_seconds)
+    return res
+
+
+def stream_cpu_check(reqs, kept, seconds):
+    """The reference's own products for a subsample of the stream, timed on
+    the host, each compared limb for limb with the GPU's product."""
+    import oracle
+    L, kind, nthreads = ref_library()
+    if L is None:
+        return None
+    t0 = time.perf_counter()
+    done, same, t_ref = 0, 0, 0.0
+    for k in sorted(kept):
+        if time.perf_counter() - t0 > seconds:
+            break
+        r = reqs[k]
+        if r[0] == 0:
+            ops, z = kept[k]
+            an, bn = r[1], r[2]
+            t = time.perf_counter()
+            want = oracle.ref_mpn_mul(ops[:an], ops[an:an + bn])
+            t_ref += time.perf_counter() - t
+        else:
+            a, b, z = kept[k]
+            _, an, bn, aw, bw = r
+            zw = aw + bw + 1
+            t = time.perf_counter()
+            want = oracle.ref_fmpz_poly_mul_raw(a.reshape(an, aw), b.reshape(bn, bw), zw)
+            t_ref += time.perf_counter() - t
+            want = want.reshape(-1)
+        done += 1
+        same += int(np.array_equal(np.asarray(want).reshape(-1), np.asarray(z).reshape(-1)))
+    return {"checked": done, "identical": same, "ref_seconds": t_ref, "cores": min(nthreads, 8),
+            "kind": kind,
+            "sample": "every %d-th request of the stream, reference product vs GPU product" %
+            max(1, len(reqs) // 24)}
+
+
+def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, tun, train_info):
     """4096 uneven products (an = round(2^U), U ~ U[10,18]; bn = an / 2^V,
     V ~ U[0,4]): the per-instance device entry point in a loop against one
     planned batch.  Returns the `batch` object of the JSON line."""
+    from flint_b200 import tuner
     from flint_b200.workload import batch_operands, uneven_batch
     sizes = uneven_batch(BATCH_SEED, BATCH_N)
     host, spans = batch_operands(7, sizes)
@@ -222,19 +324,8 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds):
     B0.check(s)
     exact_default = bool(torch.equal(d_out, d_ref))
     B0.close()
-    # learned schedule: autotuner timings (batched marginal cost) of a training
-    # sample from the same distribution, the cost model trained on them by the
-    # library's CUDA kernels, then one configuration per request of the batch
-    from flint_b200 import tuner
-    t0 = time.perf_counter()
-    train = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 1, 160)]
-    tun = tuner.Autotuner(ctx, reps=3, batched=True)
-    X, tt = tuner.dataset(tun, train)
-    t_tune = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    model = tuner.CostModel(seed=11)
-    fit_loss = model.fit(X, tt, epochs=400)
-    t_fit = time.perf_counter() - t0
+    # learned schedule: one configuration per request of the batch from the
+    # cost model; its regret on held-out requests of this distribution
     held = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 2, 48)]
     reg = tuner.regret(tun, held, model.choose(held))
     t0 = time.perf_counter()
@@ -279,9 +370,7 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds):
                           "schedule": "default configuration for every request"},
         "speedup_vs_per_instance": ms_plain / ms_batch,
         "speedup_vs_plain_batched": ms_default / ms_batch,
-        "learned": {"train_requests": len(train), "train_rows": int(len(X)),
-                    "tuning_s": t_tune, "fit_s": t_fit, "fit_mse_log_ms": fit_loss,
-                    "choose_s_4096": t_choose,
+        "learned": {"training": train_info, "choose_s_4096": t_choose,
                     "routes": {"transform": sum(c.route == 0 for c in configs),
                                "basecase": sum(c.route == 1 for c in configs)},
                     "held_out_regret_vs_exhaustive": reg},
@@ -339,6 +428,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 4096-product uneven batch")
+    ap.add_argument("--stream-requests", type=int, default=2000,
+                    help="requests of the mixed mpn / integer-polynomial stream (0 = skip)")
     args = ap.parse_args()
     an, bn, desc = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -445,10 +536,15 @@ def main():
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    batch = None
+    batch = stream_res = None
+    cpu_s = 0.0 if (world > 1 or args.no_cpu_baseline) else 10.0
+    if not (args.no_batch and args.stream_requests == 0):
+        model, tun, train_info = train_cost_model(ctx)
     if not args.no_batch:
-        batch = bench_batch(torch, FB, ctx, dev, stream, args.steps, args.warmup,
-                            cpu_seconds=0.0 if (world > 1 or args.no_cpu_baseline) else 10.0)
+        batch = bench_batch(torch, FB, ctx, dev, stream, args.steps, args.warmup, cpu_s, model, tun,
+                            train_info)
+    if args.stream_requests > 0:
+        stream_res = bench_stream(torch, FB, ctx, dev, stream, model, tun, args.stream_requests, cpu_s)
     clk = clocks.stop()
     e2e_ok = bool(np.array_equal(hz.numpy().view(np.uint64), z))
 
@@ -502,6 +598,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk,
         "batch": batch,
+        "stream": stream_res,
     }
     print(json.dumps(line), flush=True)
     if dist:
