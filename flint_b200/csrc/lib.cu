@@ -370,7 +370,7 @@ static LaunchShape make_shape(int logM, int logC = -1)
     L.nv = std::min(R, std::max(1, 1 << (LOG_MAXC - L.S.logC)));
     L.row_threads = L.nv * C / 32;
     L.row_grid = (R + L.nv - 1) / L.nv;                // items per prime; launch clamps
-    L.row_smem = (size_t)2 * L.nv * padw(C) * sizeof(uint32_t);   // b and a buffers
+    L.row_smem = (size_t)3 * L.nv * padw(C) * sizeof(uint32_t);   // b and two a buffers
     return L;
 }
 
@@ -395,7 +395,7 @@ static int configure_kernels()
         CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
     for (int c = 5; c <= LOG_MAXC; c++)
-        CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     done = true;
     return 0;
 }
@@ -1438,7 +1438,7 @@ static int na_setup(int dev, NaDevice &D)
         NA_CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
     for (int c = 5; c <= LOG_MAXC; c++)
-        NA_CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        NA_CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     NA_CU(cudaMemcpyToSymbol(c_na_primes, PRIMES, sizeof(uint32_t) * NA_NP));
     NA_CU(cudaMemcpyToSymbol(c_na_roots, roots, sizeof roots));
     NA_CU(cudaMemcpyToSymbol(c_w32, w32, sizeof(W32Table) * MAX_NP));

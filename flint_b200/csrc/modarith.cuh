@@ -115,19 +115,19 @@ __device__ __forceinline__ uint32_t fsub(uint32_t x, uint32_t y) { return y * c_
 
 // Gentleman-Sande butterfly, inputs and outputs in [0, p):
 // (a, b) -> (a + b, (a - b) w).
-// F selects the pipe mix: with F, two additions go to the FMA pipe (for
-// kernels whose other work is ALU-heavy); without, one does (for kernels
-// whose other work is multiplication-heavy).  The high-half multiply
-// occupies the FMA pipe for two issue slots.
-template <bool F = true>
+// F (0, 1 or 2) is the number of additions sent to the FMA pipe: 2 for
+// kernels whose other work is ALU-heavy, fewer for kernels whose other work
+// is multiplication-heavy.  The high-half multiply occupies the FMA pipe for
+// two issue slots.
+template <int F = 2>
 __device__ __forceinline__ void bfly_gs(uint32_t& a, uint32_t& b, uint32_t w, uint32_t wq, uint32_t p)
 {
-    const uint32_t s = fadd(a, b);          // FMA pipe
+    const uint32_t s = F >= 1 ? fadd(a, b) : a + b;
     const uint32_t s1 = a + b - p;          // ALU
     const uint32_t d = a - b + p;           // ALU, in [1, 2p)
     const uint32_t q = __umulhi(d, wq);
     const uint32_t r = d * w - q * p;       // [0, 2p)
-    const uint32_t r1 = F ? fadd(r, 0u - p) : r - p;
+    const uint32_t r1 = F >= 2 ? fadd(r, 0u - p) : r - p;
     a = min(s, s1);
     b = min(r, r1);
 }
@@ -144,17 +144,17 @@ __device__ __forceinline__ void bfly_gs1(uint32_t& a, uint32_t& b, uint32_t p)
 }
 
 // Cooley-Tukey butterfly, inputs and outputs in [0, p):
-// (x, y) -> (x + y w, x - y w); F as for bfly_gs
-template <bool F = true>
+// (x, y) -> (x + y w, x - y w); F as for bfly_gs (up to 3 here)
+template <int F = 2>
 __device__ __forceinline__ void bfly_ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p)
 {
     const uint32_t q = __umulhi(y, wq);
     uint32_t t = y * w - q * p;             // [0, 2p)
-    t = min(t, F ? fadd(t, 0u - p) : t - p);
-    const uint32_t s = fadd(x, t);
+    t = min(t, F >= 3 ? fadd(t, 0u - p) : t - p);
+    const uint32_t s = F >= 1 ? fadd(x, t) : x + t;
     const uint32_t s1 = x + t - p;
     const uint32_t d = x - t + p;
-    const uint32_t d1 = fsub(x, t);
+    const uint32_t d1 = F >= 2 ? fsub(x, t) : x - t;
     x = min(s, s1);
     y = min(d, d1);
 }

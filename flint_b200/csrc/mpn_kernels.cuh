@@ -238,7 +238,7 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             uint32_t xr[32];
 #pragma unroll
             for (int m = 0; m < 32; m++) xr[m] = sm[pb + padw(m * G)];
-            gs_contig<5, false>(xr, c_w32[j], p);
+            gs_contig<5, COL_FMA_ADDS>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
             twist32<LOGR>(xr, col, s, logM, th, tl, P);
 #pragma unroll
@@ -250,7 +250,7 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             uint32_t xr[R];
 #pragma unroll
             for (int m = 0; m < R; m++) xr[m] = sm[padw(m * GR) + v];
-            if constexpr (LOGR > 0) gs_contig<LOGR, false>(xr, c_w32[j], p);
+            if constexpr (LOGR > 0) gs_contig<LOGR, COL_FMA_ADDS>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
 #pragma unroll
             for (int m = 0; m < R; m++) {
@@ -267,13 +267,14 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
 
 // ---------------------------------------------------------------------------
 // Row pass, persistent: each CTA walks over items of nv rows (one prime per
-// item).  For every item: forward transform of b (result kept in registers),
-// forward transform of a, pointwise product times scale[j], inverse
-// transform; the result overwrites the a rows.  Two shared buffers hold b and
-// a; the next item's rows are fetched with cp.async into a buffer as soon as
-// the current item has finished with it, so global loads overlap the
-// transforms.  grid = min(items, SMs); block = nv * C / 32;
-// smem = 2 * nv * padw(C) words.
+// item).  For every item: forward transforms of a and b as one interleaved
+// network (shared twiddle loads, twice the independent work per thread; b's
+// spectrum ends in registers), pointwise product times scale[j], inverse
+// transform; the result overwrites the a rows.  Three shared buffers: b, and
+// a ping-pong pair for a, so the next item's a rows stream in (cp.async)
+// during the whole current item and its b rows as soon as b's spectrum is in
+// registers.  grid = min(items, resident CTAs); block = nv * C / 32;
+// smem = 3 * nv * padw(C) words.
 __device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src, bool valid)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
@@ -330,7 +331,9 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     const int per = groups * np;           // items of one product
     const int total = per * ninst;
     uint32_t* sb = sm;
-    uint32_t* sa = sm + nv * PC;
+    // a ping-pong pair at sm + nv PC and sm + 2 nv PC (pointer arithmetic, not
+    // an indexed array, so nothing goes to local memory)
+    auto sa_buf = [&](int c) { return sm + (1 + c) * nv * PC; };
     const int t = threadIdx.x;
     const int pb = (t / NSUB) * PC + 33 * (t & (NSUB - 1));
     // item -> (prime, first row, residue base of a, of b)
@@ -350,10 +353,11 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         uint32_t* A;
         const uint32_t* B;
         decode(g, j, u0, A, B);
+        rows_prefetch<LOGC>(sa_buf(0), A + ((size_t)j << logM), u0, nv, R);
         if (!squaring) rows_prefetch<LOGC>(sb, B + ((size_t)j << logM), u0, nv, R);
         else cp_async_commit();
-        rows_prefetch<LOGC>(sa, A + ((size_t)j << logM), u0, nv, R);
     }
+    int cur = 0;
     for (; g < total; g += gridDim.x) {
         int j, u0, j2 = 0, u2 = 0;
         uint32_t *A, *A2 = nullptr;
@@ -365,33 +369,42 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         const uint32_t p = P.p;
         const uint2* __restrict__ twf = T.twf + (size_t)j * TW_SZ;
         const uint2* __restrict__ twi = T.twi + (size_t)j * TW_SZ;
+        uint32_t* sa = sa_buf(cur);
 
+        // this item's a and b rows have landed; the other a buffer is free
+        // (its last item stored from it before the barrier)
+        cp_async_wait<0>();
+        __syncthreads();
+        if (g2 < total) rows_prefetch<LOGC>(sa_buf(cur ^ 1), A2 + ((size_t)j2 << logM), u2, nv, R);
+        else cp_async_commit();
+
+        uint32_t xr[32];
         uint32_t breg[32];
         if (!squaring) {
-            cp_async_wait<1>();
-            __syncthreads();
-            gs_strided_all<LOGC, 0>(sb, nv, twf, p);
+            gs_strided_all2<LOGC>(sa, sb, nv, twf, p);
 #pragma unroll
-            for (int m = 0; m < 32; m++) breg[m] = sb[pb + m];
-            gs_contig<5>(breg, c_w32[j], p);
-            __syncthreads();
+            for (int m = 0; m < 32; m++) {
+                xr[m] = sa[pb + m];
+                breg[m] = sb[pb + m];
+            }
+            gs_contig2<5>(xr, breg, c_w32[j], p);
+            __syncthreads();   // b fully read: refill it for the next item
+            if (g2 < total) rows_prefetch<LOGC>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
+            else cp_async_commit();
+        } else {
+            gs_strided_all<LOGC, 0>(sa, nv, twf, p);
+#pragma unroll
+            for (int m = 0; m < 32; m++) xr[m] = sa[pb + m];
+            gs_contig<5>(xr, c_w32[j], p);
+            cp_async_commit();
         }
-        if (!squaring && g2 < total) rows_prefetch<LOGC>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
-        else cp_async_commit();
-        cp_async_wait<1>();
-        __syncthreads();
-        gs_strided_all<LOGC, 0>(sa, nv, twf, p);
-        uint32_t xr[32];
-#pragma unroll
-        for (int m = 0; m < 32; m++) xr[m] = sa[pb + m];
-        gs_contig<5>(xr, c_w32[j], p);
         const uint32_t sc = scale[j];
 #pragma unroll
         for (int m = 0; m < 32; m++) {
             const uint32_t y = squaring ? xr[m] : breg[m];
             xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
         }
-        ct_contig<5>(xr, c_w32[j], p);
+        ct_contig<5, 3>(xr, c_w32[j], p);
 #pragma unroll
         for (int m = 0; m < 32; m++) sa[pb + m] = xr[m];
         __syncthreads();
@@ -409,9 +422,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
                 if (u < R) abase[(size_t)u * C + i] = sa[v * PC + padw(i)];
             }
         }
-        __syncthreads();
-        if (g2 < total) rows_prefetch<LOGC>(sa, A2 + ((size_t)j2 << logM), u2, nv, R);
-        else cp_async_commit();
+        cur ^= 1;
     }
     cp_async_wait<0>();
 }
@@ -449,7 +460,7 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
 #pragma unroll
             for (int m = 0; m < 32; m++) xr[m] = buf[(size_t)(32 * s + m) * C + col];
             twist32<LOGR>(xr, col, s, logM, th, tl, P);
-            ct_contig<5, false>(xr, c_w32[j], p);
+            ct_contig<5, COL_FMA_ADDS>(xr, c_w32[j], p);
             const int pb = 33 * G * s + v;
 #pragma unroll
             for (int m = 0; m < 32; m++) sm[pb + padw(m * G)] = xr[m];
@@ -474,7 +485,7 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
                 const uint32_t e = ((col * bitrev_bits(m, LOGR)) & mmask) << sh;
                 xr[m] = twist_mul(buf[(size_t)m * C + col], e, th, tl, p);
             }
-            ct_contig<LOGR, false>(xr, c_w32[j], p);
+            ct_contig<LOGR, COL_FMA_ADDS>(xr, c_w32[j], p);
 #pragma unroll
             for (int m = 0; m < R; m++) buf[(size_t)m * C + col] = xr[m];
         }

@@ -16,8 +16,8 @@
 //   * the contiguous pass (the five levels h = 16..1): each thread owns 32
 //     consecutive positions; its twiddles are powers of w_32, the same for
 //     every thread, and come from constant memory.
-// Row passes (G == 0) route two additions per butterfly to the FMA pipe,
-// column passes one (see bfly_gs).
+// Row passes (G == 0) route two (forward) or three (inverse) additions per
+// butterfly to the FMA pipe, column passes COL_FMA_ADDS (see bfly_gs).
 // Shared memory holds one pad word per 32 (physical = a + a/32), which makes
 // both kinds of pass conflict-free and lets every address be a per-thread
 // base plus a compile-time offset.
@@ -35,6 +35,7 @@
 namespace fb {
 
 constexpr int MAX_NP = 7;
+constexpr int COL_FMA_ADDS = 0;   // additions per column butterfly on the FMA pipe
 
 __host__ __device__ constexpr int padw(int a) { return a + (a >> 5); }
 
@@ -49,7 +50,7 @@ __constant__ W32Table c_w32[MAX_NP];
 // butterflies on registers
 
 // Q Gentleman-Sande levels on 2^Q consecutive positions (half-sizes 2^(Q-1)..1)
-template <int Q, bool F = true>
+template <int Q, int F = 2>
 __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table& W, uint32_t p)
 {
     constexpr int E = 1 << Q;
@@ -71,8 +72,35 @@ __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table&
     }
 }
 
+// gs_contig on two independent vectors with the same twiddles (twice the
+// independent work per thread for the scheduler)
+template <int Q, int F = 2>
+__device__ __forceinline__ void gs_contig2(uint32_t (&x)[1 << Q], uint32_t (&y)[1 << Q], const W32Table& W,
+                                           uint32_t p)
+{
+    constexpr int E = 1 << Q;
+#pragma unroll
+    for (int t = 0; t < Q; t++) {
+        const int hm = E >> (t + 1);
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            if ((m & hm) == 0) {
+                const int k = m & (hm - 1);
+                if (k == 0) {
+                    bfly_gs1(x[m], x[m + hm], p);
+                    bfly_gs1(y[m], y[m + hm], p);
+                } else {
+                    const uint2 w = W.f[k * (16 / hm)];
+                    bfly_gs<F>(x[m], x[m + hm], w.x, w.y, p);
+                    bfly_gs<F>(y[m], y[m + hm], w.x, w.y, p);
+                }
+            }
+        }
+    }
+}
+
 // Q Cooley-Tukey levels on 2^Q consecutive positions (half-sizes 1..2^(Q-1))
-template <int Q, bool F = true>
+template <int Q, int F = 2>
 __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table& W, uint32_t p)
 {
     constexpr int E = 1 << Q;
@@ -96,7 +124,7 @@ __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table&
 
 // Q Gentleman-Sande levels, half-sizes H..H/2^(Q-1), element stride S = H/2^(Q-1).
 // Level t is a separate instantiation so every register index is a constant.
-template <int Q, int H, int t, bool F>
+template <int Q, int H, int t, int F>
 __device__ __forceinline__ void gs_strided_level(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
                                                  int jj0, uint32_t p)
 {
@@ -113,15 +141,36 @@ __device__ __forceinline__ void gs_strided_level(uint32_t (&x)[1 << Q], const ui
     if constexpr (t + 1 < Q) gs_strided_level<Q, H, t + 1, F>(x, tw, jj0, p);
 }
 
-template <int Q, int H, bool F>
+template <int Q, int H, int F>
 __device__ __forceinline__ void gs_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ tw,
                                            int jj0, uint32_t p)
 {
     gs_strided_level<Q, H, 0, F>(x, tw, jj0, p);
 }
 
+// gs_strided on two vectors sharing the twiddle loads
+template <int Q, int H, int t, int F>
+__device__ __forceinline__ void gs_strided_level2(uint32_t (&x)[1 << Q], uint32_t (&y)[1 << Q],
+                                                  const uint2* __restrict__ tw, int jj0, uint32_t p)
+{
+    constexpr int E = 1 << Q;
+    constexpr int S = H >> (Q - 1);
+    constexpr int hm = E >> (t + 1);
+    constexpr int ht = H >> t;
+    uint2 w[hm];
+#pragma unroll
+    for (int k = 0; k < hm; k++) w[k] = tw[ht + jj0 + k * S];
+#pragma unroll
+    for (int m = 0; m < E; m++)
+        if ((m & hm) == 0) {
+            bfly_gs<F>(x[m], x[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
+            bfly_gs<F>(y[m], y[m + hm], w[m & (hm - 1)].x, w[m & (hm - 1)].y, p);
+        }
+    if constexpr (t + 1 < Q) gs_strided_level2<Q, H, t + 1, F>(x, y, tw, jj0, p);
+}
+
 // Q Cooley-Tukey levels, half-sizes H..2^(Q-1) H, element stride S = H
-template <int Q, int H, int t, bool F>
+template <int Q, int H, int t, int F>
 __device__ __forceinline__ void ct_strided_level(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
                                                  int jj0, uint32_t p)
 {
@@ -137,7 +186,7 @@ __device__ __forceinline__ void ct_strided_level(uint32_t (&x)[1 << Q], const ui
     if constexpr (t + 1 < Q) ct_strided_level<Q, H, t + 1, F>(x, twi, jj0, p);
 }
 
-template <int Q, int H, bool F>
+template <int Q, int H, int F>
 __device__ __forceinline__ void ct_strided(uint32_t (&x)[1 << Q], const uint2* __restrict__ twi,
                                            int jj0, uint32_t p)
 {
@@ -179,9 +228,41 @@ __device__ __forceinline__ void gs_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
-        gs_strided<Q, H, (G == 0)>(x, tw, jj0, p);
+        gs_strided<Q, H, (G == 0 ? 2 : COL_FMA_ADDS)>(x, tw, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
+    }
+}
+
+// gs_pass_smem over two row buffers (rows layout) with one set of twiddles
+template <int LOGL, int Q, int H>
+__device__ __forceinline__ void gs_pass_smem2(uint32_t* sx, uint32_t* sy, int nv,
+                                              const uint2* __restrict__ tw, uint32_t p)
+{
+    constexpr int L = 1 << LOGL;
+    constexpr int E = 1 << Q;
+    constexpr int S = H >> (Q - 1);
+    constexpr int NSUB = L / E;
+    const int TOT = nv * NSUB;
+    static_assert(S % 32 == 0, "strided pass must step by whole bank rows");
+    constexpr int PSTEP = S / 32 * 33;
+    for (int f = threadIdx.x; f < TOT; f += blockDim.x) {
+        const int s = f & (NSUB - 1), v = f / NSUB;
+        const int jj0 = s & (S - 1);
+        const int base = (s / S) * (2 * H) + jj0;
+        const int pb = v * padw(L) + padw(base);
+        uint32_t x[E], y[E];
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            x[m] = sx[pb + m * PSTEP];
+            y[m] = sy[pb + m * PSTEP];
+        }
+        gs_strided_level2<Q, H, 0, 2>(x, y, tw, jj0, p);
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            sx[pb + m * PSTEP] = x[m];
+            sy[pb + m * PSTEP] = y[m];
+        }
     }
 }
 
@@ -205,7 +286,7 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
-        ct_strided<Q, H, (G == 0)>(x, twi, jj0, p);
+        ct_strided<Q, H, (G == 0 ? 3 : COL_FMA_ADDS)>(x, twi, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
     }
@@ -235,6 +316,26 @@ template <int LOGL, int G, int QMAX = (G ? 4 : 5)>
 __device__ __forceinline__ void gs_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
 {
     if constexpr (LOGL > 5) gs_passes<LOGL, G, QMAX, (1 << (LOGL - 1)), LOGL - 5>(sm, nv, tw, p);
+}
+
+template <int LOGL, int QMAX, int H, int REM>
+__device__ __forceinline__ void gs_passes2(uint32_t* sx, uint32_t* sy, int nv, const uint2* __restrict__ tw,
+                                           uint32_t p)
+{
+    if constexpr (REM > 0) {
+        constexpr int Q = balanced_pass<REM, QMAX>();
+        gs_pass_smem2<LOGL, Q, H>(sx, sy, nv, tw, p);
+        __syncthreads();
+        gs_passes2<LOGL, QMAX, (H >> Q), REM - Q>(sx, sy, nv, tw, p);
+    }
+}
+
+// gs_strided_all for two row buffers at once (rows layout)
+template <int LOGL, int QMAX = 5>
+__device__ __forceinline__ void gs_strided_all2(uint32_t* sx, uint32_t* sy, int nv, const uint2* __restrict__ tw,
+                                                uint32_t p)
+{
+    if constexpr (LOGL > 5) gs_passes2<LOGL, QMAX, (1 << (LOGL - 1)), LOGL - 5>(sx, sy, nv, tw, p);
 }
 
 // Strided part of the inverse transform (half-sizes 32 .. L/2), after the
