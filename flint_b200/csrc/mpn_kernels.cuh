@@ -700,9 +700,13 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
 {
     constexpr int PER = 4;
     constexpr int TILE = PER * THREADS;
-    __shared__ uint64_t X0[TILE + 3], X1[TILE + 3], X2[TILE + 3];
+    constexpr int NW = THREADS / 32;
+    // last three coefficients of each warp (slot w + 1; slot 0 = the tile's
+    // halo, coefficients n0 - 3 .. n0 - 1): c0, c1, c2 of the last, c1, c2 of
+    // the one before, c2 of the one before that
+    __shared__ uint64_t wlast[NW + 1][6];
     __shared__ uint32_t sh_tile;
-    __shared__ uint32_t wg[THREADS / 32], wp[THREADS / 32];
+    __shared__ uint32_t wg[NW], wp[NW];
     __shared__ uint32_t sh_carry_in;
 
     if (threadIdx.x == 0) sh_tile = (uint32_t)(atomicAdd(ticket, 1ull) - ticket_base);
@@ -722,71 +726,96 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
         z = D.z;
     }
     const int64_t n0 = (int64_t)tile * TILE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-    // coefficients n0-3 .. n0+TILE-1 into shared memory; a thread's four
-    // residues per prime are one 16-byte load when they lie inside the array
-    if constexpr (NP == 0) {
-        // direct mode: the coefficient values are given as three planes of
-        // 2^logM 64-bit words (low, middle, high word of each coefficient)
-#pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int idx = threadIdx.x * PER + q;
-            const uint64_t n = (uint64_t)(n0 + idx);
-            uint64_t c0 = 0, c1 = 0, c2 = 0;
-            if (n < L) crt_coeff<0>(res, logM, n, K, c0, c1, c2);
-            X0[idx + 3] = c0; X1[idx + 3] = c1; X2[idx + 3] = c2;
-        }
-    } else {
+    // this thread's coefficients n0 + 4t .. n0 + 4t + 3, kept in registers;
+    // a thread's four residues per prime are one 16-byte load when they lie
+    // inside the array
+    uint64_t c0[PER], c1[PER], c2[PER];
+    {
         const uint64_t nb = (uint64_t)(n0 + threadIdx.x * PER);
-        uint32_t y[PER][NP];
-        if (nb + PER <= ((uint64_t)1 << logM)) {
+        if constexpr (NP == 0) {
+            // direct mode: values given as three planes of 2^logM 64-bit words
 #pragma unroll
-            for (int jp = 0; jp < NP; jp++) {
-                const uint4 v = *reinterpret_cast<const uint4*>(res + ((size_t)jp << logM) + nb);
-                y[0][jp] = v.x; y[1][jp] = v.y; y[2][jp] = v.z; y[3][jp] = v.w;
+            for (int q = 0; q < PER; q++) {
+                c0[q] = c1[q] = c2[q] = 0;
+                if (nb + q < L) crt_coeff<0>(res, logM, nb + q, K, c0[q], c1[q], c2[q]);
             }
         } else {
+            uint32_t y[PER][NP];
+            if (nb + PER <= ((uint64_t)1 << logM)) {
 #pragma unroll
-            for (int q = 0; q < PER; q++)
+                for (int jp = 0; jp < NP; jp++) {
+                    const uint4 v = *reinterpret_cast<const uint4*>(res + ((size_t)jp << logM) + nb);
+                    y[0][jp] = v.x; y[1][jp] = v.y; y[2][jp] = v.z; y[3][jp] = v.w;
+                }
+            } else {
 #pragma unroll
-                for (int jp = 0; jp < NP; jp++)
-                    y[q][jp] = (nb + q < L) ? res[((size_t)jp << logM) + nb + q] : 0u;
-        }
+                for (int q = 0; q < PER; q++)
 #pragma unroll
-        for (int q = 0; q < PER; q++) {
-            const int idx = threadIdx.x * PER + q;
-            uint64_t c0 = 0, c1 = 0, c2 = 0;
-            if (nb + q < L) crt_values<NP>(y[q], K, c0, c1, c2);
-            X0[idx + 3] = c0; X1[idx + 3] = c1; X2[idx + 3] = c2;
+                    for (int jp = 0; jp < NP; jp++)
+                        y[q][jp] = (nb + q < L) ? res[((size_t)jp << logM) + nb + q] : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < PER; q++) {
+                c0[q] = c1[q] = c2[q] = 0;
+                if (nb + q < L) crt_values<NP>(y[q], K, c0[q], c1[q], c2[q]);
+            }
         }
     }
-    if (threadIdx.x < 3) {
-        const int64_t n = n0 - 3 + threadIdx.x;
-        uint64_t c0 = 0, c1 = 0, c2 = 0;
-        if (n >= 0 && (uint64_t)n < L) crt_coeff<NP>(res, logM, (uint64_t)n, K, c0, c1, c2);
-        X0[threadIdx.x] = c0; X1[threadIdx.x] = c1; X2[threadIdx.x] = c2;
+    if (lane == 31) {
+        uint64_t* w = wlast[warp + 1];
+        w[0] = c0[3]; w[1] = c1[3]; w[2] = c2[3]; w[3] = c1[2]; w[4] = c2[2]; w[5] = c2[1];
+    }
+    if (threadIdx.x == 0) {
+        // halo: coefficients n0 - 1, n0 - 2, n0 - 3 (zero before the product)
+        uint64_t h0[3] = {0, 0, 0}, h1[3] = {0, 0, 0}, h2[3] = {0, 0, 0};
+#pragma unroll
+        for (int d = 1; d <= 3; d++) {
+            const int64_t n = n0 - d;
+            if (n >= 0 && (uint64_t)n < L) crt_coeff<NP>(res, logM, (uint64_t)n, K, h0[d - 1], h1[d - 1], h2[d - 1]);
+        }
+        uint64_t* w = wlast[0];
+        w[0] = h0[0]; w[1] = h1[0]; w[2] = h2[0]; w[3] = h1[1]; w[4] = h2[1]; w[5] = h2[2];
     }
     __syncthreads();
+    // the previous thread's last three coefficients (shuffle, or the slot of
+    // the previous warp / the halo for lane 0)
+    uint64_t p0 = __shfl_up_sync(0xffffffffu, c0[3], 1);
+    uint64_t p1 = __shfl_up_sync(0xffffffffu, c1[3], 1);
+    uint64_t p2 = __shfl_up_sync(0xffffffffu, c2[3], 1);
+    uint64_t q1 = __shfl_up_sync(0xffffffffu, c1[2], 1);
+    uint64_t q2 = __shfl_up_sync(0xffffffffu, c2[2], 1);
+    uint64_t r2 = __shfl_up_sync(0xffffffffu, c2[1], 1);
+    if (lane == 0) {
+        const uint64_t* w = wlast[warp];
+        p0 = w[0]; p1 = w[1]; p2 = w[2]; q1 = w[3]; q2 = w[4]; r2 = w[5];
+    }
 
     // limb n receives s_n = X0[n] + X1[n-1] + X2[n-2] = lo_n + 2^64 cr_n (cr_n <= 2),
     // and then t_n = lo_n + cr_(n-1): a single-bit carry chain remains.
-    auto s_at = [&](int idx, uint64_t& lo) -> uint32_t {   // idx = n - n0 + 3
-        uint64_t s = X0[idx];
+    auto s3 = [](uint64_t a, uint64_t b, uint64_t c, uint64_t& lo) -> uint32_t {
+        uint64_t s = a;
         uint32_t cr = 0;
-        uint64_t t = s + X1[idx - 1]; cr += t < s; s = t;
-        t = s + X2[idx - 2]; cr += t < s; s = t;
+        uint64_t t = s + b; cr += t < s; s = t;
+        t = s + c; cr += t < s; s = t;
         lo = s;
         return cr;
     };
+    // X0, X1, X2 of coefficients 4t - 3 .. 4t + 3 relative to the thread
+    const uint64_t x0[5] = {p0, c0[0], c0[1], c0[2], c0[3]};               // coefficients 4t-1 .. 4t+3
+    const uint64_t x1[6] = {q1, p1, c1[0], c1[1], c1[2], c1[3]};           // 4t-2 .. 4t+3
+    const uint64_t x2[7] = {r2, q2, p2, c2[0], c2[1], c2[2], c2[3]};       // 4t-3 .. 4t+3
     uint64_t tv[PER];
     uint32_t gbits = 0, pbits = 0;
     {
-        const int idx0 = threadIdx.x * PER + 3;
         uint64_t lo_prev;
-        uint32_t cr_prev = (n0 + threadIdx.x * PER >= 1) ? s_at(idx0 - 1, lo_prev) : 0;
+        // s at limb 4t - 1: X0[4t-1] + X1[4t-2] + X2[4t-3]
+        uint32_t cr_prev = (n0 + threadIdx.x * PER >= 1) ? s3(x0[0], x1[0], x2[0], lo_prev) : 0;
+#pragma unroll
         for (int q = 0; q < PER; q++) {
             uint64_t lo;
-            const uint32_t cr = s_at(idx0 + q, lo);
+            const uint32_t cr = s3(x0[q + 1], x1[q + 1], x2[q + 1], lo);
             const uint64_t t = lo + cr_prev;
             const uint32_t g = t < lo;
             tv[q] = t;
@@ -803,7 +832,6 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
         Pt = Pt & pq;
     }
     // inclusive warp scan of (G, P)
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t Gi = Gt, Pi = Pt;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
@@ -857,11 +885,21 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
     }
     __syncthreads();
     uint32_t c = Ge | (Pe & sh_carry_in);
+    uint64_t v[PER];
+#pragma unroll
     for (int q = 0; q < PER; q++) {
-        const uint64_t n = (uint64_t)(n0 + threadIdx.x * PER + q);
-        const uint64_t v = tv[q] + c;
+        v[q] = tv[q] + c;
         c = ((gbits >> q) & 1) | (((pbits >> q) & 1) & c);
-        if (n < zn) z[n] = v;
+    }
+    const uint64_t nb = (uint64_t)(n0 + threadIdx.x * PER);
+    uint64_t* dst = z + nb;
+    if (nb + PER <= zn && ((uintptr_t)dst & 15) == 0) {
+        reinterpret_cast<ulonglong2*>(dst)[0] = make_ulonglong2(v[0], v[1]);
+        reinterpret_cast<ulonglong2*>(dst)[1] = make_ulonglong2(v[2], v[3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < PER; q++)
+            if (nb + q < zn) dst[q] = v[q];
     }
 }
 
