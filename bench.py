@@ -47,8 +47,10 @@ NS_LIMB_BITS = 64
 # proportion to the residue points, so a launch on another size scales by
 # M / 2^23.
 NCU_TRAFFIC_2P22 = {
-    "k_rows": 337.362944e6 + 122.715648e6,
-    "k_crt_carry": 167.829760e6 + 40.386304e6,
+    "k_fwd_cols": 67.559168e6 + 277.239040e6,
+    "k_rows": 337.119488e6 + 123.299328e6,
+    "k_inv_cols": 168.167680e6 + 108.828672e6,
+    "k_crt_carry": 167.904000e6 + 43.076608e6,
 }
 
 
@@ -562,9 +564,12 @@ def main():
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
     alg_pipeline = 208 * (an + bn)
     traffic = None
-    if dom in NCU_TRAFFIC_2P22 and args.workload in ("mpn24", "mpn22"):
+    if args.workload in ("mpn24", "mpn22"):
         scale = M / float(1 << 23)                # residue points relative to the capture
-        traffic = NCU_TRAFFIC_2P22[dom] * scale
+        for name, v in kern.items():
+            if name in NCU_TRAFFIC_2P22:
+                v["traffic"] = NCU_TRAFFIC_2P22[name] * scale
+        traffic = kern[dom].get("traffic")
     roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["GBps"], "peak": peak,
                 "unit": "GB/s", "frac": kern[dom]["GBps"] / peak, "traffic": traffic,
                 "peak_kind": peak_kind,
