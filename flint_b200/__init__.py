@@ -84,6 +84,8 @@ SIGNATURES = {
     "_gpu_mpn_ctx_mpn_mul_range": (None, [_CTX, _P, _U, _U, _P, _U, _P, _U]),
     "gpu_mpn_mul_device": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, _P]),
     "gpu_mpn_mul_device_noalloc": (ctypes.c_int, [_P, _P, _U, _P, _U, _P]),
+    "gpu_mpn_mul_range_device": (ctypes.c_int, [_CTX, _P, _U, _U, _P, _U, _P, _U, _P]),
+    "gpu_mpn_mulmid_default_mpn_ctx": (None, [_P, _P, _S, _P, _S, _S, _S]),
     "_gpu_nmod_poly_mul_mid_mpn_ctx": (None, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_mul_mid_status": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
@@ -303,7 +305,8 @@ class MpnCtx:
         return z
 
     def mpn_mul_range(self, lo, hi, a, b):
-        """limbs [lo, hi) of a * b (_mpn_ctx_mpn_mul_range, exact)."""
+        """limbs [lo, hi) of a * b (_mpn_ctx_mpn_mul_range): exact for lo = 0,
+        for lo > 0 a lower approximation short by at most 2 units."""
         a = _limbs(a)
         b = a if b is a else _limbs(b)
         z = np.empty(max(hi - lo, 0), dtype=np.uint64)
@@ -311,6 +314,10 @@ class MpnCtx:
             lib()._gpu_mpn_ctx_mpn_mul_range(self.ptr, z.ctypes.data, lo, hi, a.ctypes.data,
                                              len(a), b.ctypes.data, len(b))
         return z
+
+    def mpn_mul_range_device(self, z_ptr, lo, hi, a_ptr, an, b_ptr, bn, stream=None):
+        """Queue limbs [lo, hi) of a * b on device pointers (see mpn_mul_range)."""
+        _check(lib().gpu_mpn_mul_range_device(self.ptr, z_ptr, lo, hi, a_ptr, an, b_ptr, bn, stream))
 
     def mpn_mul_device(self, z_ptr, a_ptr, an, b_ptr, bn, stream=None):
         """Queue z = a * b on device pointers (ints); returns without syncing."""

@@ -680,7 +680,7 @@ static int mpn_mul_basecase_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint
     timing_mark(tr, 3, st);
     k_crt_carry<0, THREADS><<<tiles, THREADS, 0, st>>>((const uint32_t *)sums, logM, L, zn, z, X->crt[5],
                                                        X->d_status, X->d_ticket, X->ticket_base, X->epoch,
-                                                       X->d_err, nullptr, nullptr);
+                                                       X->d_err, nullptr, nullptr, 0ull);
     timing_mark(tr, 4, st);
     X->ticket_base += tiles;
     X->last_launches = 2;
@@ -688,15 +688,52 @@ static int mpn_mul_basecase_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint
     return 0;
 }
 
-// Enqueue z = a * b on `st` with device pointers (cfg NULL: default plan).
+// Cyclic length of a window product of limbs [lo, hi): coefficients
+// lo - 3 .. hi - 1 must be free of wrap-around (M >= L - lo + 3) and
+// addressable (M >= min(hi, L)), L = an + bn - 1.
+static int window_logM(uint64_t an, uint64_t bn, uint64_t lo, uint64_t hi)
+{
+    const uint64_t L = an + bn - 1;
+    const uint64_t need = std::max(std::min(hi, L), L + 3 > lo ? L + 3 - lo : 1);
+    return std::max(ceil_log2_u64(need), MIN_LOGM);
+}
+
+// Enqueue z = limbs [lo, hi) of a * b on `st` with device pointers (cfg NULL:
+// default plan; the default window is the whole product).  For lo > 0 the
+// carry chain starts at limb lo: the coefficients below lo add their words
+// that land in the window but not the carry that would ripple up from the
+// limbs below, so the result is a lower approximation of floor(a b / 2^(64 lo))
+// short by at most 2 units (and by 0 unless limb lo - 1 of the exact product
+// is within 2 of 2^64 - 1).  That is the contract of the reference's
+// _mpn_ctx_mpn_mul_range (lower approximation, deficit <= min(an, bn, lo)
+// 2^64, exact for lo = 0), and the result depends on a, b and lo only, not on
+// hi or the transform length.  A window far below the top uses a shorter
+// cyclic transform (window_logM).
 static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
                            const uint64_t *b, uint64_t bn, cudaStream_t st,
-                           const gpu_mul_config *cfg = nullptr)
+                           const gpu_mul_config *cfg = nullptr, uint64_t lo = 0, uint64_t hi = ~0ull)
 {
     MulPlan P;
     int rc = plan_mpn_cfg(an, bn, cfg, &P);
     if (rc) return rc;
-    if (P.route == GPU_MUL_ROUTE_BASECASE) return mpn_mul_basecase_enqueue(X, z, a, an, b, bn, P.logM, st);
+    const uint64_t zfull = an + bn;
+    hi = std::min(hi, zfull);
+    if (lo >= hi) return 0;
+    const bool window = lo > 0 || hi < zfull;
+    if (P.route == GPU_MUL_ROUTE_BASECASE) {
+        if (window) return set_error(GPU_FFT_SMALL_EINVAL, "the basecase route computes whole products only");
+        return mpn_mul_basecase_enqueue(X, z, a, an, b, bn, P.logM, st);
+    }
+    // limbs [lo, hi): the carry chain starts at lo; a shorter cyclic
+    // transform is used when the window allows one
+    const uint64_t base = lo;
+    if (lo > 0 && !(cfg && cfg->logM)) {
+        const int lw = window_logM(an, bn, lo, hi);
+        if (lw < P.logM) {
+            P.logM = lw;
+            P.L = make_shape(lw, cfg && cfg->logC && valid_logC(lw, cfg->logC) ? cfg->logC : -1);
+        }
+    }
     const bool sq = (a == b) && (an == bn);
     const int np = P.np, logM = P.logM;
     const size_t M = (size_t)1 << logM;
@@ -704,9 +741,9 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     rc = grow((void **)&X->d_res, &X->res_cap, res_bytes);
     if (rc) return rc;
     uint32_t *ra = X->d_res, *rb = X->d_res + (size_t)np * M;
-    const uint64_t zn = an + bn;
+    const uint64_t zn = hi;   // limbs produced: [base, hi)
     constexpr int THREADS = 256, TILE = 4 * THREADS;
-    const size_t tiles = (zn + TILE - 1) / TILE;
+    const size_t tiles = (zn - base + TILE - 1) / TILE;
     rc = ensure_status(X, tiles);
     if (rc) return rc;
     X->epoch = (X->epoch + 1) & 0x0fffffffu;
@@ -722,11 +759,11 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     if (np == 5)
         k_crt_carry<5, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
                                                           X->d_ticket, X->ticket_base, X->epoch, X->d_err,
-                                                          nullptr, nullptr);
+                                                          nullptr, nullptr, base);
     else
         k_crt_carry<6, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
                                                           X->d_ticket, X->ticket_base, X->epoch, X->d_err,
-                                                          nullptr, nullptr);
+                                                          nullptr, nullptr, base);
     launches++;
     timing_mark(tr, 4, st);
     X->ticket_base += tiles;
@@ -774,16 +811,19 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
     if (rc) return rc;
     const bool sq = (a == b) && (an == bn);
     const size_t zn = an + bn;
+    const gpu_ulong top = std::min<gpu_ulong>(hi, zn);
+    const size_t nz = top > lo ? top - lo : 0;
     uint64_t *buf;
-    rc = io_buffers(X, (sq ? an : an + bn) + zn, &buf);
+    rc = io_buffers(X, (sq ? an : an + bn) + nz, &buf);
     if (rc) return rc;
     uint64_t *da = buf, *db = sq ? buf : buf + an, *dz = buf + (sq ? an : an + bn);
-    CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, X->stream));
-    if (!sq) CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, X->stream));
-    rc = mpn_mul_enqueue(X, dz, da, an, db, bn, X->stream);
-    if (rc) return rc;
-    const gpu_ulong top = std::min<gpu_ulong>(hi, zn);
-    if (top > lo) CU(cudaMemcpyAsync(z, dz + lo, (top - lo) * 8, cudaMemcpyDeviceToHost, X->stream));
+    if (nz) {
+        CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, X->stream));
+        if (!sq) CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, X->stream));
+        rc = mpn_mul_enqueue(X, dz, da, an, db, bn, X->stream, nullptr, lo, top);
+        if (rc) return rc;
+        CU(cudaMemcpyAsync(z, dz, nz * 8, cudaMemcpyDeviceToHost, X->stream));
+    }
     rc = check_device_error(X);
     if (rc) return rc;
     if (hi > zn) memset(z + (zn > lo ? zn - lo : 0), 0, (hi - std::max<gpu_ulong>(zn, lo)) * 8);
@@ -887,6 +927,25 @@ int gpu_mpn_mul_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *
     int rc = bind_device(X);
     if (rc) return rc;
     return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn, (cudaStream_t)stream, cfg);
+}
+
+int gpu_mpn_mul_range_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong lo, gpu_ulong hi,
+                             const uint64_t *a_dev, gpu_ulong an, const uint64_t *b_dev, gpu_ulong bn,
+                             void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn, (cudaStream_t)stream, nullptr, lo, hi);
+}
+
+void gpu_mpn_mulmid_default_mpn_ctx(gpu_ulong *z, const gpu_ulong *a, gpu_slong an, const gpu_ulong *b,
+                                    gpu_slong bn, gpu_slong zlo, gpu_slong zhi)
+{
+    _gpu_mpn_ctx_mpn_mul_range(gpu_get_default_mpn_ctx(), z, (gpu_ulong)zlo, (gpu_ulong)zhi, a,
+                               (gpu_ulong)an, b, (gpu_ulong)bn);
 }
 
 int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
@@ -1517,7 +1576,7 @@ int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong
                       D.scale + (size_t)logM * MAX_NP, st, nullptr);
     k_crt_carry<NA_NP, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, L, zn, z_dev, D.ctx.crt[NA_NP],
                                                           D.status, D.ticket, 0ull, 1u, D.err,
-                                                          nullptr, nullptr);
+                                                          nullptr, nullptr, 0ull);
     return cudaGetLastError() == cudaSuccess ? GPU_FFT_SMALL_OK : GPU_FFT_SMALL_ECUDA;
 }
 

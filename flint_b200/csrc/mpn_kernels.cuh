@@ -696,7 +696,8 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
             uint64_t* __restrict__ z, CrtConst K, uint32_t* __restrict__ status,
             unsigned long long* __restrict__ ticket, unsigned long long ticket_base,
             uint32_t epoch, int* __restrict__ err,
-            const InstDesc* __restrict__ desc, const uint32_t* __restrict__ tile_inst)
+            const InstDesc* __restrict__ desc, const uint32_t* __restrict__ tile_inst,
+            uint64_t base)
 {
     constexpr int PER = 4;
     constexpr int TILE = PER * THREADS;
@@ -725,7 +726,14 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
         zn = D.an + D.bn;
         z = D.z;
     }
-    const int64_t n0 = (int64_t)tile * TILE;
+    // coefficient / limb index of the tile's first position: a window product
+    // starts at limb `base` (z[0] is limb base; limbs below it are not
+    // produced and their carry into the window is not added -- the lower
+    // approximation of a windowed product)
+    const int64_t n0 = (int64_t)base + (int64_t)tile * TILE;
+    // limbs below zn need coefficients below zn only; a window's transform
+    // length covers min(L, zn) coefficients, not necessarily L
+    L = L < zn ? L : zn;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     // this thread's coefficients n0 + 4t .. n0 + 4t + 3, kept in registers;
@@ -743,7 +751,9 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
             }
         } else {
             uint32_t y[PER][NP];
-            if (nb + PER <= ((uint64_t)1 << logM)) {
+            // 16-byte loads need nb % 4 == 0 (always true for whole products; a
+            // window may start at any limb) and the four residues inside the array
+            if ((nb & 3) == 0 && nb + PER <= ((uint64_t)1 << logM)) {
 #pragma unroll
                 for (int jp = 0; jp < NP; jp++) {
                     const uint4 v = *reinterpret_cast<const uint4*>(res + ((size_t)jp << logM) + nb);
@@ -892,7 +902,7 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
         c = ((gbits >> q) & 1) | (((pbits >> q) & 1) & c);
     }
     const uint64_t nb = (uint64_t)(n0 + threadIdx.x * PER);
-    uint64_t* dst = z + nb;
+    uint64_t* dst = z + (nb - base);
     if (nb + PER <= zn && ((uintptr_t)dst & 15) == 0) {
         reinterpret_cast<ulonglong2*>(dst)[0] = make_ulonglong2(v[0], v[1]);
         reinterpret_cast<ulonglong2*>(dst)[1] = make_ulonglong2(v[2], v[3]);

@@ -85,14 +85,31 @@ GPU_FFT_SMALL_API int gpu_mpn_ctx_mpn_mul_status(gpu_mpn_ctx_t R, gpu_ulong *z,
                                const gpu_ulong *a, gpu_ulong an,
                                const gpu_ulong *b, gpu_ulong bn);
 
-/* Limbs [lo, hi) of a * b into z[0, hi-lo).  Replaces _mpn_ctx_mpn_mul_range
-   (src/fft_small.h:462, src/fft_small/mpn_mul.c:1617-1978).  The reference
-   returns, for lo > 0, a lower approximation with a bounded deficit; this
-   implementation returns the exact limbs, which satisfies that contract. */
+/* Limbs [lo, hi) of a * b into z[0, hi-lo), zero beyond an + bn.  Replaces
+   _mpn_ctx_mpn_mul_range (src/fft_small.h:462, src/fft_small/mpn_mul.c:
+   1617-1978) with its contract (src/fft_small/test/t-mpn_mulmid.c): exact for
+   lo = 0; for lo > 0 a lower approximation of floor(a b / 2^(64 lo)) that
+   depends on a, b and lo only (not on hi), here short by at most 2 units --
+   the carry rippling up from the limbs below lo is not added, and is zero
+   unless limb lo - 1 of the exact product is within 2 of 2^64 - 1.  A window
+   well below the top of the product runs a shorter cyclic transform. */
 GPU_FFT_SMALL_API void _gpu_mpn_ctx_mpn_mul_range(gpu_mpn_ctx_t R, gpu_ulong *z,
                                 gpu_ulong lo, gpu_ulong hi,
                                 const gpu_ulong *a, gpu_ulong an,
                                 const gpu_ulong *b, gpu_ulong bn);
+
+/* Device-pointer twin of _gpu_mpn_ctx_mpn_mul_range: limbs [lo, hi) of a * b
+   into z_dev[0, min(hi, an+bn) - lo) on `stream` (no zero fill; hi is
+   clamped to an + bn). */
+GPU_FFT_SMALL_API int gpu_mpn_mul_range_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong lo, gpu_ulong hi,
+                                               const uint64_t *a_dev, gpu_ulong an,
+                                               const uint64_t *b_dev, gpu_ulong bn, void *stream);
+/* Same signature as flint_mpn_mulmid_fft_small (src/mpn_extras.h:686,
+   src/mpn_extras/mulmid_fft_small.c:26-31): the window [zlo, zhi) on the
+   calling thread's default context. */
+GPU_FFT_SMALL_API void gpu_mpn_mulmid_default_mpn_ctx(gpu_ulong *z, const gpu_ulong *a, gpu_slong an,
+                                                      const gpu_ulong *b, gpu_slong bn, gpu_slong zlo,
+                                                      gpu_slong zhi);
 
 /* Device-pointer twin of gpu_mpn_ctx_mpn_mul: a, b, z are device addresses,
    the work is queued on `stream` (a cudaStream_t; NULL is CUDA's default

@@ -369,3 +369,39 @@ def ref_fmpz_poly_mul_raw(a_raw, b_raw, zw):
         B.set_raw(b_raw)
         L._fmpz_poly_mul(Z.ptr, A.ptr, an, B.ptr, bn)
         return Z.get_raw(zw)
+
+
+def ref_mpn_mul_range(lo, hi, a, b):
+    """The reference's _mpn_ctx_mpn_mul_range (src/fft_small/mpn_mul.c:1617-1978)
+    on its default context: limbs [lo, hi) of a * b, a lower approximation
+    for lo > 0."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = a if b is a else np.ascontiguousarray(b, dtype=np.uint64)
+    if len(a) < len(b):
+        a, b = b, a
+    L = ref()
+    if not getattr(L, "_range_ready", False):
+        P, U = ctypes.c_void_p, ctypes.c_ulong
+        L._mpn_ctx_mpn_mul_range.argtypes = [P, P, U, U, P, U, P, U]
+        L._mpn_ctx_mpn_mul_range.restype = None
+        L._range_ready = True
+    z = np.zeros(max(hi - lo, 0), dtype=np.uint64)
+    if hi > lo:
+        L._mpn_ctx_mpn_mul_range(L.get_default_mpn_ctx(), z.ctypes.data, lo, hi, a.ctypes.data,
+                                 len(a), b.ctypes.data, len(b))
+    return z
+
+
+def check_mul_range_contract(a, b, lo, z):
+    """The contract of _mpn_ctx_mpn_mul_range (src/fft_small/test/t-mpn_mulmid.c:
+    96-117) for z = limbs [lo, an + bn): a lower approximation of
+    floor(a b / 2^(64 lo)) with deficit <= min(an, bn, lo) 2^64, exact for
+    lo = 0.  Returns the deficit."""
+    an, bn = len(a), len(b)
+    exact = (to_int(a) * to_int(b)) >> (64 * lo)
+    d = exact - to_int(z)
+    assert d >= 0, "not a lower approximation"
+    assert d <= min(an, bn, lo) << 64, "deficit exceeds min(an, bn, lo) 2^64"
+    if lo == 0:
+        assert d == 0, "lo = 0 must be exact"
+    return d

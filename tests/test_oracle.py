@@ -158,3 +158,14 @@ def test_mlp_oracle_gradient_matches_finite_differences():
         Pm[k] -= h
         fd = (mlp_ref.loss(Pp, X, t) - mlp_ref.loss(Pm, X, t)) / (2 * h)
         assert abs(fd - g[k]) <= 1e-6 + 1e-5 * abs(fd), (k, fd, g[k])
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference not built")
+@pytest.mark.parametrize("an,bn,lo", [(300, 200, 0), (300, 200, 250), (4000, 3999, 1),
+                                      (4000, 1000, 4990), (20000, 10000, 10000)])
+def test_reference_range_contract(an, bn, lo):
+    """The contract the GPU window product is held to, checked on the
+    reference's own _mpn_ctx_mpn_mul_range output (pins the checker)."""
+    a, b = O.rand_limbs(an * 3 + lo, an), O.rand_limbs(bn * 5 + lo, bn)
+    z = O.ref_mpn_mul_range(lo, an + bn, a, b)
+    O.check_mul_range_contract(a, b, lo, z)
