@@ -118,6 +118,19 @@ SIGNATURES = {
     "gpu_mlp_train": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_float, ctypes.c_ulonglong, _P]),
     "gpu_mlp_clear": (None, [_P]),
+    "gpu_fft_plan_init_mpn": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _U, _U, _U, ctypes.c_int]),
+    "gpu_fft_plan_init_nmod": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _U, _U, _U, _U, _U, _Nmod]),
+    "gpu_fft_plan_info": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
+    "gpu_fft_plan_clear": (None, [_P]),
+    "gpu_fft_op_init": (ctypes.c_int, [ctypes.POINTER(_P), _P]),
+    "gpu_fft_op_clear": (None, [_P]),
+    "gpu_fft_fft_mpn": (ctypes.c_int, [_P, _P, _U, _P, _P]),
+    "gpu_fft_fft_nmod": (ctypes.c_int, [_P, _P, _U, _P, _P]),
+    "gpu_fft_op_pointwise": (ctypes.c_int, [ctypes.c_int, _P, _P, _P, _P, _P]),
+    "gpu_fft_ifft": (ctypes.c_int, [_P, _P, _P]),
+    "gpu_fft_export_mpn": (ctypes.c_int, [_P, _U, _P, _P, _P]),
+    "gpu_fft_export_nmod": (ctypes.c_int, [_P, _U, _U, _P, _Nmod, _P, _P]),
+    "gpu_fft_op_check": (ctypes.c_int, [_P, _P]),
     "gpu_mpn_batch_init": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, ctypes.c_size_t, _P]),
     "gpu_mpn_batch_init_config": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _P, _P, ctypes.c_size_t,
                                                  _P]),
@@ -440,6 +453,91 @@ class MpnBatch:
 
     def __exit__(self, *exc):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+OP_MUL, OP_SQR, OP_ADDMUL, OP_SUBMUL, OP_ADD, OP_SUB, OP_NEG = range(7)
+
+
+class FftPlan:
+    """A plan of the transformed-operand API (gpu_fft_plan_*; the reference's
+    fft_small_plan_init_mpn / _nmod).  Build with FftPlan.mpn(...) or
+    FftPlan.nmod(...); operands are FftOp objects of the plan."""
+
+    def __init__(self, ctx, handle, kind, mod=None):
+        self.ctx, self._h, self.kind, self.mod = ctx, handle, kind, mod
+        np_, lm = ctypes.c_int(), ctypes.c_int()
+        _check(lib().gpu_fft_plan_info(self._h, ctypes.byref(np_), ctypes.byref(lm)))
+        self.np, self.logM = np_.value, lm.value
+
+    @classmethod
+    def mpn(cls, ctx, an_max, bn_max, len_bound=None, is_signed=False):
+        h = ctypes.c_void_p()
+        lb = len_bound if len_bound is not None else min(an_max, bn_max)
+        _check(lib().gpu_fft_plan_init_mpn(ctypes.byref(h), ctx.ptr, an_max, bn_max, lb,
+                                           1 if is_signed else 0))
+        return cls(ctx, h, "mpn")
+
+    @classmethod
+    def nmod(cls, ctx, zl, zh, zn, n, len_bound, prod_bits=None):
+        h = ctypes.c_void_p()
+        pb = prod_bits if prod_bits is not None else 2 * (int(n) - 1).bit_length()
+        _check(lib().gpu_fft_plan_init_nmod(ctypes.byref(h), ctx.ptr, zl, zh, zn, len_bound, pb,
+                                            _Nmod(n, 0, 0)))
+        return cls(ctx, h, "nmod", n)
+
+    def op(self):
+        return FftOp(self)
+
+    def pointwise(self, op, Z, A, B=None, stream=None):
+        _check(lib().gpu_fft_op_pointwise(op, Z._h, A._h, (B or A)._h, self._h, stream))
+
+    def check(self, stream=None):
+        _check(lib().gpu_fft_op_check(self._h, stream))
+
+    def close(self):
+        if self._h:
+            lib().gpu_fft_plan_clear(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FftOp:
+    """A transformed operand (gpu_fft_op_*), resident in device memory."""
+
+    def __init__(self, plan):
+        self.plan = plan
+        self._h = ctypes.c_void_p()
+        _check(lib().gpu_fft_op_init(ctypes.byref(self._h), plan._h))
+
+    def fft(self, a_ptr, an, stream=None):
+        f = lib().gpu_fft_fft_mpn if self.plan.kind == "mpn" else lib().gpu_fft_fft_nmod
+        _check(f(self._h, a_ptr, an, self.plan._h, stream))
+
+    def ifft(self, stream=None):
+        _check(lib().gpu_fft_ifft(self._h, self.plan._h, stream))
+
+    def export_mpn(self, z_ptr, zn, stream=None):
+        _check(lib().gpu_fft_export_mpn(z_ptr, zn, self._h, self.plan._h, stream))
+
+    def export_nmod(self, z_ptr, zl, zh, stream=None):
+        _check(lib().gpu_fft_export_nmod(z_ptr, zl, zh, self._h, _Nmod(self.plan.mod, 0, 0),
+                                         self.plan._h, stream))
+
+    def close(self):
+        if self._h:
+            lib().gpu_fft_op_clear(self._h)
+            self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:

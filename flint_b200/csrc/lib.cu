@@ -9,6 +9,7 @@
 #include "fmpz_kernels.cuh"
 #include "basecase_kernels.cuh"
 #include "mlp_kernels.cuh"
+#include "op_kernels.cuh"
 
 #include <cuda_runtime.h>
 #include <math.h>
@@ -331,6 +332,15 @@ static const rows_fn ROWS[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                                  k_rows<5>, k_rows<6>, k_rows<7>, k_rows<8>, k_rows<9>,
                                  k_rows<10>, k_rows<11>, k_rows<12>, k_rows<13>, k_rows<14>};
 #undef FB_COLS
+typedef void (*rows_op_fn)(DevTables, uint32_t *, int, int, int);
+static const rows_op_fn ROWS_FWD[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
+                                        k_rows_fwd<5>, k_rows_fwd<6>, k_rows_fwd<7>, k_rows_fwd<8>,
+                                        k_rows_fwd<9>, k_rows_fwd<10>, k_rows_fwd<11>, k_rows_fwd<12>,
+                                        k_rows_fwd<13>, k_rows_fwd<14>};
+static const rows_op_fn ROWS_INV[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
+                                        k_rows_inv<5>, k_rows_inv<6>, k_rows_inv<7>, k_rows_inv<8>,
+                                        k_rows_inv<9>, k_rows_inv<10>, k_rows_inv<11>, k_rows_inv<12>,
+                                        k_rows_inv<13>, k_rows_inv<14>};
 
 constexpr int MIN_LOGM = 5;
 
@@ -394,8 +404,11 @@ static int configure_kernels()
         CU(cudaFuncSetAttribute(FWD_COLS_FZ[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
         CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
-    for (int c = 5; c <= LOG_MAXC; c++)
+    for (int c = 5; c <= LOG_MAXC; c++) {
         CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+        CU(cudaFuncSetAttribute(ROWS_FWD[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(ROWS_INV[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    }
     done = true;
     return 0;
 }
@@ -845,6 +858,10 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 // ---------------------------------------------------------------------------
 // cost model of the learned schedule
 #include "mlp_host.inc"
+
+// ---------------------------------------------------------------------------
+// plans and transformed operands
+#include "op_host.inc"
 
 // ---------------------------------------------------------------------------
 // C ABI

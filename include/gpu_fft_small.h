@@ -305,6 +305,69 @@ GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device(gpu_mpn_ctx_t R, uint64_t *z_
                                                    const uint64_t *b_dev, gpu_ulong bw, gpu_ulong bn,
                                                    void *stream);
 
+/* --- plans and transformed operands ------------------------------------------
+
+   The reference's plan / op API (src/fft_small.h:466-700, src/fft_small/op.c):
+   a plan fixes the primes, the transform length and the output window; an
+   op holds one operand's forward transforms, resident in device memory
+   (np vectors of 2^logM words), so an operand transformed once can be
+   combined with many others.  Forward transforms are in the PRIMAL domain;
+   mul / sqr / addmul / submul produce the PRODUCT domain (normalisation
+   folded in once); add / sub need both operands in the same domain.  All
+   data pointers are device pointers and every call is queued on `stream`
+   (NULL = CUDA's default stream); gpu_fft_op_check synchronises and
+   reports a kernel error. */
+typedef struct gpu_fft_plan_struct *gpu_fft_plan_t;
+typedef struct gpu_fft_op_struct *gpu_fft_op_t;
+
+#define GPU_FFT_OP_MUL     0   /* Z = A B         */
+#define GPU_FFT_OP_SQR     1   /* Z = A^2         */
+#define GPU_FFT_OP_ADDMUL  2   /* Z = Z + A B     */
+#define GPU_FFT_OP_SUBMUL  3   /* Z = Z - A B     */
+#define GPU_FFT_OP_ADD     4   /* Z = A + B       */
+#define GPU_FFT_OP_SUB     5   /* Z = A - B       */
+#define GPU_FFT_OP_NEG     6   /* Z = -A          */
+
+/* fft_small_plan_init_mpn (src/fft_small.h:577-579): integer operands of at
+   most an_max and bn_max limbs, at most len_bound elementary products
+   accumulated per coefficient; is_signed adds the reference's spare factor
+   two.  Returns 0, GPU_FFT_SMALL_ENOPRIMES or GPU_FFT_SMALL_ETOOBIG. */
+GPU_FFT_SMALL_API int gpu_fft_plan_init_mpn(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, gpu_ulong an_max,
+                                            gpu_ulong bn_max, gpu_ulong len_bound, int is_signed);
+/* fft_small_plan_init_nmod (src/fft_small.h:559-561): the window [zl, zh) of
+   a length-zn convolution over Z/nZ, len_bound products of absolute value
+   below 2^prod_bits per output coefficient. */
+GPU_FFT_SMALL_API int gpu_fft_plan_init_nmod(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, gpu_ulong zl, gpu_ulong zh,
+                                             gpu_ulong zn, gpu_ulong len_bound, gpu_ulong prod_bits,
+                                             gpu_nmod_t mod);
+GPU_FFT_SMALL_API int gpu_fft_plan_info(gpu_fft_plan_t P, int *np, int *logM);
+GPU_FFT_SMALL_API void gpu_fft_plan_clear(gpu_fft_plan_t P);
+/* fft_small_op_init / fft_small_op_clear */
+GPU_FFT_SMALL_API int gpu_fft_op_init(gpu_fft_op_t *X, gpu_fft_plan_t P);
+GPU_FFT_SMALL_API void gpu_fft_op_clear(gpu_fft_op_t X);
+/* fft_small_fft_mpn / fft_small_fft_nmod: forward transforms of a (an limbs
+   or coefficients; nmod coefficients reduced mod n) into X */
+GPU_FFT_SMALL_API int gpu_fft_fft_mpn(gpu_fft_op_t X, const uint64_t *a_dev, gpu_ulong an,
+                                      gpu_fft_plan_t P, void *stream);
+GPU_FFT_SMALL_API int gpu_fft_fft_nmod(gpu_fft_op_t X, const uint64_t *a_dev, gpu_ulong an,
+                                       gpu_fft_plan_t P, void *stream);
+/* fft_small_op_mul / _sqr / _addmul / _submul / _add / _sub / _neg
+   (op = GPU_FFT_OP_*; B is ignored by SQR and NEG; Z may alias A or B) */
+GPU_FFT_SMALL_API int gpu_fft_op_pointwise(int op, gpu_fft_op_t Z, gpu_fft_op_t A, gpu_fft_op_t B,
+                                           gpu_fft_plan_t P, void *stream);
+/* fft_small_ifft: inverse transform in place */
+GPU_FFT_SMALL_API int gpu_fft_ifft(gpu_fft_op_t X, gpu_fft_plan_t P, void *stream);
+/* fft_small_export_mpn: the low zn limbs of the accumulated integer
+   (reduced mod 2^(64 zn) if it does not fit) */
+GPU_FFT_SMALL_API int gpu_fft_export_mpn(uint64_t *z_dev, gpu_ulong zn, gpu_fft_op_t X, gpu_fft_plan_t P,
+                                         void *stream);
+/* fft_small_export_nmod_range: coefficients [zl, zh) mod n (inside the plan's
+   window) */
+GPU_FFT_SMALL_API int gpu_fft_export_nmod(uint64_t *z_dev, gpu_ulong zl, gpu_ulong zh, gpu_fft_op_t X,
+                                          gpu_nmod_t mod, gpu_fft_plan_t P, void *stream);
+/* Synchronises `stream`; GPU_FFT_SMALL_ETIMEOUT if a carry wait gave up. */
+GPU_FFT_SMALL_API int gpu_fft_op_check(gpu_fft_plan_t P, void *stream);
+
 /* --- batches of uneven products (no counterpart in the reference, which
        multiplies one product per mpn_ctx_mpn_mul call, src/fft_small.h:433) */
 
