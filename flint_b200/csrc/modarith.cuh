@@ -103,10 +103,11 @@ FB_HD uint32_t limb_redc(uint64_t x, uint32_t p, uint32_t pneg_inv, uint32_t c32
 
 #ifdef __CUDACC__
 // Pipe balancing.  Integer adds, compares and min/max issue to the ALU pipe;
-// IMAD issues to the FMA pipe.  Both run at half the issue rate, and the
-// butterflies below are ALU-heavy, so some additions are written as
-// x * one + y with `one` an opaque constant-memory 1 that the compiler cannot
-// fold, which keeps them on the FMA pipe.
+// IMAD issues to the FMA pipe.  Both run at half the issue rate, so an
+// addition can be moved to the FMA pipe by writing it as x * one + y with
+// `one` an opaque constant-memory 1 that the compiler cannot fold.  The
+// butterflies take the number of such additions as a template parameter;
+// the kernels' choices are measured (ntt_smem.cuh).
 __constant__ uint32_t c_one;        // 1
 __constant__ uint32_t c_minus_one;  // 0xffffffff
 

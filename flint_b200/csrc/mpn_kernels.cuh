@@ -387,7 +387,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
                 xr[m] = sa[pb + m];
                 breg[m] = sb[pb + m];
             }
-            gs_contig2<5>(xr, breg, c_w32[j], p);
+            gs_contig2<5, ROW_GS_FMA_ADDS>(xr, breg, c_w32[j], p);
             __syncthreads();   // b fully read: refill it for the next item
             if (g2 < total) rows_prefetch<LOGC>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
             else cp_async_commit();
@@ -395,7 +395,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
             gs_strided_all<LOGC, 0>(sa, nv, twf, p);
 #pragma unroll
             for (int m = 0; m < 32; m++) xr[m] = sa[pb + m];
-            gs_contig<5>(xr, c_w32[j], p);
+            gs_contig<5, ROW_GS_FMA_ADDS>(xr, c_w32[j], p);
             cp_async_commit();
         }
         const uint32_t sc = scale[j];
@@ -404,7 +404,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
             const uint32_t y = squaring ? xr[m] : breg[m];
             xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
         }
-        ct_contig<5, 3>(xr, c_w32[j], p);
+        ct_contig<5, ROW_CT_FMA_ADDS>(xr, c_w32[j], p);
 #pragma unroll
         for (int m = 0; m < 32; m++) sa[pb + m] = xr[m];
         __syncthreads();

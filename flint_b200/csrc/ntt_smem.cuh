@@ -16,8 +16,8 @@
 //   * the contiguous pass (the five levels h = 16..1): each thread owns 32
 //     consecutive positions; its twiddles are powers of w_32, the same for
 //     every thread, and come from constant memory.
-// Row passes (G == 0) route two (forward) or three (inverse) additions per
-// butterfly to the FMA pipe, column passes COL_FMA_ADDS (see bfly_gs).
+// How many additions per butterfly go to the FMA pipe is set per pass kind
+// (ROW_GS_FMA_ADDS, ROW_CT_FMA_ADDS, COL_FMA_ADDS; see bfly_gs).
 // Shared memory holds one pad word per 32 (physical = a + a/32), which makes
 // both kinds of pass conflict-free and lets every address be a per-thread
 // base plus a compile-time offset.
@@ -35,7 +35,23 @@
 namespace fb {
 
 constexpr int MAX_NP = 7;
-constexpr int COL_FMA_ADDS = 0;   // additions per column butterfly on the FMA pipe
+// Additions per butterfly sent to the FMA pipe: column passes, row forward
+// (Gentleman-Sande) passes, row inverse (Cooley-Tukey) passes.  Measured on
+// the B200 (2^24 x 2^24 product): every kernel is fastest with all additions
+// on the ALU pipe (row pass 1.98 ms with 2/3 FMA additions, 1.74 ms with
+// none); the FMA pipe is left to the multiplications.
+#ifndef FB_COL_FMA_ADDS
+#define FB_COL_FMA_ADDS 0
+#endif
+#ifndef FB_ROW_GS_FMA_ADDS
+#define FB_ROW_GS_FMA_ADDS 0
+#endif
+#ifndef FB_ROW_CT_FMA_ADDS
+#define FB_ROW_CT_FMA_ADDS 0
+#endif
+constexpr int COL_FMA_ADDS = FB_COL_FMA_ADDS;
+constexpr int ROW_GS_FMA_ADDS = FB_ROW_GS_FMA_ADDS;
+constexpr int ROW_CT_FMA_ADDS = FB_ROW_CT_FMA_ADDS;
 
 __host__ __device__ constexpr int padw(int a) { return a + (a >> 5); }
 
@@ -228,7 +244,7 @@ __device__ __forceinline__ void gs_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
-        gs_strided<Q, H, (G == 0 ? 2 : COL_FMA_ADDS)>(x, tw, jj0, p);
+        gs_strided<Q, H, (G == 0 ? ROW_GS_FMA_ADDS : COL_FMA_ADDS)>(x, tw, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
     }
@@ -257,7 +273,7 @@ __device__ __forceinline__ void gs_pass_smem2(uint32_t* sx, uint32_t* sy, int nv
             x[m] = sx[pb + m * PSTEP];
             y[m] = sy[pb + m * PSTEP];
         }
-        gs_strided_level2<Q, H, 0, 2>(x, y, tw, jj0, p);
+        gs_strided_level2<Q, H, 0, ROW_GS_FMA_ADDS>(x, y, tw, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) {
             sx[pb + m * PSTEP] = x[m];
@@ -286,7 +302,7 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
-        ct_strided<Q, H, (G == 0 ? 3 : COL_FMA_ADDS)>(x, twi, jj0, p);
+        ct_strided<Q, H, (G == 0 ? ROW_CT_FMA_ADDS : COL_FMA_ADDS)>(x, twi, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
     }
