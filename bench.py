@@ -408,6 +408,41 @@ def batch_cpu_baseline(sizes, host, spans, seconds):
             "sample": "first %d of the %d products, one mpn_ctx_mpn_mul each" % (k, len(spans))}
 
 
+def bench_precomp(torch, FB, ctx, dev, stream, steps):
+    """Transformed-operand reuse (the reference's op API): b of 2^22 limbs
+    transformed once, then for each a of 2^22 limbs: forward transform of a,
+    pointwise product, inverse, export -- against the full product."""
+    n = 1 << 22
+    g = torch.Generator(device=dev)
+    g.manual_seed(123)
+    a = torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64, device=dev, generator=g)
+    b = torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64, device=dev, generator=g)
+    z1 = torch.empty(2 * n, dtype=torch.int64, device=dev)
+    z2 = torch.empty_like(z1)
+    s = stream.cuda_stream
+    P = FB.FftPlan.mpn(ctx, n, n)
+    A, B, Z = P.op(), P.op(), P.op()
+    B.fft(b.data_ptr(), n, s)
+
+    def with_op():
+        A.fft(a.data_ptr(), n, s)
+        P.pointwise(FB.OP_MUL, Z, A, B, s)
+        Z.ifft(s)
+        Z.export_mpn(z1.data_ptr(), 2 * n, s)
+
+    ms_op = time_on_stream(torch, stream, with_op, steps, 3)
+    ms_full = time_on_stream(torch, stream, lambda: ctx.mpn_mul_device(z2.data_ptr(), a.data_ptr(), n,
+                                                                       b.data_ptr(), n, s), steps, 3)
+    P.check(s)
+    same = bool(torch.equal(z1, z2))
+    for o in (A, B, Z):
+        o.close()
+    P.close()
+    return {"workload": "a x b, 2^22 x 2^22 limbs, b transformed once (plan/op API)",
+            "ms_with_transformed_b": ms_op, "ms_full_product": ms_full,
+            "speedup": ms_full / ms_op, "identical": same}
+
+
 def kernel_bytes(name, an, bn, np_, M, L):
     """Algorithmic bytes each kernel must move in the four-pass design:
     residues are 4-byte words, np primes, M-point transforms."""
@@ -539,6 +574,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     batch = stream_res = None
+    precomp = bench_precomp(torch, FB, ctx, dev, stream, max(3, args.steps // 2))
     cpu_s = 0.0 if (world > 1 or args.no_cpu_baseline) else 10.0
     if not (args.no_batch and args.stream_requests == 0):
         model, tun, train_info = train_cost_model(ctx)
@@ -604,6 +640,7 @@ def main():
         "clocks": clk,
         "batch": batch,
         "stream": stream_res,
+        "transformed_operand": precomp,
     }
     print(json.dumps(line), flush=True)
     if dist:
