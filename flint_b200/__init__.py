@@ -88,6 +88,8 @@ SIGNATURES = {
     "gpu_mpn_mulmid_default_mpn_ctx": (None, [_P, _P, _S, _P, _S, _S, _S]),
     "_gpu_nmod_poly_mul_mid_mpn_ctx": (None, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_mul_mid_status": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
+    "_gpu_nmod_poly_divrem_mpn_ctx": (None, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
+    "_gpu_nmod_poly_divrem_status": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
     "gpu_mpn_mul_default_mpn_ctx": (None, [_P, _P, _S, _P, _S]),
     "_gpu_nmod_poly_mul_mid_default_mpn_ctx": (None, [_P, _S, _S, _P, _S, _P, _S, _Nmod]),
@@ -392,6 +394,15 @@ class MpnCtx:
                                               ctypes.byref(cfg) if cfg is not None else None,
                                               copies, reps, ctypes.byref(ms)))
         return ms.value
+
+    def nmod_poly_divrem(self, a, b, n):
+        """(q, r) with a = q b + r mod n, deg r < deg b (_nmod_poly_divrem_mpn_ctx)."""
+        a, b = _limbs(a), _limbs(b)
+        q = np.empty(len(a) - len(b) + 1, dtype=np.uint64)
+        r = np.empty(len(b) - 1, dtype=np.uint64)
+        _check(lib()._gpu_nmod_poly_divrem_status(q.ctypes.data, r.ctypes.data, a.ctypes.data, len(a),
+                                                  b.ctypes.data, len(b), _Nmod(n, 0, 0), self.ptr))
+        return q, r
 
     @property
     def last_launches(self):

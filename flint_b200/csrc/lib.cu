@@ -972,6 +972,19 @@ int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
     return nmod_mul_mid_host(get_ctx(R), z, zl, zh, a, an, b, bn, mod.n);
 }
 
+int _gpu_nmod_poly_divrem_status(gpu_ulong *q, gpu_ulong *r, const gpu_ulong *a, gpu_ulong an,
+                                 const gpu_ulong *b, gpu_ulong bn, gpu_nmod_t mod, gpu_mpn_ctx_t R)
+{
+    return nmod_divrem_host(get_ctx(R), q, r, a, an, b, bn, mod.n);
+}
+
+void _gpu_nmod_poly_divrem_mpn_ctx(gpu_ulong *q, gpu_ulong *r, const gpu_ulong *a, gpu_ulong an,
+                                   const gpu_ulong *b, gpu_ulong bn, gpu_nmod_t mod, gpu_mpn_ctx_t R)
+{
+    int rc = _gpu_nmod_poly_divrem_status(q, r, a, an, b, bn, mod, R);
+    if (rc) raise_error(rc);
+}
+
 void _gpu_nmod_poly_mul_mid_mpn_ctx(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
                                     const gpu_ulong *a, gpu_ulong an, const gpu_ulong *b, gpu_ulong bn,
                                     gpu_nmod_t mod, gpu_mpn_ctx_t R)

@@ -66,3 +66,49 @@ k_crt_nmod(const uint32_t* __restrict__ res, int logM, uint64_t zl, uint64_t zh,
 }
 
 }  // namespace fb
+
+namespace fb {
+
+// Elementwise helpers of the nmod division (values in [0, n), n < 2^64).
+__device__ __forceinline__ uint64_t nmod_add64(uint64_t x, uint64_t y, uint64_t n)
+{
+    const uint64_t s = x + y;
+    return (s < x || s >= n) ? s - n : s;
+}
+
+__device__ __forceinline__ uint64_t nmod_sub64(uint64_t x, uint64_t y, uint64_t n)
+{
+    return x >= y ? x - y : x - y + n;
+}
+
+// dst[i] = src[len - 1 - i]
+__global__ void k_nmod_reverse(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t len)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[len - 1 - i];
+}
+
+// dst[i] = -src[i] mod n
+__global__ void k_nmod_neg(uint64_t* __restrict__ dst, const uint64_t* __restrict__ src, uint64_t len,
+                           uint64_t n)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < len;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i] ? n - src[i] : 0;
+}
+
+// r[i] = (sum_{k = i mod N, k < an} a[k]) - c[i] mod n, for i < cnt
+// (the reference's _nmod_poly_sub_mod_xpNm1, nmod_poly_mul.c:1196-1212)
+__global__ void k_nmod_fold_sub(uint64_t* __restrict__ r, const uint64_t* __restrict__ a, uint64_t an,
+                                uint64_t N, const uint64_t* __restrict__ c, uint64_t cnt, uint64_t n)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t s = nmod_sub64(a[i], c[i], n);
+        for (uint64_t k = i + N; k < an; k += N) s = nmod_add64(s, a[k], n);
+        r[i] = s;
+    }
+}
+
+}  // namespace fb

@@ -154,6 +154,21 @@ GPU_FFT_SMALL_API int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, 
                                   const gpu_ulong *b, gpu_ulong bn,
                                   gpu_nmod_t mod, gpu_mpn_ctx_t R);
 
+/* q[0, an-bn+1) and r[0, bn-1): quotient and remainder of a by b mod n
+   (an >= bn > 1, b's leading coefficient a unit mod n, inputs reduced mod n).
+   Replaces _nmod_poly_divrem_mpn_ctx (src/fft_small.h:776-782,
+   src/fft_small/nmod_poly_mul.c:1248-1277): the power-series inverse of the
+   reversed divisor by Newton iteration, the quotient from one middle product,
+   the remainder from a cyclic product mod x^N - 1, all on the device. */
+GPU_FFT_SMALL_API void _gpu_nmod_poly_divrem_mpn_ctx(gpu_ulong *q, gpu_ulong *r,
+                                                     const gpu_ulong *a, gpu_ulong an,
+                                                     const gpu_ulong *b, gpu_ulong bn,
+                                                     gpu_nmod_t mod, gpu_mpn_ctx_t R);
+GPU_FFT_SMALL_API int _gpu_nmod_poly_divrem_status(gpu_ulong *q, gpu_ulong *r,
+                                                   const gpu_ulong *a, gpu_ulong an,
+                                                   const gpu_ulong *b, gpu_ulong bn,
+                                                   gpu_nmod_t mod, gpu_mpn_ctx_t R);
+
 /* --- default context (replaces src/fft_small/default_ctx.c:29-51) ---------- */
 
 /* One context per host thread, created on first use with the reference's

@@ -405,3 +405,36 @@ def check_mul_range_contract(a, b, lo, z):
     if lo == 0:
         assert d == 0, "lo = 0 must be exact"
     return d
+
+
+def check_nmod_divrem(a, b, n, q, r):
+    """a = q b + r mod n with r of bn - 1 coefficients, checked with the
+    reference's own _nmod_poly_mul_mid_mpn_ctx for the product q b (the
+    reference's _nmod_poly_divrem_mpn_ctx reaches _nmod_poly_inv_series,
+    which needs FLINT's generic-ring module, outside the compiled closure).
+    Quotient and remainder are unique when b's leading coefficient is a
+    unit, so the identity pins them."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    an, bn = len(a), len(b)
+    assert len(q) == an - bn + 1 and len(r) == bn - 1
+    qb = ref_nmod_mul_mid(0, an, np.ascontiguousarray(q, dtype=np.uint64), np.ascontiguousarray(b, dtype=np.uint64), n)
+    rr = np.zeros(an, dtype=object)
+    rr[:bn - 1] = [int(x) for x in r]
+    lhs = [(int(x) - int(y)) % n for x, y in zip(a, rr)]
+    return lhs == [int(x) for x in qb]
+
+
+def nmod_divrem_python(a, b, n):
+    """Schoolbook division with remainder mod n in Python integers (small sizes)."""
+    a = [int(x) % n for x in a]
+    b = [int(x) % n for x in b]
+    inv = pow(b[-1], -1, n)
+    qn = len(a) - len(b) + 1
+    q = [0] * qn
+    for k in range(qn - 1, -1, -1):
+        c = a[k + len(b) - 1] * inv % n
+        q[k] = c
+        if c:
+            for j in range(len(b)):
+                a[k + j] = (a[k + j] - c * b[j]) % n
+    return q, a[:len(b) - 1]

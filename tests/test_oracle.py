@@ -169,3 +169,19 @@ def test_reference_range_contract(an, bn, lo):
     a, b = O.rand_limbs(an * 3 + lo, an), O.rand_limbs(bn * 5 + lo, bn)
     z = O.ref_mpn_mul_range(lo, an + bn, a, b)
     O.check_mul_range_contract(a, b, lo, z)
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference not built")
+@pytest.mark.parametrize("an,bn,bits", [(50, 20, 20), (3000, 1200, 63), (500, 499, 2)])
+def test_nmod_divrem_python_satisfies_identity(an, bn, bits):
+    """Schoolbook division (the small-size checker) against the identity
+    a = q b + r, with q b from the reference's own multiplication; a planted
+    error in r is caught."""
+    n = (1 << (bits - 1)) + 1 if bits > 2 else 3
+    a, b = O.rand_below(an, an, n), O.rand_below(bn, bn, n)
+    b[-1] = max(int(b[-1]), 1)
+    q, r = O.nmod_divrem_python(a, b, n)
+    assert O.check_nmod_divrem(a, b, n, q, r)
+    if r:
+        r[0] = (r[0] + 1) % n
+        assert not O.check_nmod_divrem(a, b, n, q, r)
