@@ -777,16 +777,17 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
         uint64_t* w = wlast[warp + 1];
         w[0] = c0[3]; w[1] = c1[3]; w[2] = c2[3]; w[3] = c1[2]; w[4] = c2[2]; w[5] = c2[1];
     }
-    if (threadIdx.x == 0) {
-        // halo: coefficients n0 - 1, n0 - 2, n0 - 3 (zero before the product)
-        uint64_t h0[3] = {0, 0, 0}, h1[3] = {0, 0, 0}, h2[3] = {0, 0, 0};
-#pragma unroll
-        for (int d = 1; d <= 3; d++) {
-            const int64_t n = n0 - d;
-            if (n >= 0 && (uint64_t)n < L) crt_coeff<NP>(res, logM, (uint64_t)n, K, h0[d - 1], h1[d - 1], h2[d - 1]);
-        }
+    if (threadIdx.x < 3) {
+        // halo: coefficients n0 - 1, n0 - 2, n0 - 3 (zero before the product),
+        // one per lane of warp 0 so the three CRTs run side by side
+        const int d = threadIdx.x + 1;
+        const int64_t n = n0 - d;
+        uint64_t h0 = 0, h1 = 0, h2 = 0;
+        if (n >= 0 && (uint64_t)n < L) crt_coeff<NP>(res, logM, (uint64_t)n, K, h0, h1, h2);
         uint64_t* w = wlast[0];
-        w[0] = h0[0]; w[1] = h1[0]; w[2] = h2[0]; w[3] = h1[1]; w[4] = h2[1]; w[5] = h2[2];
+        if (d == 1) { w[0] = h0; w[1] = h1; w[2] = h2; }
+        else if (d == 2) { w[3] = h1; w[4] = h2; }
+        else { w[5] = h2; }
     }
     __syncthreads();
     // the previous thread's last three coefficients (shuffle, or the slot of
