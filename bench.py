@@ -177,6 +177,22 @@ def cpu_baseline_run(an, bn, steps, warmup, max_seconds=60.0):
 BATCH_N, BATCH_SEED = 4096, 4096
 
 
+def replica_seeds(rank):
+    """Operand seeds of rank `rank`: every replica multiplies its own operands."""
+    return 3 + 1000 * rank, 4 + 1000 * rank
+
+
+def max_over_ranks(x, dist, device):
+    """Max of a per-rank time over all ranks (replicas finish when the
+    slowest does); identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def time_on_stream(torch, stream, fn, steps, warmup):
     """Mean milliseconds of fn() over `steps` calls, CUDA events on `stream`."""
     for _ in range(max(warmup, 3)):
@@ -502,8 +518,9 @@ def main():
         torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
 
-    a = splitmix_limbs(3 + 1000 * rank, an)
-    b = splitmix_limbs(4 + 1000 * rank, bn)
+    sa, sb = replica_seeds(rank)
+    a = splitmix_limbs(sa, an)
+    b = splitmix_limbs(sb, bn)
     ctx = FB.MpnCtx()
     np_, logM = FB.mpn_mul_plan(an, bn)
     M, L = 1 << logM, an + bn - 1
@@ -540,10 +557,7 @@ def main():
     ms = e0.elapsed_time(e1)
     ktimes = ctx.kernel_times()
     ctx.set_timing(False)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     ms_step = ms / args.steps
     gbits_step = NS_LIMB_BITS * (an + bn) / 1e9
     value = world * gbits_step / (ms_step / 1e3)
@@ -569,19 +583,20 @@ def main():
     for _ in range(e2e_steps):
         e2e_step()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    batch = stream_res = None
-    precomp = bench_precomp(torch, FB, ctx, dev, stream, max(3, args.steps // 2))
+    e2e_s = max_over_ranks(e2e_s, dist, dev)
+    # the batch, stream and transformed-operand legs are single-GPU
+    # measurements: run at N = 1 only
+    batch = stream_res = precomp = None
+    single = world == 1
+    if single:
+        precomp = bench_precomp(torch, FB, ctx, dev, stream, max(3, args.steps // 2))
     cpu_s = 0.0 if (world > 1 or args.no_cpu_baseline) else 10.0
-    if not (args.no_batch and args.stream_requests == 0):
+    if single and not (args.no_batch and args.stream_requests == 0):
         model, tun, train_info = train_cost_model(ctx)
-    if not args.no_batch:
+    if single and not args.no_batch:
         batch = bench_batch(torch, FB, ctx, dev, stream, args.steps, args.warmup, cpu_s, model, tun,
                             train_info)
-    if args.stream_requests > 0:
+    if single and args.stream_requests > 0:
         stream_res = bench_stream(torch, FB, ctx, dev, stream, model, tun, args.stream_requests, cpu_s)
     clk = clocks.stop()
     e2e_ok = bool(np.array_equal(hz.numpy().view(np.uint64), z))
