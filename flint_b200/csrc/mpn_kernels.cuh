@@ -241,8 +241,12 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             gs_contig<5, COL_FMA_ADDS>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
             twist32<LOGR>(xr, col, s, logM, th, tl, P);
+            // rows 32 s .. 32 s + 31 of column col: a pointer bump per row keeps
+            // the address arithmetic on the ALU pipe (the FMA pipe is this
+            // kernel's busiest unit)
+            uint32_t* o = out + ((size_t)(32 * s) << logC) + col;
 #pragma unroll
-            for (int m = 0; m < 32; m++) out[(size_t)(32 * s + m) * C + col] = xr[m];
+            for (int m = 0; m < 32; m++, o += C) *o = xr[m];
         }
     } else {
         // short columns: one thread owns a whole column
