@@ -328,9 +328,15 @@ constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
 static const fwd_cols_fn FWD_COLS[12] = {FB_COLS(k_fwd_cols, , false)};
 static const fwd_cols_fn FWD_COLS_FZ[12] = {FB_COLS(k_fwd_cols, , true)};
 static const inv_cols_fn INV_COLS[12] = {FB_COLS(k_inv_cols)};
+// Rows run with 32 elements per thread (k_rows<LOGC, 5>).  The kernel also
+// builds with 16 per thread (k_rows<14, 4>: 1024 threads, 32 warps per SM, 64
+// registers); measured on the 2^24 product that is slower (1.88 against
+// 1.74 ms: one more shared-memory pass, and the register cap), so the
+// dispatch keeps 32.
 static const rows_fn ROWS[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                                  k_rows<5>, k_rows<6>, k_rows<7>, k_rows<8>, k_rows<9>,
                                  k_rows<10>, k_rows<11>, k_rows<12>, k_rows<13>, k_rows<14>};
+static int row_loge(int) { return 5; }
 #undef FB_COLS
 typedef void (*rows_op_fn)(DevTables, uint32_t *, int, int, int);
 static const rows_op_fn ROWS_FWD[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -378,7 +384,7 @@ static LaunchShape make_shape(int logM, int logC = -1)
     L.col_grid = C / L.S.G;
     L.col_smem = (size_t)(padw(R * L.S.G) + 32) * sizeof(uint32_t);
     L.nv = std::min(R, std::max(1, 1 << (LOG_MAXC - L.S.logC)));
-    L.row_threads = L.nv * C / 32;
+    L.row_threads = (L.nv * C) >> row_loge(L.S.logC);
     L.row_grid = (R + L.nv - 1) / L.nv;                // items per prime; launch clamps
     L.row_smem = (size_t)3 * L.nv * padw(C) * sizeof(uint32_t);   // b and two a buffers
     return L;

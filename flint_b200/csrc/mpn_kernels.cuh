@@ -295,20 +295,22 @@ __device__ __forceinline__ void cp_async4_full(uint32_t* dst, const uint32_t* sr
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src));
 }
 
-template <int LOGC>
+// LOGE: log2 of the elements each thread owns in the row kernel's
+// contiguous pass (blockDim = nv C / 2^LOGE)
+template <int LOGC, int LOGE = 5>
 __device__ __forceinline__ void rows_prefetch(uint32_t* dst, const uint32_t* __restrict__ base,
                                               int u0, int nv, int R)
 {
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
-    constexpr int NSUB = C / 32;
+    constexpr int NSUB = C >> LOGE;
     if (nv == 1 && NSUB % 32 == 0) {
-        // one row, blockDim == C / 32: element t + k NSUB, compile-time offsets
+        // one row, blockDim == NSUB: element t + k NSUB, compile-time offsets
         const int t = threadIdx.x;
         const uint32_t* src = base + (size_t)u0 * C + t;
         uint32_t* d = dst + padw(t);
 #pragma unroll
-        for (int k = 0; k < 32; k++) cp_async4_full(d + k * (NSUB / 32 * 33), src + k * NSUB);
+        for (int k = 0; k < (1 << LOGE); k++) cp_async4_full(d + k * (NSUB / 32 * 33), src + k * NSUB);
     } else {
         for (int f = threadIdx.x; f < nv * C; f += blockDim.x) {
             const int v = f >> LOGC, i = f & (C - 1);
@@ -319,8 +321,8 @@ __device__ __forceinline__ void rows_prefetch(uint32_t* dst, const uint32_t* __r
     cp_async_commit();
 }
 
-template <int LOGC>
-__global__ void __launch_bounds__(512, 1)
+template <int LOGC, int LOGE = 5>
+__global__ void __launch_bounds__(LOGE == 4 ? 1024 : 512, 1)
 k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
        int logR, int nv, int np, const uint32_t* __restrict__ scale, int squaring,
        const InstDesc* __restrict__ desc, int ninst)
@@ -328,7 +330,9 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     extern __shared__ uint32_t sm[];
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
-    constexpr int NSUB = C / 32;
+    constexpr int E = 1 << LOGE;          // elements per thread in the contiguous pass
+    constexpr int NSUB = C / E;
+    constexpr int QMAX = LOGE;            // strided passes: at least one sub-transform per thread
     const int R = 1 << logR;
     const int logM = logR + LOGC;
     const int groups = (R + nv - 1) / nv;
@@ -339,7 +343,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     // an indexed array, so nothing goes to local memory)
     auto sa_buf = [&](int c) { return sm + (1 + c) * nv * PC; };
     const int t = threadIdx.x;
-    const int pb = (t / NSUB) * PC + 33 * (t & (NSUB - 1));
+    const int pb = (t / NSUB) * PC + padw(E * (t & (NSUB - 1)));
     // item -> (prime, first row, residue base of a, of b)
     auto decode = [&](int gg, int& jj, int& uu, uint32_t*& A, const uint32_t*& B) {
         const int inst = gg / per;
@@ -357,8 +361,8 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         uint32_t* A;
         const uint32_t* B;
         decode(g, j, u0, A, B);
-        rows_prefetch<LOGC>(sa_buf(0), A + ((size_t)j << logM), u0, nv, R);
-        if (!squaring) rows_prefetch<LOGC>(sb, B + ((size_t)j << logM), u0, nv, R);
+        rows_prefetch<LOGC, LOGE>(sa_buf(0), A + ((size_t)j << logM), u0, nv, R);
+        if (!squaring) rows_prefetch<LOGC, LOGE>(sb, B + ((size_t)j << logM), u0, nv, R);
         else cp_async_commit();
     }
     int cur = 0;
@@ -379,46 +383,46 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         // (its last item stored from it before the barrier)
         cp_async_wait<0>();
         __syncthreads();
-        if (g2 < total) rows_prefetch<LOGC>(sa_buf(cur ^ 1), A2 + ((size_t)j2 << logM), u2, nv, R);
+        if (g2 < total) rows_prefetch<LOGC, LOGE>(sa_buf(cur ^ 1), A2 + ((size_t)j2 << logM), u2, nv, R);
         else cp_async_commit();
 
-        uint32_t xr[32];
-        uint32_t breg[32];
+        uint32_t xr[E];
+        uint32_t breg[E];
         if (!squaring) {
-            gs_strided_all2<LOGC>(sa, sb, nv, twf, p);
+            gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
 #pragma unroll
-            for (int m = 0; m < 32; m++) {
+            for (int m = 0; m < E; m++) {
                 xr[m] = sa[pb + m];
                 breg[m] = sb[pb + m];
             }
-            gs_contig2<5, ROW_GS_FMA_ADDS>(xr, breg, c_w32[j], p);
+            gs_contig2<LOGE, ROW_GS_FMA_ADDS>(xr, breg, c_w32[j], p);
             __syncthreads();   // b fully read: refill it for the next item
-            if (g2 < total) rows_prefetch<LOGC>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
+            if (g2 < total) rows_prefetch<LOGC, LOGE>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
             else cp_async_commit();
         } else {
-            gs_strided_all<LOGC, 0>(sa, nv, twf, p);
+            gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
 #pragma unroll
-            for (int m = 0; m < 32; m++) xr[m] = sa[pb + m];
-            gs_contig<5, ROW_GS_FMA_ADDS>(xr, c_w32[j], p);
+            for (int m = 0; m < E; m++) xr[m] = sa[pb + m];
+            gs_contig<LOGE, ROW_GS_FMA_ADDS>(xr, c_w32[j], p);
             cp_async_commit();
         }
         const uint32_t sc = scale[j];
 #pragma unroll
-        for (int m = 0; m < 32; m++) {
+        for (int m = 0; m < E; m++) {
             const uint32_t y = squaring ? xr[m] : breg[m];
             xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
         }
-        ct_contig<5, ROW_CT_FMA_ADDS>(xr, c_w32[j], p);
+        ct_contig<LOGE, ROW_CT_FMA_ADDS>(xr, c_w32[j], p);
 #pragma unroll
-        for (int m = 0; m < 32; m++) sa[pb + m] = xr[m];
+        for (int m = 0; m < E; m++) sa[pb + m] = xr[m];
         __syncthreads();
-        ct_strided_all<LOGC, 0>(sa, nv, twi, p);
+        ct_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twi, p);
         uint32_t* __restrict__ abase = A + ((size_t)j << logM);
         if (nv == 1 && NSUB % 32 == 0) {
             uint32_t* dst = abase + (size_t)u0 * C + t;
             const uint32_t* s_ = sa + padw(t);
 #pragma unroll
-            for (int k = 0; k < 32; k++) dst[k * NSUB] = s_[k * (NSUB / 32 * 33)];
+            for (int k = 0; k < E; k++) dst[k * NSUB] = s_[k * (NSUB / 32 * 33)];
         } else {
             for (int f = t; f < nv * C; f += blockDim.x) {
                 const int v = f >> LOGC, i = f & (C - 1);

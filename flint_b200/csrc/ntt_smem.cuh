@@ -50,6 +50,11 @@ constexpr int MAX_NP = 7;
 #define FB_ROW_CT_FMA_ADDS 0
 #endif
 constexpr int COL_FMA_ADDS = FB_COL_FMA_ADDS;
+// unroll factor of the strided passes' sub-transform loops
+#ifndef FB_PASS_UNROLL
+#define FB_PASS_UNROLL 1
+#endif
+constexpr int PASS_UNROLL = FB_PASS_UNROLL;
 constexpr int ROW_GS_FMA_ADDS = FB_ROW_GS_FMA_ADDS;
 constexpr int ROW_CT_FMA_ADDS = FB_ROW_CT_FMA_ADDS;
 
@@ -232,8 +237,12 @@ __device__ __forceinline__ void gs_pass_smem(uint32_t* sm, int nv, const uint2* 
     constexpr int S = H >> (Q - 1);
     constexpr int NSUB = L / E;
     const int TOT = (G ? G : nv) * NSUB;
-    static_assert(S * (G ? G : 1) % 32 == 0, "strided pass must step by whole bank rows");
-    constexpr int PSTEP = (S * (G ? G : 1)) / 32 * 33;
+    // element m of a sub-transform sits at pb + padw(m S G'): a compile-time
+    // offset when S G' is a multiple of 32, and also for S = 16 in the rows
+    // layout (the base then lies in the low half of a 32-word bank row)
+    static_assert(S * (G ? G : 1) % 32 == 0 || (G == 0 && S == 16), "unsupported pass stride");
+    constexpr int SG = S * (G ? G : 1);
+#pragma unroll PASS_UNROLL
     for (int f = threadIdx.x; f < TOT; f += blockDim.x) {
         int v, s;
         if (G) { v = f & (G - 1); s = f / (G ? G : 1); }
@@ -243,10 +252,10 @@ __device__ __forceinline__ void gs_pass_smem(uint32_t* sm, int nv, const uint2* 
         const int pb = G ? padw(base * G) + v : v * padw(L) + padw(base);
         uint32_t x[E];
 #pragma unroll
-        for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
+        for (int m = 0; m < E; m++) x[m] = sm[pb + padw(m * SG)];
         gs_strided<Q, H, (G == 0 ? ROW_GS_FMA_ADDS : COL_FMA_ADDS)>(x, tw, jj0, p);
 #pragma unroll
-        for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
+        for (int m = 0; m < E; m++) sm[pb + padw(m * SG)] = x[m];
     }
 }
 
@@ -260,8 +269,8 @@ __device__ __forceinline__ void gs_pass_smem2(uint32_t* sx, uint32_t* sy, int nv
     constexpr int S = H >> (Q - 1);
     constexpr int NSUB = L / E;
     const int TOT = nv * NSUB;
-    static_assert(S % 32 == 0, "strided pass must step by whole bank rows");
-    constexpr int PSTEP = S / 32 * 33;
+    static_assert(S % 32 == 0 || S == 16, "unsupported pass stride");
+#pragma unroll PASS_UNROLL
     for (int f = threadIdx.x; f < TOT; f += blockDim.x) {
         const int s = f & (NSUB - 1), v = f / NSUB;
         const int jj0 = s & (S - 1);
@@ -270,14 +279,14 @@ __device__ __forceinline__ void gs_pass_smem2(uint32_t* sx, uint32_t* sy, int nv
         uint32_t x[E], y[E];
 #pragma unroll
         for (int m = 0; m < E; m++) {
-            x[m] = sx[pb + m * PSTEP];
-            y[m] = sy[pb + m * PSTEP];
+            x[m] = sx[pb + padw(m * S)];
+            y[m] = sy[pb + padw(m * S)];
         }
         gs_strided_level2<Q, H, 0, ROW_GS_FMA_ADDS>(x, y, tw, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) {
-            sx[pb + m * PSTEP] = x[m];
-            sy[pb + m * PSTEP] = y[m];
+            sx[pb + padw(m * S)] = x[m];
+            sy[pb + padw(m * S)] = y[m];
         }
     }
 }
@@ -290,8 +299,9 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
     constexpr int S = H;
     constexpr int NSUB = L / E;
     const int TOT = (G ? G : nv) * NSUB;
-    static_assert(S * (G ? G : 1) % 32 == 0, "strided pass must step by whole bank rows");
-    constexpr int PSTEP = (S * (G ? G : 1)) / 32 * 33;
+    static_assert(S * (G ? G : 1) % 32 == 0 || (G == 0 && S == 16), "unsupported pass stride");
+    constexpr int SG = S * (G ? G : 1);
+#pragma unroll PASS_UNROLL
     for (int f = threadIdx.x; f < TOT; f += blockDim.x) {
         int v, s;
         if (G) { v = f & (G - 1); s = f / (G ? G : 1); }
@@ -301,10 +311,10 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
         const int pb = G ? padw(base * G) + v : v * padw(L) + padw(base);
         uint32_t x[E];
 #pragma unroll
-        for (int m = 0; m < E; m++) x[m] = sm[pb + m * PSTEP];
+        for (int m = 0; m < E; m++) x[m] = sm[pb + padw(m * SG)];
         ct_strided<Q, H, (G == 0 ? ROW_CT_FMA_ADDS : COL_FMA_ADDS)>(x, twi, jj0, p);
 #pragma unroll
-        for (int m = 0; m < E; m++) sm[pb + m * PSTEP] = x[m];
+        for (int m = 0; m < E; m++) sm[pb + padw(m * SG)] = x[m];
     }
 }
 
@@ -328,10 +338,11 @@ __device__ __forceinline__ void gs_passes(uint32_t* sm, int nv, const uint2* __r
     }
 }
 
-template <int LOGL, int G, int QMAX = (G ? 4 : 5)>
+// LOGE: levels of the contiguous (register) pass that follows, 5 or 4
+template <int LOGL, int G, int QMAX = (G ? 4 : 5), int LOGE = 5>
 __device__ __forceinline__ void gs_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
 {
-    if constexpr (LOGL > 5) gs_passes<LOGL, G, QMAX, (1 << (LOGL - 1)), LOGL - 5>(sm, nv, tw, p);
+    if constexpr (LOGL > LOGE) gs_passes<LOGL, G, QMAX, (1 << (LOGL - 1)), LOGL - LOGE>(sm, nv, tw, p);
 }
 
 template <int LOGL, int QMAX, int H, int REM>
@@ -347,11 +358,11 @@ __device__ __forceinline__ void gs_passes2(uint32_t* sx, uint32_t* sy, int nv, c
 }
 
 // gs_strided_all for two row buffers at once (rows layout)
-template <int LOGL, int QMAX = 5>
+template <int LOGL, int QMAX = 5, int LOGE = 5>
 __device__ __forceinline__ void gs_strided_all2(uint32_t* sx, uint32_t* sy, int nv, const uint2* __restrict__ tw,
                                                 uint32_t p)
 {
-    if constexpr (LOGL > 5) gs_passes2<LOGL, QMAX, (1 << (LOGL - 1)), LOGL - 5>(sx, sy, nv, tw, p);
+    if constexpr (LOGL > LOGE) gs_passes2<LOGL, QMAX, (1 << (LOGL - 1)), LOGL - LOGE>(sx, sy, nv, tw, p);
 }
 
 // Strided part of the inverse transform (half-sizes 32 .. L/2), after the
@@ -367,10 +378,10 @@ __device__ __forceinline__ void ct_passes(uint32_t* sm, int nv, const uint2* __r
     }
 }
 
-template <int LOGL, int G, int QMAX = (G ? 4 : 5)>
+template <int LOGL, int G, int QMAX = (G ? 4 : 5), int LOGE = 5>
 __device__ __forceinline__ void ct_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ twi, uint32_t p)
 {
-    if constexpr (LOGL > 5) ct_passes<LOGL, G, QMAX, 32, LOGL - 5>(sm, nv, twi, p);
+    if constexpr (LOGL > LOGE) ct_passes<LOGL, G, QMAX, (1 << LOGE), LOGL - LOGE>(sm, nv, twi, p);
 }
 
 }  // namespace fb
