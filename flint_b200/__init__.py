@@ -91,6 +91,7 @@ SIGNATURES = {
     "_gpu_nmod_poly_divrem_mpn_ctx": (None, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_divrem_status": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
+    "gpu_default_mpn_ctx_cleanup": (None, []),
     "gpu_mpn_mul_default_mpn_ctx": (None, [_P, _P, _S, _P, _S]),
     "_gpu_nmod_poly_mul_mid_default_mpn_ctx": (None, [_P, _S, _S, _P, _S, _P, _S, _Nmod]),
     "_gpu_fmpz_poly_mul_mid_mpn_ctx": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _CTX]),

@@ -1000,20 +1000,21 @@ void _gpu_nmod_poly_mul_mid_mpn_ctx(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
 }
 
 static thread_local gpu_mpn_ctx_struct g_default_ctx = {nullptr};
-static thread_local bool g_default_registered = false;
-
-struct DefaultCtxReaper {
-    ~DefaultCtxReaper() {}
-};
 
 gpu_mpn_ctx_struct *gpu_get_default_mpn_ctx(void)
 {
-    if (!g_default_ctx.impl) {
-        // same starting prime as the reference's DEFAULT_PRIME
-        gpu_mpn_ctx_init(&g_default_ctx, 0x0003f00000000001ull);
-        g_default_registered = true;
-    }
+    // same starting prime as the reference's DEFAULT_PRIME
+    if (!g_default_ctx.impl) gpu_mpn_ctx_init(&g_default_ctx, 0x0003f00000000001ull);
     return &g_default_ctx;
+}
+
+// the calling thread's default context is released here, as the cleanup
+// hook mpn_ctx_cleanup (src/fft_small/default_ctx.c:19-27) does under
+// flint_cleanup; a later use creates a new one
+void gpu_default_mpn_ctx_cleanup(void)
+{
+    if (g_default_ctx.impl) gpu_mpn_ctx_clear(&g_default_ctx);
+    g_default_ctx.impl = nullptr;
 }
 
 void gpu_mpn_mul_default_mpn_ctx(gpu_ulong *r1, const gpu_ulong *i1, gpu_slong n1,

@@ -205,9 +205,27 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
         const uint64_t step = (uint64_t)(512 / GG) * C;
         uint64_t n = (uint64_t)u_t * C + i0 + c;
         uint32_t* d = sm + padw(u_t * GG) + c;
+        if constexpr (!FZ && LOGR >= 5) {
+            // step is a power of two: the number of loads inside the operand
+            // is a shift, and a pointer bump per row keeps the 64-bit address
+            // arithmetic off the FMA pipe (measured 1.267 -> 1.249 ms for the
+            // two operands of a 2^24 x 2^24 product)
+            constexpr int K = R * GG / 512;
+            const int lstep = (31 - __clz(512 / GG)) + logC;
+            int kin = 0;
+            if (n < xn) {
+                const uint64_t q = ((xn - n - 1) >> lstep) + 1;
+                kin = q < (uint64_t)K ? (int)q : K;
+            }
+            const uint64_t* px = x + n;
 #pragma unroll 8
-        for (int k = 0; k < R * GG / 512; k++, n += step)
-            d[k * 528] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
+            for (int k = 0; k < K; k++, px += step)
+                d[k * 528] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
+        } else {
+#pragma unroll 8
+            for (int k = 0; k < R * GG / 512; k++, n += step)
+                d[k * 528] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
+        }
     } else if (FZ || xn <= M) {
         for (int f = threadIdx.x; f < tot; f += blockDim.x) {
             const int u = f / GR, c = f - u * GR;

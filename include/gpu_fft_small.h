@@ -175,6 +175,12 @@ GPU_FFT_SMALL_API int _gpu_nmod_poly_divrem_status(gpu_ulong *q, gpu_ulong *r,
    default starting prime. */
 GPU_FFT_SMALL_API gpu_mpn_ctx_struct *gpu_get_default_mpn_ctx(void);
 
+/* Releases the calling thread's default context (its device buffers and
+   streams), as mpn_ctx_cleanup does when flint_cleanup runs
+   (src/fft_small/default_ctx.c:19-27); the next default-context call makes
+   a new one.  No-op when the thread has none. */
+GPU_FFT_SMALL_API void gpu_default_mpn_ctx_cleanup(void);
+
 /* Same signature and argument meaning as mpn_mul_default_mpn_ctx
    (src/fft_small.h:852): r1 = i1 * i2, n1 >= n2 >= 1. */
 GPU_FFT_SMALL_API void gpu_mpn_mul_default_mpn_ctx(gpu_ulong *r1, const gpu_ulong *i1, gpu_slong n1,

@@ -124,6 +124,12 @@ def test_default_context_entry_point():
     FB.lib().gpu_mpn_mul_default_mpn_ctx(z.ctypes.data, a.ctypes.data, 4000, b.ctypes.data, 1000)
     assert (z == O.gmp_mpn_mul(a, b)).all()
     assert FB.lib().gpu_get_default_mpn_ctx() is not None
+    # cleanup releases the thread's context; the next call makes a new one
+    FB.lib().gpu_default_mpn_ctx_cleanup()
+    FB.lib().gpu_default_mpn_ctx_cleanup()
+    z[:] = 0
+    FB.lib().gpu_mpn_mul_default_mpn_ctx(z.ctypes.data, a.ctypes.data, 4000, b.ctypes.data, 1000)
+    assert (z == O.gmp_mpn_mul(a, b)).all()
     del ctypes
 
 
