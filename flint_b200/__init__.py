@@ -91,6 +91,19 @@ SIGNATURES = {
     "_gpu_nmod_poly_divrem_mpn_ctx": (None, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_divrem_status": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
+    "gpu_mulmod_2expp1_ctx_init_status": (ctypes.c_int, [_P, _CTX, _S, _S]),
+    "gpu_mulmod_2expp1_ctx_init": (None, [_P, _CTX, _S, _S]),
+    "gpu_mulmod_2expp1_ctx_clear": (None, [_P]),
+    "gpu_mulmod_2expp1_ctx_info": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "gpu_mulmod_2expp1_choose_np": (_S, [_S, _S]),
+    "gpu_mulmod_2expp1_status": (ctypes.c_int, [_P, _P, _P, _P]),
+    "gpu_mulmod_2expp1": (None, [_P, _P, _P, _P]),
+    "gpu_mulmod_2expp1_batch_device": (ctypes.c_int, [_P, _P, _P, _P, _U, _U, _P]),
+    "gpu_mulmod_2expp1_transformed_size": (_S, [_P, _U]),
+    "gpu_mulmod_2expp1_transform_device": (ctypes.c_int, [_P, _P, _P, _U, _U, _P]),
+    "gpu_mulmod_2expp1_mul_cached_device": (ctypes.c_int, [_P, _P, _P, _P, _U, _U, _P]),
+    "gpu_mulmod_2expp1_transform": (ctypes.c_int, [_P, _P, _P]),
+    "gpu_mulmod_2expp1_mul_cached": (ctypes.c_int, [_P, _P, _P, _P]),
     "gpu_default_mpn_ctx_cleanup": (None, []),
     "gpu_mpn_mul_default_mpn_ctx": (None, [_P, _P, _S, _P, _S]),
     "_gpu_nmod_poly_mul_mid_default_mpn_ctx": (None, [_P, _S, _S, _P, _S, _P, _S, _Nmod]),
@@ -474,6 +487,70 @@ class MpnBatch:
 
 
 OP_MUL, OP_SQR, OP_ADDMUL, OP_SUBMUL, OP_ADD, OP_SUB, OP_NEG = range(7)
+
+
+class Mulmod2expp1:
+    """GPU counterpart of sd_fft_mpn_mulmod_2expp1_ctx_t (src/fft_small.h:
+    889-923): products modulo 2^N + 1 of (n + 1)-limb operands, N = 64 n."""
+
+    def __init__(self, ctx, N, m=0):
+        self.ctx = ctx
+        self._c = _Ctx()
+        _check(lib().gpu_mulmod_2expp1_ctx_init_status(ctypes.byref(self._c), ctx.ptr, N, m))
+        v = [ctypes.c_long() for _ in range(4)]
+        _check(lib().gpu_mulmod_2expp1_ctx_info(ctypes.byref(self._c), *[ctypes.byref(x) for x in v]))
+        self.N, self.m, self.b, self.np = (x.value for x in v)
+        self.n = self.N // 64
+
+    @property
+    def ptr(self):
+        return ctypes.byref(self._c)
+
+    def mul(self, x, y):
+        """z = x y mod 2^N + 1 (host arrays of n + 1 limbs)."""
+        x = _limbs(x)
+        y = x if y is x else _limbs(y)
+        if len(x) != self.n + 1 or len(y) != self.n + 1:
+            raise ValueError("operands have n + 1 limbs")
+        z = np.zeros(self.n + 1, dtype=np.uint64)
+        _check(lib().gpu_mulmod_2expp1_status(self.ptr, z.ctypes.data, x.ctypes.data, y.ctypes.data))
+        return z
+
+    def batch_device(self, z_ptr, x_ptr, y_ptr, count, stride=None, stream=None):
+        _check(lib().gpu_mulmod_2expp1_batch_device(self.ptr, z_ptr, x_ptr, y_ptr, count,
+                                                    stride or self.n + 1, stream))
+
+    def transformed_size(self, count=1):
+        return int(lib().gpu_mulmod_2expp1_transformed_size(self.ptr, count))
+
+    def transform_device(self, F_ptr, y_ptr, count, stride=None, stream=None):
+        _check(lib().gpu_mulmod_2expp1_transform_device(self.ptr, F_ptr, y_ptr, count,
+                                                        stride or self.n + 1, stream))
+
+    def mul_cached_device(self, z_ptr, x_ptr, F_ptr, count, stride=None, stream=None):
+        _check(lib().gpu_mulmod_2expp1_mul_cached_device(self.ptr, z_ptr, x_ptr, F_ptr, count,
+                                                         stride or self.n + 1, stream))
+
+    def close(self):
+        if self._c.impl:
+            lib().gpu_mulmod_2expp1_ctx_clear(ctypes.byref(self._c))
+            self._c.impl = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def mulmod_2expp1_choose_np(b, depth):
+    return int(lib().gpu_mulmod_2expp1_choose_np(b, depth))
 
 
 class FftPlan:

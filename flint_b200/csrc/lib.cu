@@ -10,6 +10,7 @@
 #include "basecase_kernels.cuh"
 #include "mlp_kernels.cuh"
 #include "op_kernels.cuh"
+#include "neg_kernels.cuh"
 
 #include <cuda_runtime.h>
 #include <math.h>
@@ -314,7 +315,7 @@ typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_
                             uint32_t *, uint32_t *, int, int, const InstDesc *, int, FzShape);
 typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int, const InstDesc *);
 typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, const uint32_t *,
-                        int, const InstDesc *, int);
+                        int, const InstDesc *, int, int);
 
 template <int LOGR>
 constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
@@ -338,7 +339,7 @@ static const rows_fn ROWS[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                                  k_rows<10>, k_rows<11>, k_rows<12>, k_rows<13>, k_rows<14>};
 static int row_loge(int) { return 5; }
 #undef FB_COLS
-typedef void (*rows_op_fn)(DevTables, uint32_t *, int, int, int);
+typedef void (*rows_op_fn)(DevTables, uint32_t *, int, int, int, int);
 static const rows_op_fn ROWS_FWD[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                                         k_rows_fwd<5>, k_rows_fwd<6>, k_rows_fwd<7>, k_rows_fwd<8>,
                                         k_rows_fwd<9>, k_rows_fwd<10>, k_rows_fwd<11>, k_rows_fwd<12>,
@@ -663,7 +664,8 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     timing_mark(tr, 1, st);
     const int items = L.row_grid * np * (desc ? ninst : 1);
     ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
-        X->T, ra, rb, S.logR, L.nv, np, d_scale, (sq && !desc) ? 1 : 0, desc, desc ? ninst : 1);
+        X->T, ra, rb, S.logR, L.nv, np, d_scale, (sq && !desc) ? 1 : 0, desc, desc ? ninst : 1,
+        1 << S.logR);
     timing_mark(tr, 2, st);
     if (S.logR > 0)
         INV_COLS[S.logR]<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
@@ -868,6 +870,10 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 // ---------------------------------------------------------------------------
 // plans and transformed operands
 #include "op_host.inc"
+
+// ---------------------------------------------------------------------------
+// negacyclic products mod 2^N + 1
+#include "neg_host.inc"
 
 // ---------------------------------------------------------------------------
 // C ABI

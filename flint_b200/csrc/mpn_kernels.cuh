@@ -343,7 +343,7 @@ template <int LOGC, int LOGE = 5>
 __global__ void __launch_bounds__(LOGE == 4 ? 1024 : 512, 1)
 k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
        int logR, int nv, int np, const uint32_t* __restrict__ scale, int squaring,
-       const InstDesc* __restrict__ desc, int ninst)
+       const InstDesc* __restrict__ desc, int ninst, int rows)
 {
     extern __shared__ uint32_t sm[];
     constexpr int C = 1 << LOGC;
@@ -351,7 +351,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     constexpr int E = 1 << LOGE;          // elements per thread in the contiguous pass
     constexpr int NSUB = C / E;
     constexpr int QMAX = LOGE;            // strided passes: at least one sub-transform per thread
-    const int R = 1 << logR;
+    const int R = rows;                    // rows per prime (<= 2^logR, the prime stride's rows)
     const int logM = logR + LOGC;
     const int groups = (R + nv - 1) / nv;
     const int per = groups * np;           // items of one product

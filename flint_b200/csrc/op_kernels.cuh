@@ -16,16 +16,17 @@
 namespace fb {
 
 // forward row transforms of one operand, in place: grid = items
-// (row groups x primes), block = nv C / 32, smem = nv padw(C) words
+// (row groups x primes), block = nv C / 32, smem = nv padw(C) words; rows of
+// prime j start at buf + j 2^(logR + LOGC), of which the first `rows` are used
 template <int LOGC>
 __global__ void __launch_bounds__(512)
-k_rows_fwd(DevTables T, uint32_t* __restrict__ buf, int logR, int nv, int np)
+k_rows_fwd(DevTables T, uint32_t* __restrict__ buf, int logR, int nv, int np, int rows)
 {
     extern __shared__ uint32_t sm[];
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
     constexpr int NSUB = C / 32;
-    const int R = 1 << logR;
+    const int R = rows;                    // rows per prime (<= 2^logR)
     const int logM = logR + LOGC;
     const int groups = (R + nv - 1) / nv;
     const int j = blockIdx.x / groups;
@@ -57,13 +58,13 @@ k_rows_fwd(DevTables T, uint32_t* __restrict__ buf, int logR, int nv, int np)
 // pointwise stage); launch shape as k_rows_fwd
 template <int LOGC>
 __global__ void __launch_bounds__(512)
-k_rows_inv(DevTables T, uint32_t* __restrict__ buf, int logR, int nv, int np)
+k_rows_inv(DevTables T, uint32_t* __restrict__ buf, int logR, int nv, int np, int rows)
 {
     extern __shared__ uint32_t sm[];
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
     constexpr int NSUB = C / 32;
-    const int R = 1 << logR;
+    const int R = rows;                    // rows per prime (<= 2^logR)
     const int logM = logR + LOGC;
     const int groups = (R + nv - 1) / nv;
     const int j = blockIdx.x / groups;

@@ -192,6 +192,75 @@ GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gp
                                             const gpu_ulong *b, gpu_slong bn,
                                             gpu_nmod_t mod);
 
+/* --- negacyclic products mod 2^N + 1 (replaces src/fft_small/negacyclic.c,
+       the pointwise engine of Schoenhage-Strassen convolutions) ------------ */
+
+/* Operands and results are n + 1 limbs, N = 64 n: the n low limbs and a top
+   limb that is 0 or 1 (inputs may be unreduced below 2^(N+1), as in the
+   reference, negacyclic.c:288-290); results are the unique representative in
+   [0, 2^N], top limb 1 only for 2^N itself.  A context fixes N and the digit
+   split N = m b; it uses (and must not outlive) an mpn context. */
+typedef struct { void *impl; } gpu_mulmod_2expp1_ctx_struct;
+typedef gpu_mulmod_2expp1_ctx_struct gpu_mulmod_2expp1_ctx_t[1];
+
+/* As sd_fft_mpn_mulmod_2expp1_ctx_init (src/fft_small.h:908, negacyclic.c:
+   65-175): N a positive multiple of 64, m a power of two >= 16 dividing N,
+   or 0 to let the context choose.  The digit count actually used is a power
+   of two in [32, 2^14]: a request outside that range is moved into it by
+   doubling or halving the digit size, and a request whose digits are too
+   wide for six 31-bit primes takes more, narrower digits.  The product does
+   not depend on the split.
+   Returns 0, GPU_FFT_SMALL_EINVAL or GPU_FFT_SMALL_ENOPRIMES (no split fits
+   six 31-bit primes: 2 b + log2 m + 2 must stay below their ~183 bits). */
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_ctx_init_status(gpu_mulmod_2expp1_ctx_struct *C, gpu_mpn_ctx_t R,
+                                                         gpu_slong N, gpu_slong m);
+/* Same, raising errors through the error handler (the reference throws). */
+GPU_FFT_SMALL_API void gpu_mulmod_2expp1_ctx_init(gpu_mulmod_2expp1_ctx_struct *C, gpu_mpn_ctx_t R,
+                                                  gpu_slong N, gpu_slong m);
+/* As sd_fft_mpn_mulmod_2expp1_ctx_clear (src/fft_small.h:910). */
+GPU_FFT_SMALL_API void gpu_mulmod_2expp1_ctx_clear(gpu_mulmod_2expp1_ctx_struct *C);
+/* The context's N, digit count m, digit bits b and prime count (the fields
+   C->N, C->m, C->b, C->np of the reference's context struct). */
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_ctx_info(const gpu_mulmod_2expp1_ctx_struct *C, gpu_slong *N,
+                                                 gpu_slong *m, gpu_slong *b, gpu_slong *np);
+/* As sd_fft_mpn_mulmod_2expp1_choose_np (src/fft_small.h:907) over this
+   library's primes: the fewest that hold the biased coefficient bound
+   2^(2 b + depth + 1) with one bit to spare; -1 when six do not. */
+GPU_FFT_SMALL_API gpu_slong gpu_mulmod_2expp1_choose_np(gpu_slong b, gpu_slong depth);
+/* As sd_fft_mpn_mulmod_2expp1 (src/fft_small.h:911): z = x y mod 2^N + 1,
+   host pointers.  The reference's scratch argument has no counterpart (the
+   context owns its device buffers; a context is not reentrant). */
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_status(const gpu_mulmod_2expp1_ctx_struct *C, gpu_ulong *z,
+                                               const gpu_ulong *x, const gpu_ulong *y);
+GPU_FFT_SMALL_API void gpu_mulmod_2expp1(const gpu_mulmod_2expp1_ctx_struct *C, gpu_ulong *z,
+                                         const gpu_ulong *x, const gpu_ulong *y);
+/* Batched device form (the pointwise stage of one convolution in one call):
+   z_i = x_i y_i mod 2^N + 1 for i < count, operand i at x + i stride (stride
+   >= n + 1 limbs), all device pointers, queued on `stream`.  x == y squares. */
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_batch_device(const gpu_mulmod_2expp1_ctx_struct *C, uint64_t *z,
+                                                     const uint64_t *x, const uint64_t *y,
+                                                     gpu_ulong count, gpu_ulong stride, void *stream);
+/* Staged form (sd_fft_mpn_mulmod_2expp1_transformed_size / _transform /
+   _mul_cached, src/fft_small.h:916-923): the transforms of `count` operands
+   take gpu_mulmod_2expp1_transformed_size(C, count) 32-bit words of device
+   memory; mul_cached multiplies operand i of x by cached transform i and
+   must be given the same count as the transform call that filled F (the
+   layout depends on it). */
+GPU_FFT_SMALL_API gpu_slong gpu_mulmod_2expp1_transformed_size(const gpu_mulmod_2expp1_ctx_struct *C,
+                                                               gpu_ulong count);
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_transform_device(const gpu_mulmod_2expp1_ctx_struct *C, uint32_t *F,
+                                                         const uint64_t *y, gpu_ulong count,
+                                                         gpu_ulong stride, void *stream);
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_mul_cached_device(const gpu_mulmod_2expp1_ctx_struct *C, uint64_t *z,
+                                                          const uint64_t *x, const uint32_t *F,
+                                                          gpu_ulong count, gpu_ulong stride, void *stream);
+/* One-operand host forms of the staged pair; F is device memory of
+   gpu_mulmod_2expp1_transformed_size(C, 1) words. */
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_transform(const gpu_mulmod_2expp1_ctx_struct *C, uint32_t *F,
+                                                  const gpu_ulong *y);
+GPU_FFT_SMALL_API int gpu_mulmod_2expp1_mul_cached(const gpu_mulmod_2expp1_ctx_struct *C, gpu_ulong *z,
+                                                   const gpu_ulong *x, const uint32_t *F);
+
 /* --- explicit schedules (no counterpart in the reference; its counterpart
        is the profile choice of mpn_ctx_best_profile, src/fft_small/mpn_mul.c:
        1248-1340, which is internal) --------------------------------------- */

@@ -438,3 +438,132 @@ def nmod_divrem_python(a, b, n):
             for j in range(len(b)):
                 a[k + j] = (a[k + j] - c * b[j]) % n
     return q, a[:len(b) - 1]
+
+
+# ---------------------------------------------------------------- mod 2^N + 1
+def negmul_python(x, y, N):
+    """z = x y mod 2^N + 1 by Python integers.  x, y have n + 1 limbs
+    (N = 64 n; the top limb 0 or 1, possibly unreduced); z is the unique
+    representative in [0, 2^N] in n + 1 limbs.  The same check the reference
+    uses, a full product folded once (src/fft_small/test/
+    t-sd_fft_mpn_mulmod_2expp1.c:21-48)."""
+    n = N // 64
+    v = to_int(x) * to_int(y)
+    # one fold (2^N = -1) leaves |v| < 2^(N+2): the final % has a tiny quotient
+    v = ((v & ((1 << N) - 1)) - (v >> N)) % ((1 << N) + 1)
+    return from_int(v, n + 1)
+
+
+def negacyclic_digits_python(x, y, N, m):
+    """The reference's negacyclic algorithm restated on Python integers, small
+    m only (src/fft_small/negacyclic.c): b-bit digits with digit 0 lowered by
+    the top limb (negacyclic.c:243-289, 322-323), the negacyclic convolution
+    of the digit vectors (there: twist by w^i, cyclic transforms, untwist by
+    w^-i m^-1, negacyclic.c:327-438; here: schoolbook), biased coefficients
+    c_i + B with B = 2^(2b + log2 m) (negacyclic.c:137-161, 429-438), their sum
+    at bit offsets b i minus the bias polynomial and the fold of the part
+    above 2^N (negacyclic.c:440-488)."""
+    n = N // 64
+    b = N // m
+    depth = m.bit_length() - 1
+    mask = (1 << b) - 1
+
+    def digits(v):
+        lo = to_int(np.asarray(v, dtype=np.uint64)[:n])
+        d = [(lo >> (b * i)) & mask for i in range(m)]
+        d[0] -= int(int(v[n]) != 0)
+        return d
+
+    dx, dy = digits(x), digits(y)
+    B = 1 << (2 * b + depth)
+    c = [0] * m
+    for i in range(m):
+        xi = dx[i]
+        if xi == 0:
+            continue
+        for j in range(m):
+            k = i + j
+            if k < m:
+                c[k] += xi * dy[j]
+            else:
+                c[k - m] -= xi * dy[j]
+    W = 0
+    bias = 0
+    for i in range(m):
+        assert 0 <= c[i] + B < 2 * B
+        W += (c[i] + B) << (b * i)
+        bias += B << (b * i)
+    w = W - bias
+    lo, hi = w & ((1 << N) - 1), w >> N      # hi signed (arithmetic shift)
+    return from_int((lo - hi) % ((1 << N) + 1), n + 1)
+
+
+class _RefNegCtx:
+    """sd_fft_mpn_mulmod_2expp1 of the compiled reference, for small
+    configurations its own test covers (src/fft_small/test/
+    t-sd_fft_mpn_mulmod_2expp1.c:53-80): the context struct is held in an
+    opaque buffer, its leading fields N, b, m, depth, np read back."""
+
+    def __init__(self, N, m):
+        L = ref()
+        P, S = ctypes.c_void_p, ctypes.c_long
+        for name, args in (("sd_fft_mpn_mulmod_2expp1_ctx_init", [P, P, S, S]),
+                           ("sd_fft_mpn_mulmod_2expp1_ctx_clear", [P]),
+                           ("sd_fft_mpn_mulmod_2expp1_scratch_init", [P, P]),
+                           ("sd_fft_mpn_mulmod_2expp1_scratch_clear", [P]),
+                           ("sd_fft_mpn_mulmod_2expp1", [P, P, P, P, P])):
+            getattr(L, name).argtypes = args
+            getattr(L, name).restype = None
+        self.L = L
+        self.C = ctypes.create_string_buffer(16384)
+        self.S = ctypes.create_string_buffer(256)
+        L.sd_fft_mpn_mulmod_2expp1_ctx_init(self.C, L.get_default_mpn_ctx(), N, m)
+        L.sd_fft_mpn_mulmod_2expp1_scratch_init(self.S, self.C)
+        f = np.frombuffer(self.C.raw[:40], dtype=np.int64)
+        self.N, self.b, self.m, self.depth, self.np = (int(v) for v in f)
+
+    def mul(self, x, y):
+        x = np.ascontiguousarray(x, dtype=np.uint64)
+        y = x if y is x else np.ascontiguousarray(y, dtype=np.uint64)
+        z = np.zeros(self.N // 64 + 1, dtype=np.uint64)
+        self.L.sd_fft_mpn_mulmod_2expp1(self.C, z.ctypes.data, x.ctypes.data, y.ctypes.data,
+                                        self.S)
+        return z
+
+    def close(self):
+        if self.C is not None:
+            self.L.sd_fft_mpn_mulmod_2expp1_scratch_clear(self.S)
+            self.L.sd_fft_mpn_mulmod_2expp1_ctx_clear(self.C)
+            self.C = None
+
+
+def ref_mulmod_2expp1(x, y, N, m):
+    """The reference's sd_fft_mpn_mulmod_2expp1 on its default context."""
+    R = _RefNegCtx(N, m)
+    try:
+        return R.mul(x, y)
+    finally:
+        R.close()
+
+
+def neg_operand(seed, n, kind="rand"):
+    """An (n + 1)-limb operand of the shapes the reference's test draws
+    (t-sd_fft_mpn_mulmod_2expp1.c:109-137): random low limbs with top limb 0,
+    "two_n" (2^N), "unreduced" (top limb 1 over random low limbs), "sparse"
+    (one random limb), "ones" (all low limbs 2^64 - 1), "zero"."""
+    x = np.zeros(n + 1, dtype=np.uint64)
+    if kind == "rand":
+        x[:n] = rand_limbs(seed, n, top_nonzero=False)
+    elif kind == "two_n":
+        x[n] = 1
+    elif kind == "unreduced":
+        x[:n] = rand_limbs(seed, n, top_nonzero=False)
+        x[n] = 1
+    elif kind == "sparse":
+        r = rand_limbs(seed, 2, top_nonzero=False)
+        x[int(r[0]) % n] = r[1]
+    elif kind == "ones":
+        x[:n] = np.uint64((1 << 64) - 1)
+    elif kind != "zero":
+        raise ValueError(kind)
+    return x

@@ -108,13 +108,44 @@ def fmpz_inputs(case):
     return a, b, zw, case.get("zl", 0), case.get("zh", zn)
 
 
+# z = x y mod 2^N + 1 by the reference's sd_fft_mpn_mulmod_2expp1: digit
+# sizes and counts drawn from its own test (t-sd_fft_mpn_mulmod_2expp1.c:
+# 56-60), operand shapes as its switch (:109-137)
+NEG_CASES = [
+    dict(name="neg_b64_m16", b=64, m=16, kx="rand", ky="rand", seed=71),
+    dict(name="neg_b64_m128", b=64, m=128, kx="rand", ky="rand", seed=72),
+    dict(name="neg_b84_m32", b=84, m=32, kx="rand", ky="rand", seed=73),
+    dict(name="neg_b88_m128", b=88, m=128, kx="rand", ky="rand", seed=74),
+    dict(name="neg_b112_m64", b=112, m=64, kx="unreduced", ky="rand", seed=75),
+    dict(name="neg_b126_m32", b=126, m=32, kx="rand", ky="rand", seed=76),
+    dict(name="neg_b128_m16", b=128, m=16, kx="rand", ky="two_n", seed=77),
+    dict(name="neg_b136_m64", b=136, m=64, kx="sparse", ky="rand", seed=78),
+    dict(name="neg_b144_m128", b=144, m=128, kx="rand", ky="rand", seed=79),
+    dict(name="neg_b168_m32", b=168, m=32, kx="ones", ky="ones", seed=80),
+    dict(name="neg_b192_m128", b=192, m=128, kx="rand", ky="rand", seed=81),
+    dict(name="neg_b34_m64", b=34, m=64, kx="rand", ky="rand", seed=82),
+    dict(name="neg_b40_m128", b=40, m=128, kx="two_n", ky="two_n", seed=83),
+    dict(name="neg_b46_m32", b=46, m=32, kx="rand", ky="square", seed=84),
+    dict(name="neg_b50_m64", b=50, m=64, kx="unreduced", ky="unreduced", seed=85),
+    dict(name="neg_b50_m128_zero", b=50, m=128, kx="zero", ky="rand", seed=86),
+]
+
+
+def neg_inputs(case):
+    N = case["b"] * case["m"]
+    n = N // 64
+    x = O.neg_operand(case["seed"], n, case["kx"])
+    y = x if case["ky"] == "square" else O.neg_operand(case["seed"] + 1000, n, case["ky"])
+    return N, x, y
+
+
 def main():
     if not O.have_ref():
         raise SystemExit("oracle/_ref/libflint_ref.so missing: run python oracle/build_ref.py")
     O.ref().flint_set_num_threads(os.cpu_count() or 1)
     out = {"generator": "oracle.rand_limbs / oracle.rand_below (splitmix64)",
            "source": "reference fft_small (oracle/_ref/libflint_ref.so)",
-           "mpn": [], "nmod": [], "fmpz": []}
+           "mpn": [], "nmod": [], "fmpz": [], "neg": []}
     for case in MPN_CASES:
         t = time.time()
         a, b = mpn_inputs(case)
@@ -126,6 +157,12 @@ def main():
         n, a, b = nmod_inputs(case)
         z = O.ref_nmod_mul_mid(case["zl"], case["zh"], a, b, n)
         out["nmod"].append(dict(case, modulus="%x" % n, **record(z)))
+        print("%-28s %.2fs" % (case["name"], time.time() - t))
+    for case in NEG_CASES:
+        t = time.time()
+        N, x, y = neg_inputs(case)
+        z = O.ref_mulmod_2expp1(x, y, N, case["m"])
+        out["neg"].append(dict(case, N=N, **record(z)))
         print("%-28s %.2fs" % (case["name"], time.time() - t))
     for case in FMPZ_CASES:
         t = time.time()

@@ -185,3 +185,37 @@ def test_nmod_divrem_python_satisfies_identity(an, bn, bits):
     if r:
         r[0] = (r[0] + 1) % n
         assert not O.check_nmod_divrem(a, b, n, q, r)
+
+
+# ------------------------------------------------ products mod 2^N + 1
+def test_golden_covers_negacyclic(golden):
+    assert len(golden["neg"]) >= 12
+
+
+@pytest.mark.parametrize("i", range(16))
+def test_negmul_oracles_match_golden(golden, i):
+    """Both restatements (a folded Python product, and the reference's
+    digit/bias/fold algorithm) reproduce the reference's outputs."""
+    from tests.golden.make_golden import neg_inputs
+    case = golden["neg"][i]
+    N, x, y = neg_inputs(case)
+    _check_record(case, O.negmul_python(x, y, N))
+    if case["m"] <= 64:
+        _check_record(case, O.negacyclic_digits_python(x, y, N, case["m"]))
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_negmul_oracle_vs_reference(seed):
+    if not O.have_ref():
+        pytest.skip("compiled reference absent")
+    rng = np.random.default_rng(seed)
+    b = int(rng.choice([34, 40, 46, 50, 64, 84, 88, 128]))
+    m = 16 << int(rng.integers(0, 4))
+    N = b * m
+    if N % 64:
+        pytest.skip("N not a multiple of 64")
+    n = N // 64
+    for kx, ky in (("rand", "rand"), ("unreduced", "two_n"), ("ones", "sparse")):
+        x = O.neg_operand(300 + seed, n, kx)
+        y = O.neg_operand(400 + seed, n, ky)
+        assert (O.negmul_python(x, y, N) == O.ref_mulmod_2expp1(x, y, N, m)).all()
