@@ -459,6 +459,102 @@ def bench_precomp(torch, FB, ctx, dev, stream, steps):
             "speedup": ms_full / ms_op, "identical": same}
 
 
+# products mod 2^N + 1 (Schoenhage-Strassen pointwise stage): ring size in
+# bits, products per batch; operands of every batch exceed L2 (126 MB)
+NEG_WORKLOADS = [(47104, 16384), (1 << 20, 512)]
+
+
+def neg_cpu_baseline(N, X, Y, seconds):
+    """The reference's sd_fft_mpn_mulmod_2expp1 (its own digit split, m = 0)
+    over the batch in order, one product per call, on every host thread (each
+    with its own context and scratch; ctypes releases the GIL)."""
+    import oracle
+    if not oracle.have_ref():
+        return None, None
+    nthreads = os.cpu_count() or 1
+    count = len(X)
+    nxt = [0]
+    lock = threading.Lock()
+    done = [0] * nthreads
+    outs = {}
+    t0 = time.perf_counter()
+
+    def work(t):
+        R = oracle._RefNegCtx(N, 0)
+        try:
+            while time.perf_counter() - t0 < seconds:
+                with lock:
+                    i = nxt[0]
+                    nxt[0] += 1
+                if i >= count:
+                    break
+                z = R.mul(X[i], Y[i])
+                if i < 8:
+                    outs[i] = z
+                done[t] += 1
+        finally:
+            R.close()
+
+    th = [threading.Thread(target=work, args=(t,)) for t in range(nthreads)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    dt = time.perf_counter() - t0
+    k = sum(done)
+    return ({"value": k / dt, "unit": "products/s", "cores": nthreads, "kind": "reference",
+             "sample": "%d of the %d products, one sd_fft_mpn_mulmod_2expp1 call each" % (k, count)},
+            outs)
+
+
+def bench_negacyclic(torch, FB, ctx, dev, stream, steps, cpu_seconds):
+    """Batches of products mod 2^N + 1 (gpu_mulmod_2expp1_batch_device),
+    device-resident, against the reference's engine on the host cores."""
+    res = []
+    s = stream.cuda_stream
+    peak, peak_kind = load_peaks()
+    for N, count in NEG_WORKLOADS:
+        n = N // 64
+        g = torch.Generator(device=dev)
+        g.manual_seed(N)
+        X = torch.randint(-(1 << 63), (1 << 63) - 1, (count, n + 1), dtype=torch.int64, device=dev,
+                          generator=g)
+        Y = torch.randint(-(1 << 63), (1 << 63) - 1, (count, n + 1), dtype=torch.int64, device=dev,
+                          generator=g)
+        X[:, n] = 0
+        Y[:, n] = 0
+        Z = torch.empty_like(X)
+        C = FB.Mulmod2expp1(ctx, N, 0)
+        fn = lambda: C.batch_device(Z.data_ptr(), X.data_ptr(), Y.data_ptr(), count, None, s)  # noqa: E731
+        ms = time_on_stream(torch, stream, fn, steps, 3)
+        # HBM bytes per product: operands and result (n + 1 limbs each), the
+        # residues written by the split (2 np m words), read and written by the
+        # row pass (2 np m + np m) and read by the finisher (np m)
+        alg = count * (24 * (n + 1) + 24 * C.np * C.m)
+        gbps = alg / (ms / 1e3) / 1e9
+        item = {"workload": "%d products mod 2^%d + 1, uniform random operands" % (count, N),
+                "N": N, "count": count, "m": C.m, "b": C.b, "primes": C.np,
+                "ms_per_batch": ms, "products_per_s": count / (ms / 1e3),
+                "operand_Gbit_s": 2 * N * count / (ms / 1e3) / 1e9,
+                "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved": gbps, "peak": peak,
+                             "unit": "GB/s", "frac": gbps / peak, "peak_kind": peak_kind},
+                "gpu_launches_per_batch": 4}
+        if cpu_seconds > 0:
+            Xh = X.cpu().numpy().view(np.uint64)
+            Yh = Y.cpu().numpy().view(np.uint64)
+            cb, outs = neg_cpu_baseline(N, Xh, Yh, cpu_seconds)
+            if cb is not None:
+                item["cpu_baseline"] = cb
+                item["speedup_vs_cpu"] = item["products_per_s"] / cb["value"]
+                Zh = Z.cpu().numpy().view(np.uint64)
+                item["identical_to_reference_sample"] = bool(outs) and all(
+                    np.array_equal(Zh[i], z) for i, z in outs.items())
+        C.close()
+        res.append(item)
+        del X, Y, Z
+    return res
+
+
 def kernel_bytes(name, an, bn, np_, M, L):
     """Algorithmic bytes each kernel must move in the four-pass design:
     residues are 4-byte words, np primes, M-point transforms."""
@@ -481,6 +577,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 4096-product uneven batch")
+    ap.add_argument("--no-negacyclic", action="store_true",
+                    help="skip the products mod 2^N + 1")
+    ap.add_argument("--negacyclic-only", action="store_true",
+                    help="run only the products mod 2^N + 1 (profiling); prints their results")
     ap.add_argument("--stream-requests", type=int, default=2000,
                     help="requests of the mixed mpn / integer-polynomial stream (0 = skip)")
     args = ap.parse_args()
@@ -517,6 +617,14 @@ def main():
     else:
         torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+
+    if args.negacyclic_only:
+        ctx = FB.MpnCtx()
+        res = bench_negacyclic(torch, FB, ctx, dev, torch.cuda.current_stream(dev), args.steps,
+                               0.0 if args.no_cpu_baseline else 5.0)
+        if rank == 0:
+            print(json.dumps({"negacyclic": res}), flush=True)
+        return
 
     sa, sb = replica_seeds(rank)
     a = splitmix_limbs(sa, an)
@@ -586,11 +694,14 @@ def main():
     e2e_s = max_over_ranks(e2e_s, dist, dev)
     # the batch, stream and transformed-operand legs are single-GPU
     # measurements: run at N = 1 only
-    batch = stream_res = precomp = None
+    batch = stream_res = precomp = negacyclic = None
     single = world == 1
+    cpu_s = 0.0 if (world > 1 or args.no_cpu_baseline) else 10.0
     if single:
         precomp = bench_precomp(torch, FB, ctx, dev, stream, max(3, args.steps // 2))
-    cpu_s = 0.0 if (world > 1 or args.no_cpu_baseline) else 10.0
+        if not args.no_negacyclic:
+            negacyclic = bench_negacyclic(torch, FB, ctx, dev, stream, max(3, args.steps // 2),
+                                          min(cpu_s, 5.0))
     if single and not (args.no_batch and args.stream_requests == 0):
         model, tun, train_info = train_cost_model(ctx)
     if single and not args.no_batch:
@@ -656,6 +767,7 @@ def main():
         "batch": batch,
         "stream": stream_res,
         "transformed_operand": precomp,
+        "negacyclic": negacyclic,
     }
     print(json.dumps(line), flush=True)
     if dist:
