@@ -43,6 +43,15 @@ class _Nmod(ctypes.Structure):
     _fields_ = [("n", ctypes.c_ulong), ("ninv", ctypes.c_ulong), ("norm", ctypes.c_ulong)]
 
 
+class _MulPrecomp(ctypes.Structure):
+    _fields_ = [("impl", ctypes.c_void_p), ("bn", ctypes.c_ulong), ("btrunc", ctypes.c_ulong),
+                ("depth", ctypes.c_ulong)]
+
+
+class _DivremPrecomp(ctypes.Structure):
+    _fields_ = [("quo_maker", _MulPrecomp), ("rem_maker", _MulPrecomp)]
+
+
 class MulReq(ctypes.Structure):
     """gpu_mpn_mul_req: one product z = a * b of a batch (device pointers)."""
     _fields_ = [("z", ctypes.c_void_p), ("a", ctypes.c_void_p), ("an", ctypes.c_ulong),
@@ -91,6 +100,16 @@ SIGNATURES = {
     "_gpu_nmod_poly_divrem_mpn_ctx": (None, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_divrem_status": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
+    "gpu_mul_precomp_init_status": (ctypes.c_int, [_P, _P, _U, _U, _U, _Nmod, _CTX]),
+    "_gpu_mul_precomp_init": (None, [_P, _P, _U, _U, _U, _Nmod, _CTX]),
+    "_gpu_mul_precomp_clear": (None, [_P]),
+    "_gpu_nmod_poly_mul_mid_precomp": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _Nmod, _CTX]),
+    "gpu_nmod_poly_mul_mid_precomp_device": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _P]),
+    "_gpu_nmod_poly_divrem_precomp_init_status": (ctypes.c_int, [_P, _P, _U, _U, _Nmod, _CTX]),
+    "_gpu_nmod_poly_divrem_precomp_init": (None, [_P, _P, _U, _U, _Nmod, _CTX]),
+    "_gpu_nmod_poly_divrem_precomp": (ctypes.c_int, [_P, _P, _P, _U, _P, _Nmod, _CTX]),
+    "gpu_nmod_poly_divrem_precomp_device": (ctypes.c_int, [_P, _P, _P, _U, _P, _P]),
+    "_gpu_nmod_poly_divrem_precomp_clear": (None, [_P]),
     "gpu_mulmod_2expp1_ctx_init_status": (ctypes.c_int, [_P, _CTX, _S, _S]),
     "gpu_mulmod_2expp1_ctx_init": (None, [_P, _CTX, _S, _S]),
     "gpu_mulmod_2expp1_ctx_clear": (None, [_P]),
@@ -535,6 +554,98 @@ class Mulmod2expp1:
         if self._c.impl:
             lib().gpu_mulmod_2expp1_ctx_clear(ctypes.byref(self._c))
             self._c.impl = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MulPrecomp:
+    """GPU counterpart of mul_precomp_struct (src/fft_small.h:796-822): b's
+    transforms of length 2^depth for modulus n, reused by mul_mid."""
+
+    def __init__(self, ctx, b, depth, n, btrunc=None):
+        self.ctx, self.n = ctx, int(n)
+        b = _limbs(b)
+        self._m = _MulPrecomp()
+        _check(lib().gpu_mul_precomp_init_status(ctypes.byref(self._m), b.ctypes.data, len(b),
+                                                 btrunc or len(b), depth, _Nmod(self.n, 0, 0), ctx.ptr))
+        self.bn, self.depth = len(b), int(self._m.depth)
+
+    @property
+    def ptr(self):
+        return ctypes.byref(self._m)
+
+    def mul_mid(self, zl, zh, a):
+        """Coefficients [zl, zh) of a b mod n, or None when the window does
+        not fit the transform (the reference's 0 return)."""
+        a = _limbs(a)
+        z = np.zeros(max(zh - zl, 0), dtype=np.uint64)
+        ok = lib()._gpu_nmod_poly_mul_mid_precomp(z.ctypes.data, zl, zh, a.ctypes.data, len(a), self.ptr,
+                                                   _Nmod(self.n, 0, 0), self.ctx.ptr)
+        return z if ok else None
+
+    def mul_mid_device(self, z_ptr, zl, zh, a_ptr, an, stream=None):
+        _check(lib().gpu_nmod_poly_mul_mid_precomp_device(z_ptr, zl, zh, a_ptr, an, self.ptr, stream))
+
+    def close(self):
+        if self._m.impl:
+            lib()._gpu_mul_precomp_clear(ctypes.byref(self._m))
+            self._m.impl = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DivremPrecomp:
+    """GPU counterpart of nmod_poly_divrem_precomp_struct (src/fft_small.h:
+    824-848): division by a fixed b with quotients up to Bn coefficients."""
+
+    def __init__(self, ctx, b, Bn, n):
+        self.ctx, self.n = ctx, int(n)
+        b = _limbs(b)
+        self._m = _DivremPrecomp()
+        _check(lib()._gpu_nmod_poly_divrem_precomp_init_status(ctypes.byref(self._m), b.ctypes.data, len(b),
+                                                              Bn, _Nmod(self.n, 0, 0), ctx.ptr))
+        self.bn, self.Bn = len(b), int(Bn)
+
+    @property
+    def ptr(self):
+        return ctypes.byref(self._m)
+
+    def divrem(self, a):
+        """(q, r) with a = q b + r, or None when the quotient is longer than Bn."""
+        a = _limbs(a)
+        q = np.zeros(len(a) - self.bn + 1, dtype=np.uint64)
+        r = np.zeros(self.bn - 1, dtype=np.uint64)
+        ok = lib()._gpu_nmod_poly_divrem_precomp(q.ctypes.data, r.ctypes.data, a.ctypes.data, len(a), self.ptr,
+                                                 _Nmod(self.n, 0, 0), self.ctx.ptr)
+        return (q, r) if ok else None
+
+    def divrem_device(self, q_ptr, r_ptr, a_ptr, an, stream=None):
+        _check(lib().gpu_nmod_poly_divrem_precomp_device(q_ptr, r_ptr, a_ptr, an, self.ptr, stream))
+
+    def close(self):
+        if self._m.quo_maker.impl or self._m.rem_maker.impl:
+            lib()._gpu_nmod_poly_divrem_precomp_clear(ctypes.byref(self._m))
+            self._m.quo_maker.impl = self._m.rem_maker.impl = None
 
     def __enter__(self):
         return self

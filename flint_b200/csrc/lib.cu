@@ -872,6 +872,10 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 #include "op_host.inc"
 
 // ---------------------------------------------------------------------------
+// precomputed transforms for nmod products and division
+#include "precomp_host.inc"
+
+// ---------------------------------------------------------------------------
 // negacyclic products mod 2^N + 1
 #include "neg_host.inc"
 

@@ -98,6 +98,18 @@ __global__ void k_nmod_neg(uint64_t* __restrict__ dst, const uint64_t* __restric
         dst[i] = src[i] ? n - src[i] : 0;
 }
 
+// dst[i] = sum_{k = i mod N, k < an} a[k] mod n, for i < N (a mod x^N - 1)
+__global__ void k_nmod_fold(uint64_t* __restrict__ dst, const uint64_t* __restrict__ a, uint64_t an,
+                            uint64_t N, uint64_t n)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t s = 0;
+        for (uint64_t k = i; k < an; k += N) s = nmod_add64(s, a[k], n);
+        dst[i] = s;
+    }
+}
+
 // r[i] = (sum_{k = i mod N, k < an} a[k]) - c[i] mod n, for i < cnt
 // (the reference's _nmod_poly_sub_mod_xpNm1, nmod_poly_mul.c:1196-1212)
 __global__ void k_nmod_fold_sub(uint64_t* __restrict__ r, const uint64_t* __restrict__ a, uint64_t an,

@@ -192,6 +192,75 @@ GPU_FFT_SMALL_API void _gpu_nmod_poly_mul_mid_default_mpn_ctx(gpu_ulong *res, gp
                                             const gpu_ulong *b, gpu_slong bn,
                                             gpu_nmod_t mod);
 
+/* --- precomputed transforms for nmod products and division (replaces
+       mul_precomp_struct, _mul_precomp_init/_clear, _nmod_poly_mul_mid_precomp
+       and the nmod_poly_divrem_precomp_* family, src/fft_small.h:796-848,
+       src/fft_small/nmod_poly_mul.c:1054-1320) --------------------------- */
+
+/* b's forward transforms of length 2^depth (at least 32) for one modulus,
+   kept in device memory; bn and btrunc are recorded as in the reference
+   (the GPU transforms at full length).  Operands longer than the transform
+   are folded mod x^M - 1 and mod n, so every cyclic coefficient sums at most
+   M products: the prime count is chosen for M (n - 1)^2 once. */
+typedef struct {
+    void *impl;
+    gpu_ulong bn;
+    gpu_ulong btrunc;
+    gpu_ulong depth;   /* log2 of the transform length actually used */
+} gpu_mul_precomp_struct;
+
+/* As _mul_precomp_init (src/fft_small.h:803-808): b on the host, reduced mod
+   n; depth <= 25.  Returns 0, GPU_FFT_SMALL_EINVAL, _ETOOBIG, _ENOPRIMES or
+   _ECUDA; the void form raises through the error handler. */
+GPU_FFT_SMALL_API int gpu_mul_precomp_init_status(gpu_mul_precomp_struct *M, const gpu_ulong *b, gpu_ulong bn,
+                                                  gpu_ulong btrunc, gpu_ulong depth, gpu_nmod_t mod,
+                                                  gpu_mpn_ctx_t R);
+GPU_FFT_SMALL_API void _gpu_mul_precomp_init(gpu_mul_precomp_struct *M, const gpu_ulong *b, gpu_ulong bn,
+                                             gpu_ulong btrunc, gpu_ulong depth, gpu_nmod_t mod, gpu_mpn_ctx_t R);
+/* As _mul_precomp_clear (src/fft_small.h:810-814). */
+GPU_FFT_SMALL_API void _gpu_mul_precomp_clear(gpu_mul_precomp_struct *M);
+/* As _nmod_poly_mul_mid_precomp (src/fft_small.h:816-822): z = coefficients
+   [zl, zh) of a b mod n (zero beyond an + bn - 1), host pointers; returns 1,
+   or 0 when the window does not fit the transform without wrap-around
+   (zh > 2^depth or an + bn - 1 - zl > 2^depth), as the reference's
+   _fft_small_plan_fit_window refusal; other errors raise. */
+GPU_FFT_SMALL_API int _gpu_nmod_poly_mul_mid_precomp(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
+                                                     const gpu_ulong *a, gpu_ulong an, gpu_mul_precomp_struct *M,
+                                                     gpu_nmod_t mod, gpu_mpn_ctx_t R);
+/* Device-pointer form queued on `stream`: 0, or GPU_FFT_SMALL_ETOOBIG when
+   the window does not fit. */
+GPU_FFT_SMALL_API int gpu_nmod_poly_mul_mid_precomp_device(uint64_t *z, gpu_ulong zl, gpu_ulong zh,
+                                                           const uint64_t *a, gpu_ulong an,
+                                                           gpu_mul_precomp_struct *M, void *stream);
+
+typedef struct {
+    gpu_mul_precomp_struct quo_maker[1];   /* rev(rev(b)^-1 mod x^Bn), 2^depth >= 2 Bn - 1 */
+    gpu_mul_precomp_struct rem_maker[1];   /* b, 2^depth = N >= bn - 1 */
+} gpu_nmod_poly_divrem_precomp_struct;
+
+/* As _nmod_poly_divrem_precomp_init (src/fft_small.h:834-840): the inverse
+   series of the reversed divisor to precision Bn (device Newton iteration)
+   and both transforms.  b's leading coefficient must be a unit mod n. */
+GPU_FFT_SMALL_API int _gpu_nmod_poly_divrem_precomp_init_status(gpu_nmod_poly_divrem_precomp_struct *M,
+                                                                const gpu_ulong *b, gpu_ulong bn, gpu_ulong Bn,
+                                                                gpu_nmod_t mod, gpu_mpn_ctx_t R);
+GPU_FFT_SMALL_API void _gpu_nmod_poly_divrem_precomp_init(gpu_nmod_poly_divrem_precomp_struct *M,
+                                                          const gpu_ulong *b, gpu_ulong bn, gpu_ulong Bn,
+                                                          gpu_nmod_t mod, gpu_mpn_ctx_t R);
+/* As _nmod_poly_divrem_precomp (src/fft_small.h:842-848): a = q b + r with
+   q of an - bn + 1 and r of bn - 1 coefficients, host pointers; returns 1, or
+   0 when the quotient is longer than the precision Bn. */
+GPU_FFT_SMALL_API int _gpu_nmod_poly_divrem_precomp(gpu_ulong *q, gpu_ulong *r, const gpu_ulong *a, gpu_ulong an,
+                                                    gpu_nmod_poly_divrem_precomp_struct *M, gpu_nmod_t mod,
+                                                    gpu_mpn_ctx_t R);
+/* Device-pointer form queued on `stream`: 0, or GPU_FFT_SMALL_ETOOBIG when
+   the quotient is longer than Bn. */
+GPU_FFT_SMALL_API int gpu_nmod_poly_divrem_precomp_device(uint64_t *q, uint64_t *r, const uint64_t *a,
+                                                          gpu_ulong an, gpu_nmod_poly_divrem_precomp_struct *M,
+                                                          void *stream);
+/* As _nmod_poly_divrem_precomp_clear (src/fft_small.h:828-832). */
+GPU_FFT_SMALL_API void _gpu_nmod_poly_divrem_precomp_clear(gpu_nmod_poly_divrem_precomp_struct *M);
+
 /* --- negacyclic products mod 2^N + 1 (replaces src/fft_small/negacyclic.c,
        the pointwise engine of Schoenhage-Strassen convolutions) ------------ */
 
