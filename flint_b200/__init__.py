@@ -155,6 +155,14 @@ SIGNATURES = {
     "gpu_mlp_clear": (None, [_P]),
     "gpu_fft_plan_init_mpn": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _U, _U, _U, ctypes.c_int]),
     "gpu_fft_plan_init_nmod": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _U, _U, _U, _U, _U, _Nmod]),
+    "gpu_fft_plan_init_mpn_np": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _U, _U, _U, ctypes.c_int, ctypes.c_int]),
+    "gpu_fft_plan_init_nmod_cyclic": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, _U, _U, _U, _U, _Nmod]),
+    "gpu_fft_plan_init_mpn_cyclic": (ctypes.c_int, [ctypes.POINTER(_P), _CTX, ctypes.POINTER(_U), _U]),
+    "gpu_fft_op_sizeof_data": (_U, [_P]),
+    "gpu_fft_op_init_borrowed": (ctypes.c_int, [ctypes.POINTER(_P), _P, _P]),
+    "gpu_fft_export_mpn_signed": (ctypes.c_int, [_P, _U, ctypes.POINTER(ctypes.c_int), _P, _U, _P, _P]),
+    "gpu_fft_export_mpn_signed_trunc": (ctypes.c_int, [_P, _U, ctypes.POINTER(ctypes.c_int), _P, _U, _U, _P,
+                                                        _P]),
     "gpu_fft_plan_info": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     "gpu_fft_plan_clear": (None, [_P]),
     "gpu_fft_op_init": (ctypes.c_int, [ctypes.POINTER(_P), _P]),
@@ -684,6 +692,32 @@ class FftPlan:
         return cls(ctx, h, "mpn")
 
     @classmethod
+    def mpn_np(cls, ctx, an_max, bn_max, len_bound, is_signed, np_):
+        h = ctypes.c_void_p()
+        _check(lib().gpu_fft_plan_init_mpn_np(ctypes.byref(h), ctx.ptr, an_max, bn_max, len_bound,
+                                              1 if is_signed else 0, np_))
+        return cls(ctx, h, "mpn")
+
+    @classmethod
+    def mpn_cyclic(cls, ctx, nn, len_bound=1):
+        """(plan, nn rounded up) for products mod 2^(64 nn) - 1."""
+        h = ctypes.c_void_p()
+        v = ctypes.c_ulong(nn)
+        _check(lib().gpu_fft_plan_init_mpn_cyclic(ctypes.byref(h), ctx.ptr, ctypes.byref(v), len_bound))
+        return cls(ctx, h, "mpn"), v.value
+
+    @classmethod
+    def nmod_cyclic(cls, ctx, depth, zh, n, len_bound=None, prod_bits=None):
+        h = ctypes.c_void_p()
+        pb = prod_bits if prod_bits is not None else 2 * (int(n) - 1).bit_length()
+        _check(lib().gpu_fft_plan_init_nmod_cyclic(ctypes.byref(h), ctx.ptr, depth, zh,
+                                                   len_bound or (1 << depth), pb, _Nmod(n, 0, 0)))
+        return cls(ctx, h, "nmod", n)
+
+    def sizeof_data(self):
+        return int(lib().gpu_fft_op_sizeof_data(self._h))
+
+    @classmethod
     def nmod(cls, ctx, zl, zh, zn, n, len_bound, prod_bits=None):
         h = ctypes.c_void_p()
         pb = prod_bits if prod_bits is not None else 2 * (int(n) - 1).bit_length()
@@ -691,8 +725,10 @@ class FftPlan:
                                             _Nmod(n, 0, 0)))
         return cls(ctx, h, "nmod", n)
 
-    def op(self):
-        return FftOp(self)
+    def op(self, data_ptr=None):
+        """A transformed operand; with data_ptr, in that caller-owned device
+        memory (sizeof_data() bytes)."""
+        return FftOp(self, data_ptr)
 
     def pointwise(self, op, Z, A, B=None, stream=None):
         _check(lib().gpu_fft_op_pointwise(op, Z._h, A._h, (B or A)._h, self._h, stream))
@@ -715,10 +751,13 @@ class FftPlan:
 class FftOp:
     """A transformed operand (gpu_fft_op_*), resident in device memory."""
 
-    def __init__(self, plan):
+    def __init__(self, plan, data_ptr=None):
         self.plan = plan
         self._h = ctypes.c_void_p()
-        _check(lib().gpu_fft_op_init(ctypes.byref(self._h), plan._h))
+        if data_ptr is None:
+            _check(lib().gpu_fft_op_init(ctypes.byref(self._h), plan._h))
+        else:
+            _check(lib().gpu_fft_op_init_borrowed(ctypes.byref(self._h), plan._h, data_ptr))
 
     def fft(self, a_ptr, an, stream=None):
         f = lib().gpu_fft_fft_mpn if self.plan.kind == "mpn" else lib().gpu_fft_fft_nmod
@@ -729,6 +768,14 @@ class FftOp:
 
     def export_mpn(self, z_ptr, zn, stream=None):
         _check(lib().gpu_fft_export_mpn(z_ptr, zn, self._h, self.plan._h, stream))
+
+    def export_mpn_signed(self, z_ptr, zn, nslots, lo_limbs=0, stream=None):
+        """Limbs [lo_limbs, lo_limbs + zn) of |value| into z; returns the sign
+        (1 negative).  Synchronises the stream."""
+        sg = ctypes.c_int()
+        _check(lib().gpu_fft_export_mpn_signed_trunc(z_ptr, zn, ctypes.byref(sg), self._h, nslots, lo_limbs,
+                                                     self.plan._h, stream))
+        return sg.value
 
     def export_nmod(self, z_ptr, zl, zh, stream=None):
         _check(lib().gpu_fft_export_nmod(z_ptr, zl, zh, self._h, _Nmod(self.plan.mod, 0, 0),

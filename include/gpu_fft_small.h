@@ -499,11 +499,38 @@ GPU_FFT_SMALL_API int gpu_fft_plan_init_mpn(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, 
 GPU_FFT_SMALL_API int gpu_fft_plan_init_nmod(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, gpu_ulong zl, gpu_ulong zh,
                                              gpu_ulong zn, gpu_ulong len_bound, gpu_ulong prod_bits,
                                              gpu_nmod_t mod);
+/* fft_small_plan_init_mpn_np (src/fft_small.h:587-589): as
+   gpu_fft_plan_init_mpn with the prime count forced (np = 0: the automatic
+   choice; otherwise np primes if they hold the bound, else
+   GPU_FFT_SMALL_ENOPRIMES; the reference's two-prime geometry does not exist
+   here, 64-bit coefficients need five primes). */
+GPU_FFT_SMALL_API int gpu_fft_plan_init_mpn_np(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, gpu_ulong an_max,
+                                               gpu_ulong bn_max, gpu_ulong len_bound, int is_signed, int np);
+/* fft_small_plan_init_nmod_cyclic (src/fft_small.h:591-593): convolutions
+   mod x^N - 1, N = 2^depth (5 <= depth <= 25), output coefficients [0, zh).
+   Operands longer than N are folded mod x^N - 1 and mod n by the forward
+   transform. */
+GPU_FFT_SMALL_API int gpu_fft_plan_init_nmod_cyclic(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, gpu_ulong depth,
+                                                    gpu_ulong zh, gpu_ulong len_bound, gpu_ulong prod_bits,
+                                                    gpu_nmod_t mod);
+/* fft_small_plan_init_mpn_cyclic (src/fft_small.h:600-601): products of
+   integers of at most *nn limbs mod 2^(64 *nn) - 1, *nn rounded up to a
+   power of two (at least 32) and written back.  gpu_fft_export_mpn gives
+   the non-negative sum of the coefficients (below len_bound 2^(64 nn + 128 +
+   log2 nn)); export at least nn + 3 limbs and fold the top limbs back. */
+GPU_FFT_SMALL_API int gpu_fft_plan_init_mpn_cyclic(gpu_fft_plan_t *P, gpu_mpn_ctx_t R, gpu_ulong *nn,
+                                                   gpu_ulong len_bound);
 GPU_FFT_SMALL_API int gpu_fft_plan_info(gpu_fft_plan_t P, int *np, int *logM);
 GPU_FFT_SMALL_API void gpu_fft_plan_clear(gpu_fft_plan_t P);
 /* fft_small_op_init / fft_small_op_clear */
 GPU_FFT_SMALL_API int gpu_fft_op_init(gpu_fft_op_t *X, gpu_fft_plan_t P);
 GPU_FFT_SMALL_API void gpu_fft_op_clear(gpu_fft_op_t X);
+/* fft_small_op_sizeof_data / fft_small_op_init_borrowed (src/fft_small.h:
+   636-638): an operand in caller-provided device memory of
+   gpu_fft_op_sizeof_data(P) bytes (16-byte aligned, outliving the operand;
+   gpu_fft_op_clear does not free it). */
+GPU_FFT_SMALL_API gpu_ulong gpu_fft_op_sizeof_data(gpu_fft_plan_t P);
+GPU_FFT_SMALL_API int gpu_fft_op_init_borrowed(gpu_fft_op_t *X, gpu_fft_plan_t P, void *data_dev);
 /* fft_small_fft_mpn / fft_small_fft_nmod: forward transforms of a (an limbs
    or coefficients; nmod coefficients reduced mod n) into X */
 GPU_FFT_SMALL_API int gpu_fft_fft_mpn(gpu_fft_op_t X, const uint64_t *a_dev, gpu_ulong an,
@@ -524,6 +551,19 @@ GPU_FFT_SMALL_API int gpu_fft_export_mpn(uint64_t *z_dev, gpu_ulong zn, gpu_fft_
    window) */
 GPU_FFT_SMALL_API int gpu_fft_export_nmod(uint64_t *z_dev, gpu_ulong zl, gpu_ulong zh, gpu_fft_op_t X,
                                           gpu_nmod_t mod, gpu_fft_plan_t P, void *stream);
+/* fft_small_export_mpn_signed / _signed_trunc (src/fft_small.h:681-686):
+   the value sum_(j < nslots) c_j 2^(64 j) with every coefficient c_j in the
+   centered range (-P/2, P/2] (plans made with is_signed keep true values in
+   it); z receives limbs [lo_limbs, lo_limbs + zn) of its absolute value and
+   *sign its sign (0 when those limbs are zero).  lo_limbs + zn must be at
+   least nslots + 3 so that the sign is inside.  The window is exact (the
+   reference's truncated form may drop carries from below it).  Synchronises
+   `stream` to return the sign. */
+GPU_FFT_SMALL_API int gpu_fft_export_mpn_signed(uint64_t *z_dev, gpu_ulong zn, int *sign, gpu_fft_op_t X,
+                                                gpu_ulong nslots, gpu_fft_plan_t P, void *stream);
+GPU_FFT_SMALL_API int gpu_fft_export_mpn_signed_trunc(uint64_t *z_dev, gpu_ulong zn, int *sign, gpu_fft_op_t X,
+                                                      gpu_ulong nslots, gpu_ulong lo_limbs, gpu_fft_plan_t P,
+                                                      void *stream);
 /* Synchronises `stream`; GPU_FFT_SMALL_ETIMEOUT if a carry wait gave up. */
 GPU_FFT_SMALL_API int gpu_fft_op_check(gpu_fft_plan_t P, void *stream);
 
