@@ -109,7 +109,10 @@ __device__ __forceinline__ uint64_t bits64(uint64_t v0, uint64_t v1, uint64_t v2
     return o ? (lo >> o) | (hi << (64 - o)) : lo;
 }
 
-constexpr int NEG_THREADS = 512;
+#ifndef FB_NEG_THREADS
+#define FB_NEG_THREADS 512
+#endif
+constexpr int NEG_THREADS = FB_NEG_THREADS;   // one output limb per thread per tile
 constexpr int NEG_CMAX = 2560;   // biased coefficients held per recomposition tile
 
 // Carry-lookahead over one tile (one limb per thread): (g, p) -> carry into

@@ -147,10 +147,16 @@ def dataset(tuner, reqs):
 
 
 class CostModel:
-    """Learned schedule: predicts log time, chooses the argmin candidate."""
+    """Learned schedule: predicts log time, chooses the argmin candidate.
 
-    def __init__(self, seed=1):
+    margin > 0 makes the choice conservative: the model's argmin replaces the
+    fixed rule's configuration only when it predicts at least that relative
+    saving (a prediction error of a few percent otherwise trades the rule's
+    configuration for one that is no faster)."""
+
+    def __init__(self, seed=1, margin=0.0):
         self.net = Mlp(N_FEATURES, seed)
+        self.margin = margin
 
     def fit(self, X, t, epochs=300, batch=256, lr=2e-3, seed=7):
         return self.net.train(X, t, epochs=epochs, batch=batch, lr=lr, seed=seed)
@@ -160,10 +166,17 @@ class CostModel:
         cands = [candidates(r) for r in reqs]
         rows = [features(r, c) for r, cs in zip(reqs, cands) for c in cs]
         pred = self.net.predict(np.array(rows, dtype=np.float32))
+        keep = math.log(1.0 - self.margin) if self.margin > 0 else 0.0
         out, k = [], 0
-        for cs in cands:
+        for r, cs in zip(reqs, cands):
             p = pred[k:k + len(cs)]
-            out.append(cs[int(np.argmin(p))])
+            i = int(np.argmin(p))
+            if self.margin > 0:
+                dk = default_config(r).key()
+                j = next((n for n, c in enumerate(cs) if c.key() == dk), None)
+                if j is not None and p[i] - p[j] > keep:
+                    i = j
+            out.append(cs[i])
             k += len(cs)
         return out
 
