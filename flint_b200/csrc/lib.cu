@@ -179,6 +179,10 @@ struct Ctx {
     long kernel_count[TIMING_SLOTS] = {0};
     CrtConst crt[MAX_NP + 1];
     uint32_t cof_red[MAX_NP + 1][MAX_NP]; // (P/p_j) mod p_j for each np
+    // host-pointer products: a second stream for the copies that overlap
+    // the kernels, and events to order the two
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copy[9] = {nullptr};
 };
 
 static int grow(void **ptr, size_t *cap, size_t need)
@@ -398,7 +402,7 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
                               TimingRecord *tr, const InstDesc *desc = nullptr, int ninst = 1,
-                              const FzShape *fz = nullptr);
+                              const FzShape *fz = nullptr, cudaEvent_t b_ready = nullptr);
 
 static int upload_scales(Ctx *X);
 
@@ -513,6 +517,12 @@ static void ctx_destroy(Ctx *X)
     cudaFree(X->d_res);
     cudaFree(X->d_io);
     if (X->stream) cudaStreamDestroy(X->stream);
+    if (X->copy_stream) {
+        cudaStreamSynchronize(X->copy_stream);
+        cudaStreamDestroy(X->copy_stream);
+    }
+    for (auto &e : X->ev_copy)
+        if (e) cudaEventDestroy(e);
     delete X;
 }
 
@@ -654,13 +664,25 @@ static int rows_per_sm(const LaunchShape &L)
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
-                              TimingRecord *tr, const InstDesc *desc, int ninst, const FzShape *fz)
+                              TimingRecord *tr, const InstDesc *desc, int ninst, const FzShape *fz,
+                              cudaEvent_t b_ready)
 {
     const MulShape &S = L.S;
     const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
     const FzShape shape = fz ? *fz : FzShape{1, 1, 1};
-    (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
-        X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np, shape);
+    if (b_ready && !desc && !sq) {
+        // b is still arriving: a's column pass first, b's after its copy
+        (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
+            X->T, a, an, a, an, ra, ra, S.logC, S.G, nullptr, np, shape);
+        cudaStreamWaitEvent(st, b_ready, 0);
+        const FzShape shb = fz ? FzShape{shape.S, shape.wb, shape.wb} : shape;
+        (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
+            X->T, b, bn, b, bn, rb, rb, S.logC, S.G, nullptr, np, shb);
+    } else {
+        if (b_ready) cudaStreamWaitEvent(st, b_ready, 0);
+        (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
+            X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np, shape);
+    }
     timing_mark(tr, 1, st);
     const int items = L.row_grid * np * (desc ? ninst : 1);
     ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
@@ -730,9 +752,19 @@ static int window_logM(uint64_t an, uint64_t bn, uint64_t lo, uint64_t hi)
 // 2^64, exact for lo = 0), and the result depends on a, b and lo only, not on
 // hi or the transform length.  A window far below the top uses a shorter
 // cyclic transform (window_logM).
+// A host-pointer product copies each CRT chunk back while the next one runs:
+// after the launch of chunk k (limbs [l0, l1) of the output) the hook queues
+// its copy.
+struct CrtChunks {
+    int chunks = 1;
+    void (*hook)(void *arg, uint64_t l0, uint64_t l1) = nullptr;
+    void *arg = nullptr;
+};
+
 static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
                            const uint64_t *b, uint64_t bn, cudaStream_t st,
-                           const gpu_mul_config *cfg = nullptr, uint64_t lo = 0, uint64_t hi = ~0ull)
+                           const gpu_mul_config *cfg = nullptr, uint64_t lo = 0, uint64_t hi = ~0ull,
+                           cudaEvent_t b_ready = nullptr, const CrtChunks *chunks = nullptr)
 {
     MulPlan P;
     int rc = plan_mpn_cfg(an, bn, cfg, &P);
@@ -743,7 +775,10 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     const bool window = lo > 0 || hi < zfull;
     if (P.route == GPU_MUL_ROUTE_BASECASE) {
         if (window) return set_error(GPU_FFT_SMALL_EINVAL, "the basecase route computes whole products only");
-        return mpn_mul_basecase_enqueue(X, z, a, an, b, bn, P.logM, st);
+        if (b_ready) CU(cudaStreamWaitEvent(st, b_ready, 0));
+        rc = mpn_mul_basecase_enqueue(X, z, a, an, b, bn, P.logM, st);
+        if (!rc && chunks && chunks->hook) chunks->hook(chunks->arg, 0, zfull);
+        return rc;
     }
     // limbs [lo, hi): the carry chain starts at lo; a shorter cyclic
     // transform is used when the window allows one
@@ -776,15 +811,26 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
 
     int launches = 3;
     TimingRecord *tr = timing_begin(X, st);
-    launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr);
-    if (np == 5)
-        k_crt_carry<5, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
-                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err,
-                                                          nullptr, nullptr, base);
-    else
-        k_crt_carry<6, THREADS><<<tiles, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
-                                                          X->d_ticket, X->ticket_base, X->epoch, X->d_err,
-                                                          nullptr, nullptr, base);
+    launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr, nullptr, 1,
+                      nullptr, b_ready);
+    // tiles take their index from the ticket counter, so consecutive launches
+    // with the same ticket base continue one carry chain: tile k's look-back
+    // finds tile k - 1 finished by an earlier launch
+    const int nch = (chunks && !window) ? std::max(1, std::min<int>(chunks->chunks, (int)tiles)) : 1;
+    for (int c = 0; c < nch; c++) {
+        const size_t t0 = tiles * c / nch, t1 = tiles * (c + 1) / nch;
+        if (t1 == t0) continue;
+        if (np == 5)
+            k_crt_carry<5, THREADS><<<t1 - t0, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
+                                                                X->d_ticket, X->ticket_base, X->epoch, X->d_err,
+                                                                nullptr, nullptr, base);
+        else
+            k_crt_carry<6, THREADS><<<t1 - t0, THREADS, 0, st>>>(ra, logM, an + bn - 1, zn, z, K, X->d_status,
+                                                                X->d_ticket, X->ticket_base, X->epoch, X->d_err,
+                                                                nullptr, nullptr, base);
+        if (chunks && chunks->hook)
+            chunks->hook(chunks->arg, base + t0 * TILE, std::min<uint64_t>(zn, base + t1 * TILE));
+    }
     launches++;
     timing_mark(tr, 4, st);
     X->ticket_base += tiles;
@@ -823,6 +869,14 @@ static int bind_device(Ctx *X)
     return 0;
 }
 
+static int ensure_copy_stream(Ctx *X)
+{
+    if (X->copy_stream) return 0;
+    CU(cudaStreamCreateWithFlags(&X->copy_stream, cudaStreamNonBlocking));
+    for (auto &e : X->ev_copy) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return 0;
+}
+
 static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
                         const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
 {
@@ -839,11 +893,43 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
     if (rc) return rc;
     uint64_t *da = buf, *db = sq ? buf : buf + an, *dz = buf + (sq ? an : an + bn);
     if (nz) {
-        CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, X->stream));
-        if (!sq) CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, X->stream));
-        rc = mpn_mul_enqueue(X, dz, da, an, db, bn, X->stream, nullptr, lo, top);
+        rc = ensure_copy_stream(X);
         if (rc) return rc;
-        CU(cudaMemcpyAsync(z, dz, nz * 8, cudaMemcpyDeviceToHost, X->stream));
+        cudaStream_t S = X->stream, C = X->copy_stream;
+        // a on the compute stream; b on the copy stream once a is in (the two
+        // copies share the link), while a's column pass runs
+        CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, S));
+        cudaEvent_t b_ready = nullptr;
+        if (!sq) {
+            CU(cudaEventRecord(X->ev_copy[0], S));
+            CU(cudaStreamWaitEvent(C, X->ev_copy[0], 0));
+            CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, C));
+            CU(cudaEventRecord(X->ev_copy[1], C));
+            b_ready = X->ev_copy[1];
+        }
+        // the result comes back in chunks on the copy stream, each as soon as
+        // its CRT launch has finished
+        struct Back { Ctx *X; uint64_t *z, *dz; uint64_t lo; int k; int rc; } bk{X, z, dz, lo, 0, 0};
+        CrtChunks ch;
+        ch.chunks = lo == 0 ? 4 : 1;
+        ch.arg = &bk;
+        ch.hook = [](void *p, uint64_t l0, uint64_t l1) {
+            Back &B = *(Back *)p;
+            if (B.rc || l1 <= l0) return;
+            cudaEvent_t e = B.X->ev_copy[2 + (B.k++ % 7)];
+            if (cudaEventRecord(e, B.X->stream) != cudaSuccess ||
+                cudaStreamWaitEvent(B.X->copy_stream, e, 0) != cudaSuccess ||
+                cudaMemcpyAsync(B.z + (l0 - B.lo), B.dz + (l0 - B.lo), (l1 - l0) * 8, cudaMemcpyDeviceToHost,
+                                B.X->copy_stream) != cudaSuccess)
+                B.rc = set_error(GPU_FFT_SMALL_ECUDA, "result copy");
+        };
+        rc = mpn_mul_enqueue(X, dz, da, an, db, bn, S, nullptr, lo, top, b_ready, &ch);
+        if (!rc) rc = bk.rc;
+        if (rc) {
+            cudaStreamSynchronize(C);
+            return rc;
+        }
+        CU(cudaStreamSynchronize(C));
     }
     rc = check_device_error(X);
     if (rc) return rc;
