@@ -339,7 +339,8 @@ GPU_FFT_SMALL_API int gpu_mulmod_2expp1_mul_cached(const gpu_mulmod_2expp1_ctx_s
 
 /* How one product is computed.  Zero fields take the default: the fewest
    primes that hold the coefficient bound, the shortest transform that holds
-   the product, rows of min(2^logM, 2^14).  Any valid choice gives the same
+   the product, rows of 2^logM points up to 2^14, 2^13-point rows from 2^15
+   to 2^24 points, 2^14 at 2^25.  Any valid choice gives the same
    (exact) product; only the time differs. */
 typedef struct {
     int route;   /* GPU_MUL_ROUTE_* */

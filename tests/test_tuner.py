@@ -43,7 +43,9 @@ def test_invalid_configs_are_rejected():
     with pytest.raises(FB.GpuFftSmallError):
         FB.resolve_config(1, 10, 10, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0), 2, 2)
     c = FB.resolve_config(0, 1 << 20, 1 << 20)
-    assert c.key() == (FB.ROUTE_NTT, 5, 21, 14)
+    assert c.key() == (FB.ROUTE_NTT, 5, 21, 13)       # 2^13-point rows from 2^15 to 2^24
+    assert FB.resolve_config(0, 1 << 24, 1 << 24).key() == (FB.ROUTE_NTT, 5, 25, 14)
+    assert FB.resolve_config(0, 5000, 3000).key() == (FB.ROUTE_NTT, 5, 13, 13)
 
 
 def test_request_stream_shape():
