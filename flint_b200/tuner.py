@@ -8,7 +8,7 @@ choice per request is a gpu_mul_config:
     route   transform or basecase (schoolbook, shorter operand <= 1024 limbs)
     np      prime count (the minimum, or one more)
     logM    transform length (the minimum, or twice it)
-    logC    four-step row length (the longest allowed, or 2x / 4x shorter)
+    logC    four-step row length (the longest allowed, or 2x / 4x / 8x shorter)
 
 Every valid configuration gives the same exact product; only time differs.
 
@@ -59,7 +59,7 @@ def candidates(r):
         out.append(MulConfig(ROUTE_BASECASE, 0, 0, 0))
     for dnp in (0, 1):
         for dm in (0, 1):
-            for dc in (0, 1, 2):
+            for dc in (0, 1, 2, 3):
                 np_, logM = base.np + dnp, base.logM + dm
                 logC = min(logM, 14) - dc
                 c = MulConfig(ROUTE_NTT, np_, logM, logC)
