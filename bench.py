@@ -43,14 +43,14 @@ WORKLOADS = {
 NS_LIMB_BITS = 64
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per launch measured
-# with ncu on the 2^22 x 2^22-limb case (M = 2^23, 5 primes); traffic grows in
-# proportion to the residue points, so a launch on another size scales by
-# M / 2^23.
-NCU_TRAFFIC_2P22 = {
-    "k_fwd_cols": 67.559168e6 + 277.239040e6,
-    "k_rows": 337.119488e6 + 123.299328e6,
-    "k_inv_cols": 168.167680e6 + 108.828672e6,
-    "k_crt_carry": 167.904000e6 + 43.076608e6,
+# with ncu on the headline 2^24 x 2^24-limb product itself (M = 2^25, 5 primes;
+# profiles/*_mpn24.md); for another size the figure is scaled by M / 2^25
+# (traffic grows in proportion to the residue points).
+NCU_TRAFFIC_2P25 = {
+    "k_fwd_cols": 0.269222e9 + 1.291399e9,
+    "k_rows": 1.343594e9 + 0.626662e9,
+    "k_inv_cols": 0.671535e9 + 0.621226e9,
+    "k_crt_carry": 0.671245e9 + 0.244851e9,
 }
 
 
@@ -730,12 +730,13 @@ def main():
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"])
     alg_pipeline = 208 * (an + bn)
     traffic = None
-    if args.workload in ("mpn24", "mpn22"):
-        scale = M / float(1 << 23)                # residue points relative to the capture
-        for name, v in kern.items():
-            if name in NCU_TRAFFIC_2P22:
-                v["traffic"] = NCU_TRAFFIC_2P22[name] * scale
-        traffic = kern[dom].get("traffic")
+    scale = M / float(1 << 25)                    # residue points relative to the capture
+    for name, v in kern.items():
+        if name in NCU_TRAFFIC_2P25:
+            v["traffic"] = NCU_TRAFFIC_2P25[name] * scale
+            v["traffic_note"] = ("measured at this size" if M == 1 << 25 else
+                                 "scaled from the 2^25-point capture by residue points")
+    traffic = kern[dom].get("traffic")
     roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["GBps"], "peak": peak,
                 "unit": "GB/s", "frac": kern[dom]["GBps"] / peak, "traffic": traffic,
                 "peak_kind": peak_kind,

@@ -54,6 +54,15 @@ def test_full_size_vs_gmp(ctx):
     assert (ctx.mpn_mul(a, b) == O.gmp_mpn_mul(a, b)).all()
 
 
+@pytest.mark.parametrize("an,bn", [((1 << 25) - 4095, 4096), (1 << 25, 1)])
+def test_longest_transform_vs_gmp(ctx, an, bn):
+    """an + bn - 1 = 2^25 coefficients: the longest cyclic transform, no slack."""
+    a = O.rand_limbs(an % 1000 + 3, an)
+    b = O.rand_limbs(bn % 1000 + 4, bn)
+    assert FB.mpn_mul_plan(an, bn)[1] == 25
+    assert (ctx.mpn_mul(a, b) == O.gmp_mpn_mul(a, b)).all()
+
+
 SIZES = [(1, 1), (1, 2), (2, 2), (3, 1), (15, 17), (16, 16), (17, 16), (255, 257),
          (1000, 1), (1, 1000), (4096, 4095), (8191, 8193), (10000, 20000),
          (65536, 1), (65537, 65535), (131072, 3), (100000, 99999), (300000, 5000)]
