@@ -737,9 +737,19 @@ def main():
             v["traffic_note"] = ("measured at this size" if M == 1 << 25 else
                                  "scaled from the 2^25-point capture by residue points")
     traffic = kern[dom].get("traffic")
+    # integer-pipe roofline: the product's butterflies (two forward and one
+    # inverse transform of M points per prime) at the butterfly rate measured
+    # live by the calibration kernel
+    bfly = 3 * logM * (M // 2) * np_
+    rate = ctx.butterfly_rate()
+    t_bound = bfly / rate * 1e3
+    int_pipe = {"butterflies": bfly, "rate_per_s": rate, "t_bound_ms": t_bound,
+                "frac": t_bound / ms_step,
+                "note": "31-bit modular butterfly from registers on every SM (gpu_butterfly_rate); "
+                        "frac = butterfly-only time at that rate / measured product time"}
     roofline = {"bound": "hbm", "kernel": dom, "achieved": kern[dom]["GBps"], "peak": peak,
                 "unit": "GB/s", "frac": kern[dom]["GBps"] / peak, "traffic": traffic,
-                "peak_kind": peak_kind,
+                "peak_kind": peak_kind, "int_pipe": int_pipe,
                 "pipeline": {"alg_bytes": alg_pipeline,
                              "achieved": alg_pipeline / (ms_step / 1e3) / 1e9,
                              "frac": alg_pipeline / (ms_step / 1e3) / 1e9 / peak},

@@ -100,6 +100,7 @@ SIGNATURES = {
     "_gpu_nmod_poly_divrem_mpn_ctx": (None, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_divrem_status": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
+    "gpu_butterfly_rate": (ctypes.c_int, [_CTX, ctypes.POINTER(ctypes.c_double)]),
     "gpu_mul_precomp_init_status": (ctypes.c_int, [_P, _P, _U, _U, _U, _Nmod, _CTX]),
     "_gpu_mul_precomp_init": (None, [_P, _P, _U, _U, _U, _Nmod, _CTX]),
     "_gpu_mul_precomp_clear": (None, [_P]),
@@ -448,6 +449,12 @@ class MpnCtx:
     @property
     def last_launches(self):
         return int(lib().gpu_mpn_ctx_last_launches(self.ptr))
+
+    def butterfly_rate(self):
+        """Measured 31-bit butterflies per second from registers (gpu_butterfly_rate)."""
+        v = ctypes.c_double()
+        _check(lib().gpu_butterfly_rate(self.ptr, ctypes.byref(v)))
+        return v.value
 
     def set_timing(self, on=True):
         """Per-kernel CUDA-event timing on the launching stream (resets totals)."""

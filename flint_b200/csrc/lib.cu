@@ -1210,6 +1210,40 @@ __global__ void k_fill_limbs(uint64_t *p, uint64_t n, uint64_t seed)
     }
 }
 
+int gpu_butterfly_rate(gpu_mpn_ctx_t R, double *per_s)
+{
+    Ctx *X = get_ctx(R);
+    if (!X || !per_s) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    const int blocks = X->nsm * 8, threads = 256;
+    uint32_t *buf = nullptr;
+    CU(cudaMalloc(&buf, (size_t)blocks * threads * 16 * sizeof(uint32_t)));
+    cudaStream_t st = X->stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::vector<float> t(5);
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
+    k_bfly_rate<<<blocks, threads, 0, st>>>(buf, X->T.twf, PRIMES[0], 17u);   // warm-up
+    for (int r = 0; r < (int)t.size() && !rc; r++) {
+        cudaEventRecord(e0, st);
+        k_bfly_rate<<<blocks, threads, 0, st>>>(buf, X->T.twf, PRIMES[0], 19u + r);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "calibration sync");
+        else cudaEventElapsedTime(&t[r], e0, e1);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    cudaFree(buf);
+    if (rc) return rc;
+    std::sort(t.begin(), t.end());
+    // butterflies per launch: every thread runs CAL_ITERS x 4 levels x 8
+    const double bfly = (double)blocks * threads * CAL_ITERS * 4 * 8;
+    *per_s = bfly / (t[t.size() / 2] * 1e-3);
+    return 0;
+}
+
 int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw, gpu_ulong bn, gpu_ulong bw,
                         const gpu_mul_config *cfg, int reps, double *ms)
 {

@@ -940,4 +940,37 @@ k_crt_carry(const uint32_t* __restrict__ res, int logM, uint64_t L, uint64_t zn,
     }
 }
 
+// ---------------------------------------------------------------------------
+// Calibration: the transforms' Gentleman-Sande butterfly (same form and pipe
+// mix as the row passes) in a register-only loop, 16 values per thread, four
+// levels per iteration -- the integer-pipe peak the product kernels are
+// measured against.  Every value is stored at the end (out holds gridDim.x *
+// blockDim.x * 16 words).
+constexpr int CAL_ITERS = 256;
+
+__global__ void __launch_bounds__(256)
+k_bfly_rate(uint32_t* __restrict__ out, const uint2* __restrict__ tw, uint32_t p, uint32_t seed)
+{
+    constexpr int NV = 16;
+    uint32_t x[NV];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int i = 0; i < NV; i++) x[i] = (seed * (t + 1) * (uint32_t)(2 * i + 7)) % p;
+    uint32_t w[4], wq[4];
+#pragma unroll
+    for (int l = 0; l < 4; l++) { w[l] = tw[1 + l].x; wq[l] = tw[1 + l].y; }
+    for (int it = 0; it < CAL_ITERS; it++) {
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+            const int h = 1 << l;
+#pragma unroll
+            for (int i = 0; i < NV; i++)
+                if (!(i & h)) bfly_gs<ROW_GS_FMA_ADDS>(x[i], x[i + h], w[l], wq[l], p);
+        }
+    }
+    uint32_t* o = out + (size_t)t * NV;
+#pragma unroll
+    for (int i = 0; i < NV; i++) o[i] = x[i];
+}
+
 }  // namespace fb

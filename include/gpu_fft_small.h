@@ -368,6 +368,14 @@ GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device_config(gpu_mpn_ctx_t R, uint6
                                                           gpu_ulong bw, gpu_ulong bn,
                                                           const gpu_mul_config *cfg, void *stream);
 
+/* Integer-pipe calibration (no counterpart in the reference): the rate, in
+   butterflies per second, of the transforms' 31-bit modular butterfly run
+   from registers only on every SM (median of five timed launches of about a
+   millisecond on the context's stream).  The product kernels' compute
+   roofline: a product of transform length M with np primes and two forward
+   and one inverse transform performs 3 log2(M) M/2 np butterflies. */
+GPU_FFT_SMALL_API int gpu_butterfly_rate(gpu_mpn_ctx_t R, double *per_s);
+
 /* Autotuner measurement: median device time (CUDA events on the context's
    stream, after one warm-up call) of `reps` products under cfg, on operands
    filled on the device from a fixed seed.  kind 0: an x bn-limb mpn product

@@ -166,3 +166,10 @@ def test_errors_are_reported(ctx):
     # the context stays usable after an error
     a = O.rand_limbs(1, 100)
     assert (ctx.mpn_mul(a, a) == O.gmp_mpn_mul(a, a)).all()
+
+
+def test_butterfly_rate_calibration(ctx):
+    """The integer-pipe calibration runs and reports a plausible rate (148 SMs
+    at up to ~2 GHz, nine instructions per butterfly from registers)."""
+    r = ctx.butterfly_rate()
+    assert 5e11 < r < 2e13
