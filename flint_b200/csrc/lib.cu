@@ -376,9 +376,19 @@ static int default_logC(int logM)
     if (logM <= LOG_MAXC) return logM;
     return std::max(LOG_MAXC - 1, logM - LOG_MAXR);
 }
+// Shortest row for a transform of 2^logM points: columns at most 2^11 long,
+// and with 32 or more columns (the column kernel's 2^14-word tiles of
+// 2^(14 - logR) columns) rows at least one tile wide, which below 2^14
+// points means at most 16 columns.
+static int min_logC(int logM)
+{
+    int lo = std::max(MIN_LOGM, logM - LOG_MAXR);
+    if (logM < LOG_MAXC) lo = std::max(lo, logM - 4);
+    return lo;
+}
 static bool valid_logC(int logM, int logC)
 {
-    return logC >= std::max(MIN_LOGM, logM - LOG_MAXR) && logC <= std::min(logM, LOG_MAXC);
+    return logC >= min_logC(logM) && logC <= std::min(logM, LOG_MAXC);
 }
 
 static LaunchShape make_shape(int logM, int logC = -1)

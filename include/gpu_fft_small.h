@@ -346,7 +346,8 @@ typedef struct {
     int route;   /* GPU_MUL_ROUTE_* */
     int np;      /* primes, minimal .. 6 */
     int logM;    /* transform length 2^logM, minimal .. 2^25 */
-    int logC;    /* four-step row length 2^logC, max(5, logM - 11) .. min(logM, 14) */
+    int logC;    /* four-step row length 2^logC, max(5, logM - 11) .. min(logM, 14); below
+                    2^14 points at most 16 columns (logC >= logM - 4) */
 } gpu_mul_config;
 
 /* Fills the zero fields of cfg with the defaults for an an x bn product and

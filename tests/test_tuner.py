@@ -27,6 +27,7 @@ def test_candidates_are_valid_and_include_default(r):
     for c in cs:
         if c.route == FB.ROUTE_NTT:
             assert max(5, c.logM - 11) <= c.logC <= min(c.logM, 14)
+            assert c.logM >= 14 or c.logM - c.logC <= 4
         f = tuner.features(r, c)
         assert f.shape == (tuner.N_FEATURES,) and np.isfinite(f).all()
 
@@ -42,6 +43,9 @@ def test_invalid_configs_are_rejected():
         FB.resolve_config(0, 1 << 20, 1, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 8))        # rows too short
     with pytest.raises(FB.GpuFftSmallError):
         FB.resolve_config(1, 10, 10, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0), 2, 2)
+    with pytest.raises(FB.GpuFftSmallError):                                         # 64 columns of
+        FB.resolve_config(0, 600, 500, FB.MulConfig(FB.ROUTE_NTT, 0, 11, 5))          # 32 below 2^14
+    assert FB.resolve_config(0, 600, 500, FB.MulConfig(FB.ROUTE_NTT, 0, 11, 7)).logC == 7
     c = FB.resolve_config(0, 1 << 20, 1 << 20)
     assert c.key() == (FB.ROUTE_NTT, 5, 21, 13)       # 2^13-point rows from 2^15 to 2^24
     assert FB.resolve_config(0, 1 << 24, 1 << 24).key() == (FB.ROUTE_NTT, 5, 25, 14)
