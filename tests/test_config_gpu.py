@@ -36,6 +36,43 @@ def test_mpn_every_candidate_exact(ctx, an, bn):
         assert (dz.cpu().numpy().view(np.uint64) == want).all(), c
 
 
+def _valid_logC(logM):
+    """Row lengths the validator accepts for a transform of 2^logM points."""
+    lo = max(5, logM - 11)
+    if logM < 14:
+        lo = max(lo, logM - 4)
+    return list(range(lo, min(logM, 14) + 1))
+
+
+@pytest.mark.parametrize("logM", list(range(5, 18)) + [20, 22])
+def test_mpn_every_row_length_exact(ctx, logM):
+    """Every (transform length, row length) a caller may configure -- not only
+    the tuner's candidates -- gives the exact product; row lengths just outside
+    the rule are rejected."""
+    torch = pytest.importorskip("torch")
+    an = (1 << (logM - 1)) - 3 if logM > 5 else 9
+    bn = max(1, (1 << (logM - 1)) - an + 7) if logM > 5 else 7
+    assert FB.mpn_mul_plan(an, bn)[1] <= logM
+    a = O.rand_limbs(an + logM, an)
+    b = O.rand_limbs(bn + 3 * logM, bn)
+    want = O.gmp_mpn_mul(a, b)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    dz = torch.empty(an + bn, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream()
+    for logC in _valid_logC(logM):
+        c = FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, logM, logC))
+        dz.fill_(-1)
+        ctx.mpn_mul_device_config(dz.data_ptr(), da.data_ptr(), an, db.data_ptr(), bn, c,
+                                  s.cuda_stream)
+        s.synchronize()
+        assert (dz.cpu().numpy().view(np.uint64) == want).all(), c
+    lo = _valid_logC(logM)[0]
+    if lo > 5:
+        with pytest.raises(FB.GpuFftSmallError):
+            FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, logM, lo - 1))
+
+
 def test_basecase_all_ones_and_operand_order(ctx):
     torch = pytest.importorskip("torch")
     s = torch.cuda.current_stream()
