@@ -150,3 +150,34 @@ def test_batch_longer_than_one_chunk(ctx):
         Z = dz.cpu().numpy().view(np.uint64)
     for i in sorted(set(range(0, count, 16)) | {7, 511, 512}):
         assert (Z[i] == O.negmul_python(X[i], Y[i], N)).all(), i
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_random_rings_and_batches(ctx, seed):
+    """Random ring sizes N (multiples of 64), requested digit counts (0, 16 ..
+    2^16) and batch counts; splits the primes cannot hold must be refused with
+    ENOPRIMES, every other product exact against Python."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(4000 + seed)
+    n = int(rng.integers(1, 6000))
+    N = 64 * n
+    m = int(rng.choice([0, 16, 32, 64, 256, 1024, 1 << 14, 1 << 16]))
+    if m and N % m:
+        m = 0
+    try:
+        C = FB.Mulmod2expp1(ctx, N, m)
+    except FB.GpuFftSmallError as e:
+        assert e.code in (FB.ENOPRIMES, FB.EINVAL)
+        return
+    with C:
+        assert C.m * C.b == N and 32 <= C.m <= (1 << 14) and C.np <= 6
+        count = int(rng.integers(1, 40))
+        X = _batch(n, count, 9000 + seed, n + 1)
+        Y = _batch(n, count, 9500 + seed, n + 1)
+        dx, dy = torch.from_numpy(X.view(np.int64)).cuda(), torch.from_numpy(Y.view(np.int64)).cuda()
+        dz = torch.empty_like(dx)
+        C.batch_device(dz.data_ptr(), dx.data_ptr(), dy.data_ptr(), count, None,
+                       torch.cuda.current_stream().cuda_stream)
+        Z = dz.cpu().numpy().view(np.uint64)
+    for i in range(0, count, max(1, count // 6)):
+        assert (Z[i] == O.negmul_python(X[i], Y[i], N)).all(), (N, m, count, i)
