@@ -313,16 +313,42 @@ __device__ __forceinline__ void cp_async4_full(uint32_t* dst, const uint32_t* sr
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src));
 }
 
+// 16 bytes, both addresses 16-byte aligned; bypasses L1 (.cg)
+__device__ __forceinline__ void cp_async16(uint32_t* dst, const uint32_t* src)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src));
+}
+
 // LOGE: log2 of the elements each thread owns in the row kernel's
-// contiguous pass (blockDim = nv C / 2^LOGE)
+// contiguous pass (blockDim = nv C / 2^LOGE).  UNP: a single row (nv = 1,
+// rows of at least 2^10 words) lands unpadded, as 16-byte copies that bypass
+// L1 -- 4x fewer copy instructions than the padded layout's 4-byte ones and
+// no L1 allocation; the first forward pass pads it (gs_pass_first_unpadded).
+// The row base and dst must be 16-byte aligned (residue planes and rows are
+// multiples of 2^10 words; dst is a row buffer at a multiple of padw(C)).
 template <int LOGC, int LOGE = 5>
+__device__ __forceinline__ constexpr bool rows_unpadded(int nv)
+{
+    return LOGE == 5 && LOGC >= 10 && nv == 1;
+}
+
+template <int LOGC, int LOGE = 5, bool UNP = false>
 __device__ __forceinline__ void rows_prefetch(uint32_t* dst, const uint32_t* __restrict__ base,
                                               int u0, int nv, int R)
 {
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
     constexpr int NSUB = C >> LOGE;
-    if (nv == 1 && NSUB % 32 == 0) {
+    if (UNP && rows_unpadded<LOGC, LOGE>(nv)) {
+        // blockDim == NSUB == C / 32: 16-byte chunk c = t + k NSUB, k < 8
+        const uint32_t* src = base + (size_t)u0 * C;
+#pragma unroll
+        for (int k = 0; k < (1 << LOGE) / 4; k++) {
+            const int c = threadIdx.x + k * NSUB;
+            cp_async16(dst + 4 * c, src + 4 * c);
+        }
+    } else if (nv == 1 && NSUB % 32 == 0) {
         // one row, blockDim == NSUB: element t + k NSUB, compile-time offsets
         const int t = threadIdx.x;
         const uint32_t* src = base + (size_t)u0 * C + t;
@@ -345,7 +371,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
        int logR, int nv, int np, const uint32_t* __restrict__ scale, int squaring,
        const InstDesc* __restrict__ desc, int ninst, int rows)
 {
-    extern __shared__ uint32_t sm[];
+    extern __shared__ __align__(16) uint32_t sm[];   // 16-byte copies land in the row buffers
     constexpr int C = 1 << LOGC;
     constexpr int PC = padw(C);
     constexpr int E = 1 << LOGE;          // elements per thread in the contiguous pass
@@ -379,8 +405,8 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         uint32_t* A;
         const uint32_t* B;
         decode(g, j, u0, A, B);
-        rows_prefetch<LOGC, LOGE>(sa_buf(0), A + ((size_t)j << logM), u0, nv, R);
-        if (!squaring) rows_prefetch<LOGC, LOGE>(sb, B + ((size_t)j << logM), u0, nv, R);
+        rows_prefetch<LOGC, LOGE, true>(sa_buf(0), A + ((size_t)j << logM), u0, nv, R);
+        if (!squaring) rows_prefetch<LOGC, LOGE, true>(sb, B + ((size_t)j << logM), u0, nv, R);
         else cp_async_commit();
     }
     int cur = 0;
@@ -401,13 +427,14 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         // (its last item stored from it before the barrier)
         cp_async_wait<0>();
         __syncthreads();
-        if (g2 < total) rows_prefetch<LOGC, LOGE>(sa_buf(cur ^ 1), A2 + ((size_t)j2 << logM), u2, nv, R);
+        if (g2 < total) rows_prefetch<LOGC, LOGE, true>(sa_buf(cur ^ 1), A2 + ((size_t)j2 << logM), u2, nv, R);
         else cp_async_commit();
 
         uint32_t xr[E];
         uint32_t breg[E];
         if (!squaring) {
-            gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
+            if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all2<LOGC, QMAX, LOGE, true>(sa, sb, nv, twf, p);
+            else gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
 #pragma unroll
             for (int m = 0; m < E; m++) {
                 xr[m] = sa[pb + m];
@@ -415,10 +442,11 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
             }
             gs_contig2<LOGE, ROW_GS_FMA_ADDS>(xr, breg, c_w32[j], p);
             __syncthreads();   // b fully read: refill it for the next item
-            if (g2 < total) rows_prefetch<LOGC, LOGE>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
+            if (g2 < total) rows_prefetch<LOGC, LOGE, true>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
             else cp_async_commit();
         } else {
-            gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
+            if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all<LOGC, 0, QMAX, LOGE, true>(sa, nv, twf, p);
+            else gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
 #pragma unroll
             for (int m = 0; m < E; m++) xr[m] = sa[pb + m];
             gs_contig<LOGE, ROW_GS_FMA_ADDS>(xr, c_w32[j], p);
@@ -434,8 +462,16 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
 #pragma unroll
         for (int m = 0; m < E; m++) sa[pb + m] = xr[m];
         __syncthreads();
-        ct_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twi, p);
         uint32_t* __restrict__ abase = A + ((size_t)j << logM);
+        if constexpr (LOGC > LOGE) {
+            if (nv == 1) {
+                // one row: the last inverse pass writes it to HBM directly
+                ct_strided_all_out<LOGC, QMAX, LOGE>(sa, twi, p, abase + (size_t)u0 * C);
+                cur ^= 1;
+                continue;
+            }
+        }
+        ct_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twi, p);
         if (nv == 1 && NSUB % 32 == 0) {
             uint32_t* dst = abase + (size_t)u0 * C + t;
             const uint32_t* s_ = sa + padw(t);

@@ -327,42 +327,89 @@ constexpr int balanced_pass()
     return (REM + (REM + QMAX - 1) / QMAX - 1) / ((REM + QMAX - 1) / QMAX);
 }
 
-template <int LOGL, int G, int QMAX, int H, int REM>
+// First forward pass of rows that landed unpadded (rows layout, one row per
+// block, blockDim = L / 32; the row kernel fills them with 16-byte copies,
+// which the padded layout's 33-word lines cannot take).  The first pass has
+// H = L / 2 and stride S = L / E, so sub-transform s covers s + m S: every
+// thread reads its 32 / E sub-transforms of each vector into registers, and
+// only after a barrier -- the padded positions overlap unpadded ones other
+// threads have yet to read -- runs the levels and stores them padded.
+template <int LOGL, int Q, int NVEC>
+__device__ __forceinline__ void gs_pass_first_unpadded(uint32_t* sx, uint32_t* sy, const uint2* __restrict__ tw,
+                                                       uint32_t p)
+{
+    constexpr int L = 1 << LOGL;
+    constexpr int E = 1 << Q;
+    constexpr int H = L / 2;
+    constexpr int S = H >> (Q - 1);
+    constexpr int IT = 32 / E;
+    static_assert(S == L / E && IT >= 1 && L % 32 == 0, "unsupported first pass");
+    uint32_t x[IT][E], y[NVEC == 2 ? IT : 1][NVEC == 2 ? E : 1];
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int s = threadIdx.x + it * (L / 32);
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            x[it][m] = sx[s + m * S];
+            if constexpr (NVEC == 2) y[it][m] = sy[s + m * S];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < IT; it++) {
+        const int s = threadIdx.x + it * (L / 32);
+        if constexpr (NVEC == 2) gs_strided_level2<Q, H, 0, ROW_GS_FMA_ADDS>(x[it], y[it], tw, s, p);
+        else gs_strided<Q, H, ROW_GS_FMA_ADDS>(x[it], tw, s, p);
+        const int pb = padw(s);
+#pragma unroll
+        for (int m = 0; m < E; m++) {
+            sx[pb + padw(m * S)] = x[it][m];
+            if constexpr (NVEC == 2) sy[pb + padw(m * S)] = y[it][m];
+        }
+    }
+}
+
+// UNP: the data landed unpadded (gs_pass_first_unpadded; rows layout, nv = 1)
+template <int LOGL, int G, int QMAX, int H, int REM, bool UNP = false>
 __device__ __forceinline__ void gs_passes(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
 {
     if constexpr (REM > 0) {
         constexpr int Q = balanced_pass<REM, QMAX>();
-        gs_pass_smem<LOGL, Q, H, G>(sm, nv, tw, p);
+        if constexpr (UNP) gs_pass_first_unpadded<LOGL, Q, 1>(sm, sm, tw, p);
+        else gs_pass_smem<LOGL, Q, H, G>(sm, nv, tw, p);
         __syncthreads();
         gs_passes<LOGL, G, QMAX, (H >> Q), REM - Q>(sm, nv, tw, p);
     }
 }
 
 // LOGE: levels of the contiguous (register) pass that follows, 5 or 4
-template <int LOGL, int G, int QMAX = (G ? 4 : 5), int LOGE = 5>
+template <int LOGL, int G, int QMAX = (G ? 4 : 5), int LOGE = 5, bool UNP = false>
 __device__ __forceinline__ void gs_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ tw, uint32_t p)
 {
-    if constexpr (LOGL > LOGE) gs_passes<LOGL, G, QMAX, (1 << (LOGL - 1)), LOGL - LOGE>(sm, nv, tw, p);
+    static_assert(!UNP || (G == 0 && LOGE == 5), "unpadded landing: rows layout, 32 per thread");
+    if constexpr (LOGL > LOGE) gs_passes<LOGL, G, QMAX, (1 << (LOGL - 1)), LOGL - LOGE, UNP>(sm, nv, tw, p);
 }
 
-template <int LOGL, int QMAX, int H, int REM>
+template <int LOGL, int QMAX, int H, int REM, bool UNP = false>
 __device__ __forceinline__ void gs_passes2(uint32_t* sx, uint32_t* sy, int nv, const uint2* __restrict__ tw,
                                            uint32_t p)
 {
     if constexpr (REM > 0) {
         constexpr int Q = balanced_pass<REM, QMAX>();
-        gs_pass_smem2<LOGL, Q, H>(sx, sy, nv, tw, p);
+        if constexpr (UNP) gs_pass_first_unpadded<LOGL, Q, 2>(sx, sy, tw, p);
+        else gs_pass_smem2<LOGL, Q, H>(sx, sy, nv, tw, p);
         __syncthreads();
         gs_passes2<LOGL, QMAX, (H >> Q), REM - Q>(sx, sy, nv, tw, p);
     }
 }
 
 // gs_strided_all for two row buffers at once (rows layout)
-template <int LOGL, int QMAX = 5, int LOGE = 5>
+template <int LOGL, int QMAX = 5, int LOGE = 5, bool UNP = false>
 __device__ __forceinline__ void gs_strided_all2(uint32_t* sx, uint32_t* sy, int nv, const uint2* __restrict__ tw,
                                                 uint32_t p)
 {
-    if constexpr (LOGL > LOGE) gs_passes2<LOGL, QMAX, (1 << (LOGL - 1)), LOGL - LOGE>(sx, sy, nv, tw, p);
+    static_assert(!UNP || LOGE == 5, "unpadded landing: 32 per thread");
+    if constexpr (LOGL > LOGE) gs_passes2<LOGL, QMAX, (1 << (LOGL - 1)), LOGL - LOGE, UNP>(sx, sy, nv, tw, p);
 }
 
 // Strided part of the inverse transform (half-sizes 32 .. L/2), after the
@@ -382,6 +429,58 @@ template <int LOGL, int G, int QMAX = (G ? 4 : 5), int LOGE = 5>
 __device__ __forceinline__ void ct_strided_all(uint32_t* sm, int nv, const uint2* __restrict__ twi, uint32_t p)
 {
     if constexpr (LOGL > LOGE) ct_passes<LOGL, G, QMAX, (1 << LOGE), LOGL - LOGE>(sm, nv, twi, p);
+}
+
+// The last inverse pass of one row (rows layout, one vector) with its output
+// written straight to `out` (natural order) instead of back to shared
+// memory: sub-transform s holds positions base + m H, consecutive threads
+// take consecutive s, so each warp stores 32 consecutive words per m.
+template <int LOGL, int Q, int H>
+__device__ __forceinline__ void ct_pass_smem_out(const uint32_t* sm, const uint2* __restrict__ twi, uint32_t p,
+                                                 uint32_t* __restrict__ out)
+{
+    constexpr int L = 1 << LOGL;
+    constexpr int E = 1 << Q;
+    constexpr int S = H;
+    constexpr int NSUB = L / E;
+    static_assert(S % 32 == 0, "unsupported pass stride");
+#pragma unroll PASS_UNROLL
+    for (int s = threadIdx.x; s < NSUB; s += blockDim.x) {
+        const int jj0 = s & (S - 1);
+        const int base = (s / S) * (S * E) + jj0;
+        const int pb = padw(base);
+        uint32_t x[E];
+#pragma unroll
+        for (int m = 0; m < E; m++) x[m] = sm[pb + padw(m * S)];
+        ct_strided<Q, H, ROW_CT_FMA_ADDS>(x, twi, jj0, p);
+#pragma unroll
+        for (int m = 0; m < E; m++) out[base + m * S] = x[m];
+    }
+}
+
+template <int LOGL, int QMAX, int H, int REM>
+__device__ __forceinline__ void ct_passes_out(uint32_t* sm, const uint2* __restrict__ twi, uint32_t p,
+                                              uint32_t* __restrict__ out)
+{
+    constexpr int Q = balanced_pass<REM, QMAX>();
+    if constexpr (REM > Q) {
+        ct_pass_smem<LOGL, Q, H, 0>(sm, 1, twi, p);
+        __syncthreads();
+        ct_passes_out<LOGL, QMAX, (H << Q), REM - Q>(sm, twi, p, out);
+    } else {
+        ct_pass_smem_out<LOGL, Q, H>(sm, twi, p, out);
+    }
+}
+
+// ct_strided_all for one row (rows layout, nv = 1) whose final pass stores
+// the row to global memory at `out`; needs LOGL > LOGE.  The shared buffer
+// is read, not written, by the final pass.
+template <int LOGL, int QMAX = 5, int LOGE = 5>
+__device__ __forceinline__ void ct_strided_all_out(uint32_t* sm, const uint2* __restrict__ twi, uint32_t p,
+                                                   uint32_t* __restrict__ out)
+{
+    static_assert(LOGL > LOGE, "row shorter than the contiguous pass");
+    ct_passes_out<LOGL, QMAX, (1 << LOGE), LOGL - LOGE>(sm, twi, p, out);
 }
 
 }  // namespace fb
