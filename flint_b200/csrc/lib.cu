@@ -820,7 +820,7 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     if (rc) return rc;
     uint32_t *ra = X->d_res, *rb = X->d_res + (size_t)np * M;
     const uint64_t zn = hi;   // limbs produced: [base, hi)
-    constexpr int THREADS = 256, TILE = 4 * THREADS;
+    constexpr int THREADS = CRT_THREADS, TILE = CRT_TILE;
     const size_t tiles = (zn - base + TILE - 1) / TILE;
     rc = ensure_status(X, tiles);
     if (rc) return rc;
@@ -1520,7 +1520,7 @@ constexpr int NA_LOG_MAXM = 18;
 constexpr uint64_t NA_MAX_LIMBS = ((uint64_t)1 << NA_LOG_MAXM) + 1;
 constexpr int NA_NP = 5;
 constexpr size_t NA_RES_WORDS = (size_t)2 * NA_NP << NA_LOG_MAXM;
-constexpr int NA_TILES = (int)((NA_MAX_LIMBS + 1023) / 1024);
+constexpr int NA_TILES = (int)((NA_MAX_LIMBS + CRT_TILE - 1) / CRT_TILE);
 
 // scratch: residues of both operands, look-back status, ticket, error flag
 static __device__ __align__(256) uint32_t na_scratch[NA_RES_WORDS + NA_TILES + 8];
@@ -1755,7 +1755,7 @@ int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong
     const size_t M = (size_t)1 << logM;
     uint32_t *ra = D.res, *rb = D.res + (size_t)NA_NP * M;
     const uint64_t zn = an + bn;
-    constexpr int THREADS = 256, TILE = 4 * THREADS;
+    constexpr int THREADS = CRT_THREADS, TILE = CRT_TILE;
     const size_t tiles = (zn + TILE - 1) / TILE;
     // the scratch keeps the previous call's contents: clear the look-back
     // status, the tile ticket and the error flag
