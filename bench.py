@@ -571,6 +571,43 @@ def kernel_bytes(name, an, bn, np_, M, L):
     }[name]
 
 
+def bench_pipe(torch, FB, a, b, z, steps, dist, dev, depth=4):
+    """Host-to-host throughput of a stream of products through gpu_mpn_pipe_*:
+    each product has its own pinned input and output buffers (depth sets in
+    rotation), the timed region runs from the first submission to the last
+    completed download (host clock, fill and drain included), and every
+    output is compared with the device-resident result."""
+    an, bn = len(a), len(b)
+    sets = [(torch.from_numpy(a.view(np.int64)).pin_memory(), torch.from_numpy(b.view(np.int64)).pin_memory(),
+             torch.empty(an + bn, dtype=torch.int64).pin_memory()) for _ in range(depth)]
+    nsteps = max(4 * depth, min(steps, 12))
+    with FB.MpnPipe(depth) as P:
+        for ha, hb, hz in sets:                     # warm-up: scratch growth in every slot
+            P.wait(P.submit(ha, hb, out=hz))
+        for _, _, hz in sets:
+            hz.zero_()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        pend = []
+        for k in range(nsteps):
+            ha, hb, hz = sets[k % depth]
+            if len(pend) == depth:                  # the set is reused: its product must be home
+                P.wait(pend.pop(0))
+            pend.append(P.submit(ha, hb, out=hz))
+        for t in pend:
+            P.wait(t)
+        s = (time.perf_counter() - t0) / nsteps
+    s = max_over_ranks(s, dist, dev)
+    ok = all(bool(np.array_equal(hz.numpy().view(np.uint64), z)) for _, _, hz in sets)
+    return {"unit": "Gbit/s", "s_per_step": s, "depth": depth, "steps": nsteps,
+            "h2d_bytes_per_step": 8 * (an + bn), "d2h_bytes_per_step": 8 * (an + bn),
+            "matches_device": ok,
+            "api": "gpu_mpn_pipe_submit / gpu_mpn_pipe_wait (pinned host buffers, one set per slot)",
+            "note": "host-clock throughput of a stream of host-resident products; one product's "
+                    "download overlaps the next one's upload and kernels (full-duplex PCIe)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -696,6 +733,10 @@ def main():
         e2e_step()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     e2e_s = max_over_ranks(e2e_s, dist, dev)
+    # the same products streamed through a pipeline of host-pointer products
+    pipelined = bench_pipe(torch, FB, a, b, z, args.steps, dist, dev)
+    pipe_s = pipelined.pop("s_per_step")
+    pipelined.update(value=world * gbits_step / pipe_s, ms_per_step=pipe_s * 1e3)
     # the batch, stream and transformed-operand legs are single-GPU
     # measurements: run at N = 1 only
     batch = stream_res = precomp = negacyclic = None
@@ -774,6 +815,7 @@ def main():
         "e2e": {"value": world * gbits_step / e2e_s, "unit": "Gbit/s",
                 "h2d_bytes_per_step": 8 * (an + bn), "d2h_bytes_per_step": 8 * (an + bn),
                 "ms_per_step": e2e_s * 1e3},
+        "e2e_pipelined": pipelined,
         "gpu_launches": 4 * args.steps,
         "gpu_launches_note": "headline product only; the batch object counts its own",
         "roofline": roofline,

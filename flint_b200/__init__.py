@@ -90,6 +90,10 @@ SIGNATURES = {
     "gpu_mpn_ctx_clear": (None, [_CTX]),
     "gpu_mpn_ctx_mpn_mul": (None, [_CTX, _P, _P, _U, _P, _U]),
     "gpu_mpn_ctx_mpn_mul_status": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U]),
+    "gpu_mpn_pipe_init": (ctypes.c_int, [_CTX, ctypes.c_int]),
+    "gpu_mpn_pipe_submit": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, ctypes.POINTER(ctypes.c_longlong)]),
+    "gpu_mpn_pipe_wait": (ctypes.c_int, [_CTX, ctypes.c_longlong]),
+    "gpu_mpn_pipe_clear": (None, [_CTX]),
     "_gpu_mpn_ctx_mpn_mul_range": (None, [_CTX, _P, _U, _U, _P, _U, _P, _U]),
     "gpu_mpn_mul_device": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, _P]),
     "gpu_mpn_mul_device_noalloc": (ctypes.c_int, [_P, _P, _U, _P, _U, _P]),
@@ -466,6 +470,69 @@ class MpnCtx:
         cnt = (ctypes.c_long * 8)()
         n = lib().gpu_mpn_ctx_kernel_times(self.ptr, ms, cnt, 8)
         return {KERNEL_SLOTS[k]: (ms[k], cnt[k]) for k in range(n)}
+
+
+class MpnPipe:
+    """A pipeline of host-pointer products (gpu_mpn_pipe_*): `depth` slots
+    take submitted products in turn, so one product's download, the next
+    one's upload and another one's kernels overlap.  submit() returns a
+    ticket at once; wait(ticket) returns the product (the array z) when it
+    is complete.  The operand and output arrays are kept referenced until
+    their ticket is waited for; pinned host memory (e.g. torch's
+    pin_memory()) makes the copies asynchronous."""
+
+    def __init__(self, depth=2):
+        self._c = _Ctx()   # same one-pointer layout as the pipeline handle
+        _check(lib().gpu_mpn_pipe_init(ctypes.byref(self._c), depth))
+        self.depth = depth
+        self._held = {}
+
+    def submit(self, a, b, out=None):
+        """Queue a * b; a, b, out: 1-D uint64 arrays or pinned torch int64
+        tensors (then out is required).  Returns the ticket."""
+        if hasattr(a, "data_ptr"):
+            an, bn = a.numel(), b.numel()
+            pa, pb, pz, z = a.data_ptr(), b.data_ptr(), out.data_ptr(), out
+            if out.numel() < an + bn:
+                raise ValueError("output shorter than an + bn")
+        else:
+            a = _limbs(a)
+            b = a if b is a else _limbs(b)
+            an, bn = len(a), len(b)
+            z = np.empty(an + bn, dtype=np.uint64) if out is None else out
+            if len(z) < an + bn or z.dtype != np.uint64 or not z.flags.c_contiguous:
+                raise ValueError("output must be a contiguous uint64 array of an + bn limbs")
+            pa, pb, pz = a.ctypes.data, b.ctypes.data, z.ctypes.data
+        t = ctypes.c_longlong()
+        _check(lib().gpu_mpn_pipe_submit(ctypes.byref(self._c), pz, pa, an, pb, bn, ctypes.byref(t)))
+        self._held[t.value] = (a, b, z)
+        return t.value
+
+    def wait(self, ticket):
+        """The product of `ticket` once it is complete."""
+        try:
+            _check(lib().gpu_mpn_pipe_wait(ctypes.byref(self._c), ticket))
+        finally:
+            held = self._held.pop(ticket, None)
+        return held[2] if held else None
+
+    def close(self):
+        if self._c.impl:
+            lib().gpu_mpn_pipe_clear(ctypes.byref(self._c))
+            self._c.impl = None
+            self._held.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class MpnBatch:

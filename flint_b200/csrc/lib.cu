@@ -22,6 +22,7 @@
 #include <mutex>
 #include <string>
 #include <vector>
+#include <unordered_map>
 
 using namespace fb;
 
@@ -899,8 +900,12 @@ static int ensure_copy_stream(Ctx *X)
     return 0;
 }
 
-static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
-                        const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
+// Host-pointer product, queued: a's upload on the compute stream, b's on the
+// copy stream, the kernels, and the result's download in chunks on the copy
+// stream.  Returns once all of it is queued; mpn_mul_host_finish waits for
+// the result and checks the device error flag.
+static int mpn_mul_host_issue(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
+                              const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
 {
     if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
     if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
@@ -951,12 +956,58 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
             cudaStreamSynchronize(C);
             return rc;
         }
-        CU(cudaStreamSynchronize(C));
     }
-    rc = check_device_error(X);
+    return 0;
+}
+
+// The second half of a host-pointer product (same arguments as the issue):
+// the download is the last work queued on the copy stream, after the
+// kernels on the compute stream.
+static int mpn_mul_host_finish(Ctx *X, gpu_ulong *z, gpu_ulong an, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
+{
+    if (X->copy_stream) CU(cudaStreamSynchronize(X->copy_stream));
+    int rc = check_device_error(X);
     if (rc) return rc;
+    const gpu_ulong zn = an + bn;
     if (hi > zn) memset(z + (zn > lo ? zn - lo : 0), 0, (hi - std::max<gpu_ulong>(zn, lo)) * 8);
     return 0;
+}
+
+static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
+                        const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
+{
+    int rc = mpn_mul_host_issue(X, z, a, an, b, bn, lo, hi);
+    if (rc) return rc;
+    return mpn_mul_host_finish(X, z, an, bn, lo, hi);
+}
+
+// ---------------------------------------------------------------------------
+// Pipelines of host-pointer products: a ring of `depth` contexts (slots),
+// each with its own scratch and streams, takes products in turn, so that one
+// product's download, the next one's upload and a third one's kernels run at
+// the same time (PCIe is full duplex; copies and kernels use different
+// engines).  A submission to a busy slot first completes the product that
+// slot holds; the status of a completed product is kept until its ticket is
+// waited for (once).
+struct Pipe {
+    std::vector<Ctx *> slot;
+    std::vector<long long> cur;           // ticket in flight on the slot (-1: none)
+    std::unordered_map<long long, int> finished;   // completed, not yet waited: status
+    struct Pending { gpu_ulong *z; gpu_ulong an, bn; };
+    std::vector<Pending> pend;
+    long long next = 0;
+};
+
+static int pipe_complete(Pipe *P, int s)
+{
+    if (P->cur[s] < 0) return 0;
+    Ctx *X = P->slot[s];
+    const Pipe::Pending &q = P->pend[s];
+    int rc = bind_device(X);
+    if (!rc) rc = mpn_mul_host_finish(X, q.z, q.an, q.bn, 0, q.an + q.bn);
+    P->finished[P->cur[s]] = rc;
+    P->cur[s] = -1;
+    return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -1024,6 +1075,72 @@ void gpu_mpn_ctx_mpn_mul(gpu_mpn_ctx_t R, gpu_ulong *z, const gpu_ulong *a, gpu_
 {
     int rc = gpu_mpn_ctx_mpn_mul_status(R, z, a, an, b, bn);
     if (rc) raise_error(rc);
+}
+
+int gpu_mpn_pipe_init(gpu_mpn_pipe_t R, int depth)
+{
+    R->impl = nullptr;
+    if (depth < 1 || depth > GPU_MPN_PIPE_MAX_DEPTH)
+        return set_error(GPU_FFT_SMALL_EINVAL, "pipeline depth %d outside 1..%d", depth, GPU_MPN_PIPE_MAX_DEPTH);
+    Pipe *P = new Pipe;
+    for (int s = 0; s < depth; s++) {
+        Ctx *X = nullptr;
+        int rc = ctx_create(&X, 0);
+        if (!rc) rc = ensure_copy_stream(X);
+        if (rc) {
+            if (X) ctx_destroy(X);
+            for (Ctx *Y : P->slot) ctx_destroy(Y);
+            delete P;
+            return rc;
+        }
+        P->slot.push_back(X);
+    }
+    P->cur.assign(depth, -1);
+    P->pend.assign(depth, Pipe::Pending{nullptr, 0, 0});
+    R->impl = P;
+    return 0;
+}
+
+int gpu_mpn_pipe_submit(gpu_mpn_pipe_t R, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
+                        const gpu_ulong *b, gpu_ulong bn, long long *ticket)
+{
+    Pipe *P = (Pipe *)R->impl;
+    if (!P || !ticket) return set_error(GPU_FFT_SMALL_EINVAL, "pipeline not initialised");
+    if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
+    const int s = (int)(P->next % (long long)P->slot.size());
+    pipe_complete(P, s);   // its status stays with its own ticket
+    int rc = mpn_mul_host_issue(P->slot[s], z, a, an, b, bn, 0, an + bn);
+    if (rc) return rc;
+    P->cur[s] = P->next;
+    P->pend[s] = Pipe::Pending{z, an, bn};
+    *ticket = P->next++;
+    return 0;
+}
+
+int gpu_mpn_pipe_wait(gpu_mpn_pipe_t R, long long ticket)
+{
+    Pipe *P = (Pipe *)R->impl;
+    if (!P) return set_error(GPU_FFT_SMALL_EINVAL, "pipeline not initialised");
+    if (ticket < 0 || ticket >= P->next) return set_error(GPU_FFT_SMALL_EINVAL, "unknown ticket %lld", ticket);
+    const int s = (int)(ticket % (long long)P->slot.size());
+    if (P->cur[s] == ticket) pipe_complete(P, s);
+    auto it = P->finished.find(ticket);
+    if (it == P->finished.end()) return set_error(GPU_FFT_SMALL_EINVAL, "ticket %lld already waited for", ticket);
+    const int rc = it->second;
+    P->finished.erase(it);
+    return rc;
+}
+
+void gpu_mpn_pipe_clear(gpu_mpn_pipe_t R)
+{
+    Pipe *P = (Pipe *)R->impl;
+    if (!P) return;
+    for (size_t s = 0; s < P->slot.size(); s++) {
+        pipe_complete(P, (int)s);
+        ctx_destroy(P->slot[s]);
+    }
+    delete P;
+    R->impl = nullptr;
 }
 
 void _gpu_mpn_ctx_mpn_mul_range(gpu_mpn_ctx_t R, gpu_ulong *z, gpu_ulong lo, gpu_ulong hi,

@@ -85,6 +85,33 @@ GPU_FFT_SMALL_API int gpu_mpn_ctx_mpn_mul_status(gpu_mpn_ctx_t R, gpu_ulong *z,
                                const gpu_ulong *a, gpu_ulong an,
                                const gpu_ulong *b, gpu_ulong bn);
 
+/* Pipelines of host-pointer products (no counterpart in the reference, whose
+   calls return with the product done).  A pipeline holds `depth` contexts
+   (slots, 1..GPU_MPN_PIPE_MAX_DEPTH) that take submitted products in turn,
+   so one product's download, the next one's upload and another one's kernels
+   overlap; from pinned host memory the copies run asynchronously, from
+   pageable memory a submission waits for its uploads.
+   gpu_mpn_pipe_submit queues z[0, an+bn) = a * b (an, bn >= 1) and returns
+   a ticket; a, b and z must stay valid and unchanged until the ticket has
+   been waited for.  A submission to a busy slot first completes the product
+   that slot holds.  gpu_mpn_pipe_wait returns the product's status once z
+   holds it; every ticket is waited for once (a second wait, or an unknown
+   ticket, is EINVAL), and the statuses of completed products are kept
+   until then.
+   gpu_mpn_pipe_clear completes every product in flight and frees the
+   pipeline.  Not reentrant, like a context. */
+#define GPU_MPN_PIPE_MAX_DEPTH 4
+typedef struct {
+    void *impl;
+} gpu_mpn_pipe_struct;
+typedef gpu_mpn_pipe_struct gpu_mpn_pipe_t[1];
+GPU_FFT_SMALL_API int gpu_mpn_pipe_init(gpu_mpn_pipe_t P, int depth);
+GPU_FFT_SMALL_API int gpu_mpn_pipe_submit(gpu_mpn_pipe_t P, gpu_ulong *z,
+                        const gpu_ulong *a, gpu_ulong an,
+                        const gpu_ulong *b, gpu_ulong bn, long long *ticket);
+GPU_FFT_SMALL_API int gpu_mpn_pipe_wait(gpu_mpn_pipe_t P, long long ticket);
+GPU_FFT_SMALL_API void gpu_mpn_pipe_clear(gpu_mpn_pipe_t P);
+
 /* Limbs [lo, hi) of a * b into z[0, hi-lo), zero beyond an + bn.  Replaces
    _mpn_ctx_mpn_mul_range (src/fft_small.h:462, src/fft_small/mpn_mul.c:
    1617-1978) with its contract (src/fft_small/test/t-mpn_mulmid.c): exact for

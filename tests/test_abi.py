@@ -87,6 +87,17 @@ def test_fails_loudly_without_gpu():
     with pytest.raises(FB.GpuFftSmallError) as e:
         FB.MpnCtx()
     assert e.value.code == FB.ECUDA
+    # a pipeline of host-pointer products builds its slots from contexts
+    with pytest.raises(FB.GpuFftSmallError) as e:
+        FB.MpnPipe(2)
+    assert e.value.code == FB.ECUDA
+
+
+def test_pipe_depth_is_checked():
+    for depth in (0, 5):
+        with pytest.raises(FB.GpuFftSmallError) as e:
+            FB.MpnPipe(depth)
+        assert e.value.code == FB.EINVAL
 
 
 def test_missing_library_is_an_error(monkeypatch):
