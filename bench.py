@@ -47,10 +47,10 @@ NS_LIMB_BITS = 64
 # profiles/*_mpn24.md); for another size the figure is scaled by M / 2^25
 # (traffic grows in proportion to the residue points).
 NCU_TRAFFIC_2P25 = {
-    "k_fwd_cols": 0.269222e9 + 1.291399e9,
-    "k_rows": 1.343594e9 + 0.626662e9,
-    "k_inv_cols": 0.671535e9 + 0.621226e9,
-    "k_crt_carry": 0.671245e9 + 0.244851e9,
+    "k_fwd_cols": 0.269502e9 + 1.291129e9,
+    "k_rows": 1.343848e9 + 0.625707e9,
+    "k_inv_cols": 0.671660e9 + 0.617331e9,
+    "k_crt_carry": 0.671662e9 + 0.244607e9,
 }
 
 
