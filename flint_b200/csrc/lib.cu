@@ -162,6 +162,7 @@ struct Ctx {
     DevTables T{};
     uint32_t *d_scale = nullptr;          // [np][logM][MAX_NP] pointwise scales
     int *d_err = nullptr;
+    int *h_err = nullptr;                 // pinned copy of *d_err, read after a host-pointer product
     unsigned long long *d_ticket = nullptr;
     unsigned long long ticket_base = 0;
     uint32_t *d_status = nullptr;
@@ -466,10 +467,12 @@ static int ctx_create(Ctx **out, gpu_ulong p)
         cudaError_t e1 = cudaMalloc(&X->d_scale, sizeof(uint32_t) * (MAX_NP + 1) * (LOG_MAXM + 1) * MAX_NP);
         cudaError_t e2 = cudaMalloc(&X->d_err, sizeof(int));
         cudaError_t e3 = cudaMalloc(&X->d_ticket, sizeof(unsigned long long));
-        if (e1 || e2 || e3) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaMalloc of context state failed");
+        cudaError_t e4 = cudaHostAlloc(&X->h_err, sizeof(int), cudaHostAllocDefault);
+        if (e1 || e2 || e3 || e4) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaMalloc of context state failed");
         else {
             cudaMemset(X->d_err, 0, sizeof(int));
             cudaMemset(X->d_ticket, 0, sizeof(unsigned long long));
+            *X->h_err = 0;
         }
     }
     if (!rc) rc = upload_scales(X);
@@ -535,6 +538,7 @@ static void ctx_destroy(Ctx *X)
     cudaFree(X->d_tables);
     cudaFree(X->d_scale);
     cudaFree(X->d_err);
+    if (X->h_err) cudaFreeHost(X->h_err);
     cudaFree(X->d_ticket);
     cudaFree(X->d_status);
     cudaFree(X->d_res);
@@ -900,12 +904,22 @@ static int ensure_copy_stream(Ctx *X)
     return 0;
 }
 
+// Copy streams shared by several contexts (a pipeline): all uploads on one
+// stream and all downloads on another, so each direction of the link moves
+// one product at a time; per-product events order them with the kernels.
+struct HostLinks {
+    cudaStream_t up, down;
+    cudaEvent_t a_in, b_in, done;   // a uploaded, b uploaded, last download queued
+};
+
 // Host-pointer product, queued: a's upload on the compute stream, b's on the
-// copy stream, the kernels, and the result's download in chunks on the copy
-// stream.  Returns once all of it is queued; mpn_mul_host_finish waits for
-// the result and checks the device error flag.
+// copy stream (or both on links->up), the kernels, and the result's download
+// in chunks on the copy stream (or links->down).  Returns once all of it is
+// queued; mpn_mul_host_finish waits for the result and checks the device
+// error flag.
 static int mpn_mul_host_issue(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
-                              const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
+                              const gpu_ulong *b, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi,
+                              const HostLinks *links = nullptr)
 {
     if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
     if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
@@ -923,20 +937,33 @@ static int mpn_mul_host_issue(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulon
         rc = ensure_copy_stream(X);
         if (rc) return rc;
         cudaStream_t S = X->stream, C = X->copy_stream;
-        // a on the compute stream; b on the copy stream once a is in (the two
-        // copies share the link), while a's column pass runs
-        CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, S));
+        const cudaStream_t down = links ? links->down : C;
         cudaEvent_t b_ready = nullptr;
-        if (!sq) {
-            CU(cudaEventRecord(X->ev_copy[0], S));
-            CU(cudaStreamWaitEvent(C, X->ev_copy[0], 0));
-            CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, C));
-            CU(cudaEventRecord(X->ev_copy[1], C));
-            b_ready = X->ev_copy[1];
+        if (links) {
+            CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, links->up));
+            CU(cudaEventRecord(links->a_in, links->up));
+            CU(cudaStreamWaitEvent(S, links->a_in, 0));
+            if (!sq) {
+                CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, links->up));
+                CU(cudaEventRecord(links->b_in, links->up));
+                b_ready = links->b_in;
+            }
+        } else {
+            // a on the compute stream; b on the copy stream once a is in (the
+            // two copies share the link), while a's column pass runs
+            CU(cudaMemcpyAsync(da, a, an * 8, cudaMemcpyHostToDevice, S));
+            if (!sq) {
+                CU(cudaEventRecord(X->ev_copy[0], S));
+                CU(cudaStreamWaitEvent(C, X->ev_copy[0], 0));
+                CU(cudaMemcpyAsync(db, b, bn * 8, cudaMemcpyHostToDevice, C));
+                CU(cudaEventRecord(X->ev_copy[1], C));
+                b_ready = X->ev_copy[1];
+            }
         }
-        // the result comes back in chunks on the copy stream, each as soon as
-        // its CRT launch has finished
-        struct Back { Ctx *X; uint64_t *z, *dz; uint64_t lo; int k; int rc; } bk{X, z, dz, lo, 0, 0};
+        // the result comes back in chunks on the download stream, each as
+        // soon as its CRT launch has finished
+        struct Back { Ctx *X; cudaStream_t down; uint64_t *z, *dz; uint64_t lo; int k; int rc; } bk{
+            X, down, z, dz, lo, 0, 0};
         CrtChunks ch;
         ch.chunks = lo == 0 ? 4 : 1;
         ch.arg = &bk;
@@ -944,16 +971,23 @@ static int mpn_mul_host_issue(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulon
             Back &B = *(Back *)p;
             if (B.rc || l1 <= l0) return;
             cudaEvent_t e = B.X->ev_copy[2 + (B.k++ % 7)];
-            if (cudaEventRecord(e, B.X->stream) != cudaSuccess ||
-                cudaStreamWaitEvent(B.X->copy_stream, e, 0) != cudaSuccess ||
+            if (cudaEventRecord(e, B.X->stream) != cudaSuccess || cudaStreamWaitEvent(B.down, e, 0) != cudaSuccess ||
                 cudaMemcpyAsync(B.z + (l0 - B.lo), B.dz + (l0 - B.lo), (l1 - l0) * 8, cudaMemcpyDeviceToHost,
-                                B.X->copy_stream) != cudaSuccess)
+                                B.down) != cudaSuccess)
                 B.rc = set_error(GPU_FFT_SMALL_ECUDA, "result copy");
         };
         rc = mpn_mul_enqueue(X, dz, da, an, db, bn, S, nullptr, lo, top, b_ready, &ch);
         if (!rc) rc = bk.rc;
+        // the error flag follows the result home (pinned word: no staging copy
+        // that would queue behind other products' transfers)
+        if (!rc && cudaMemcpyAsync(X->h_err, X->d_err, sizeof(int), cudaMemcpyDeviceToHost, down) != cudaSuccess)
+            rc = set_error(GPU_FFT_SMALL_ECUDA, "error flag copy");
+        if (!rc && links && cudaEventRecord(links->done, down) != cudaSuccess)
+            rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventRecord");
         if (rc) {
-            cudaStreamSynchronize(C);
+            if (links) cudaStreamSynchronize(links->up);
+            cudaStreamSynchronize(S);
+            cudaStreamSynchronize(down);
             return rc;
         }
     }
@@ -963,11 +997,23 @@ static int mpn_mul_host_issue(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulon
 // The second half of a host-pointer product (same arguments as the issue):
 // the download is the last work queued on the copy stream, after the
 // kernels on the compute stream.
-static int mpn_mul_host_finish(Ctx *X, gpu_ulong *z, gpu_ulong an, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi)
+static int mpn_mul_host_finish(Ctx *X, gpu_ulong *z, gpu_ulong an, gpu_ulong bn, gpu_ulong lo, gpu_ulong hi,
+                               const HostLinks *links = nullptr)
 {
-    if (X->copy_stream) CU(cudaStreamSynchronize(X->copy_stream));
-    int rc = check_device_error(X);
-    if (rc) return rc;
+    int rc = 0;
+    if (links) CU(cudaEventSynchronize(links->done));
+    else if (X->copy_stream) CU(cudaStreamSynchronize(X->copy_stream));
+    if (an + bn > lo && std::min<gpu_ulong>(hi, an + bn) > lo) {
+        // the flag was copied behind the last download
+        if (*X->h_err) {
+            *X->h_err = 0;
+            cudaMemsetAsync(X->d_err, 0, sizeof(int), X->stream);
+            return set_error(GPU_FFT_SMALL_ETIMEOUT, "carry look-back wait exceeded its limit");
+        }
+    } else {
+        rc = check_device_error(X);
+        if (rc) return rc;
+    }
     const gpu_ulong zn = an + bn;
     if (hi > zn) memset(z + (zn > lo ? zn - lo : 0), 0, (hi - std::max<gpu_ulong>(zn, lo)) * 8);
     return 0;
@@ -983,14 +1029,20 @@ static int mpn_mul_host(Ctx *X, gpu_ulong *z, const gpu_ulong *a, gpu_ulong an,
 
 // ---------------------------------------------------------------------------
 // Pipelines of host-pointer products: a ring of `depth` contexts (slots),
-// each with its own scratch and streams, takes products in turn, so that one
-// product's download, the next one's upload and a third one's kernels run at
-// the same time (PCIe is full duplex; copies and kernels use different
-// engines).  A submission to a busy slot first completes the product that
-// slot holds; the status of a completed product is kept until its ticket is
-// waited for (once).
+// each with its own scratch and kernel stream, takes products in turn, so
+// that one product's download, the next one's upload and a third one's
+// kernels run at the same time (PCIe is full duplex; copies and kernels use
+// different engines).  All uploads go through one stream and all downloads
+// through another (HostLinks): each direction carries one product at a
+// time, in submission order, at the full rate of the link, instead of
+// several products' copies sharing it and all finishing late.  A submission
+// to a busy slot first completes the product that slot holds (so its device
+// buffers are free before the next upload into them is queued); the status
+// of a completed product is kept until its ticket is waited for (once).
 struct Pipe {
     std::vector<Ctx *> slot;
+    cudaStream_t up = nullptr, down = nullptr;
+    std::vector<HostLinks> links;         // per slot: the shared streams and its events
     std::vector<long long> cur;           // ticket in flight on the slot (-1: none)
     std::unordered_map<long long, int> finished;   // completed, not yet waited: status
     struct Pending { gpu_ulong *z; gpu_ulong an, bn; };
@@ -1004,10 +1056,21 @@ static int pipe_complete(Pipe *P, int s)
     Ctx *X = P->slot[s];
     const Pipe::Pending &q = P->pend[s];
     int rc = bind_device(X);
-    if (!rc) rc = mpn_mul_host_finish(X, q.z, q.an, q.bn, 0, q.an + q.bn);
+    if (!rc) rc = mpn_mul_host_finish(X, q.z, q.an, q.bn, 0, q.an + q.bn, &P->links[s]);
     P->finished[P->cur[s]] = rc;
     P->cur[s] = -1;
     return rc;
+}
+
+static void pipe_free(Pipe *P)
+{
+    for (Ctx *X : P->slot) ctx_destroy(X);
+    for (HostLinks &L : P->links)
+        for (cudaEvent_t e : {L.a_in, L.b_in, L.done})
+            if (e) cudaEventDestroy(e);
+    if (P->up) cudaStreamDestroy(P->up);
+    if (P->down) cudaStreamDestroy(P->down);
+    delete P;
 }
 
 // ---------------------------------------------------------------------------
@@ -1083,17 +1146,27 @@ int gpu_mpn_pipe_init(gpu_mpn_pipe_t R, int depth)
     if (depth < 1 || depth > GPU_MPN_PIPE_MAX_DEPTH)
         return set_error(GPU_FFT_SMALL_EINVAL, "pipeline depth %d outside 1..%d", depth, GPU_MPN_PIPE_MAX_DEPTH);
     Pipe *P = new Pipe;
-    for (int s = 0; s < depth; s++) {
+    int rc = 0;
+    for (int s = 0; s < depth && !rc; s++) {
         Ctx *X = nullptr;
-        int rc = ctx_create(&X, 0);
+        rc = ctx_create(&X, 0);
         if (!rc) rc = ensure_copy_stream(X);
-        if (rc) {
-            if (X) ctx_destroy(X);
-            for (Ctx *Y : P->slot) ctx_destroy(Y);
-            delete P;
-            return rc;
-        }
-        P->slot.push_back(X);
+        if (X) P->slot.push_back(X);
+    }
+    if (!rc && (cudaStreamCreateWithFlags(&P->up, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&P->down, cudaStreamNonBlocking) != cudaSuccess))
+        rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaStreamCreate failed");
+    for (int s = 0; s < depth && !rc; s++) {
+        HostLinks L{P->up, P->down, nullptr, nullptr, nullptr};
+        if (cudaEventCreateWithFlags(&L.a_in, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&L.b_in, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
+            rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate failed");
+        P->links.push_back(L);
+    }
+    if (rc) {
+        pipe_free(P);
+        return rc;
     }
     P->cur.assign(depth, -1);
     P->pend.assign(depth, Pipe::Pending{nullptr, 0, 0});
@@ -1109,7 +1182,7 @@ int gpu_mpn_pipe_submit(gpu_mpn_pipe_t R, gpu_ulong *z, const gpu_ulong *a, gpu_
     if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
     const int s = (int)(P->next % (long long)P->slot.size());
     pipe_complete(P, s);   // its status stays with its own ticket
-    int rc = mpn_mul_host_issue(P->slot[s], z, a, an, b, bn, 0, an + bn);
+    int rc = mpn_mul_host_issue(P->slot[s], z, a, an, b, bn, 0, an + bn, &P->links[s]);
     if (rc) return rc;
     P->cur[s] = P->next;
     P->pend[s] = Pipe::Pending{z, an, bn};
@@ -1135,11 +1208,8 @@ void gpu_mpn_pipe_clear(gpu_mpn_pipe_t R)
 {
     Pipe *P = (Pipe *)R->impl;
     if (!P) return;
-    for (size_t s = 0; s < P->slot.size(); s++) {
-        pipe_complete(P, (int)s);
-        ctx_destroy(P->slot[s]);
-    }
-    delete P;
+    for (size_t s = 0; s < P->slot.size(); s++) pipe_complete(P, (int)s);
+    pipe_free(P);
     R->impl = nullptr;
 }
 
