@@ -94,6 +94,9 @@ SIGNATURES = {
     "gpu_mpn_pipe_submit": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, ctypes.POINTER(ctypes.c_longlong)]),
     "gpu_mpn_pipe_wait": (ctypes.c_int, [_CTX, ctypes.c_longlong]),
     "gpu_mpn_pipe_clear": (None, [_CTX]),
+    "gpu_test_crt_lookback_timeout": (ctypes.c_int, [_CTX]),
+    "gpu_test_set_device_error": (ctypes.c_int, [_CTX]),
+    "gpu_test_pipe_slot_ctx": (ctypes.c_void_p, [_CTX, ctypes.c_int]),
     "_gpu_mpn_ctx_mpn_mul_range": (None, [_CTX, _P, _U, _U, _P, _U, _P, _U]),
     "gpu_mpn_mul_device": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, _P]),
     "gpu_mpn_mul_device_noalloc": (ctypes.c_int, [_P, _P, _U, _P, _U, _P]),

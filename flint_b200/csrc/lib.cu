@@ -1407,6 +1407,56 @@ __global__ void k_fill_limbs(uint64_t *p, uint64_t n, uint64_t seed)
     }
 }
 
+int gpu_test_crt_lookback_timeout(gpu_mpn_ctx_t R)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    // one tile of a 1024-coefficient product whose ticket makes it tile 1:
+    // its look-back waits on tile 0's status word, which nothing publishes in
+    // this epoch, until the spin limit; every access stays inside the
+    // 5 x 1024 residues, the 1024-limb output and the two status words
+    constexpr int logM = 10;
+    const size_t M = (size_t)1 << logM;
+    rc = grow((void **)&X->d_res, &X->res_cap, 5 * M * sizeof(uint32_t));
+    if (!rc) rc = ensure_status(X, 2);
+    uint64_t *dz = nullptr;
+    if (!rc) rc = io_buffers(X, M, &dz);
+    if (rc) return rc;
+    cudaStream_t st = X->stream;
+    CU(cudaMemsetAsync(X->d_res, 0, 5 * M * sizeof(uint32_t), st));
+    X->epoch = (X->epoch + 1) & 0x0fffffffu;
+    if (X->epoch == 0) {
+        CU(cudaMemsetAsync(X->d_status, 0, X->status_cap * sizeof(uint32_t), st));
+        X->epoch = 1;
+    }
+    k_crt_carry<5, CRT_THREADS><<<1, CRT_THREADS, 0, st>>>(X->d_res, logM, M - 1, M, dz, X->crt[5], X->d_status,
+                                                          X->d_ticket, X->ticket_base - 1, X->epoch, X->d_err,
+                                                          nullptr, nullptr, 0ull);
+    CU(cudaGetLastError());
+    X->ticket_base += 1;
+    return check_device_error(X);
+}
+
+void *gpu_test_pipe_slot_ctx(gpu_mpn_pipe_t R, int slot)
+{
+    Pipe *P = (Pipe *)R->impl;
+    if (!P || slot < 0 || slot >= (int)P->slot.size()) return nullptr;
+    return P->slot[slot];
+}
+
+int gpu_test_set_device_error(gpu_mpn_ctx_t R)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    int rc = bind_device(X);
+    if (rc) return rc;
+    CU(cudaMemsetAsync(X->d_err, 1, sizeof(int), X->stream));
+    CU(cudaStreamSynchronize(X->stream));
+    return 0;
+}
+
 int gpu_butterfly_rate(gpu_mpn_ctx_t R, double *per_s)
 {
     Ctx *X = get_ctx(R);

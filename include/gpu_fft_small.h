@@ -396,6 +396,21 @@ GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device_config(gpu_mpn_ctx_t R, uint6
                                                           gpu_ulong bw, gpu_ulong bn,
                                                           const gpu_mul_config *cfg, void *stream);
 
+/* Test hooks for the failure paths of the bounded device waits, which valid
+   inputs do not reach (no counterpart in the reference).
+   gpu_test_crt_lookback_timeout runs one CRT/carry tile whose carry
+   look-back waits for a predecessor that never publishes its status, so the
+   wait runs out (a few seconds) and the kernel sets the context's error
+   flag and finishes; returns the status the host reads back
+   (GPU_FFT_SMALL_ETIMEOUT) and leaves the context usable.
+   gpu_test_set_device_error sets the error flag as such a kernel would: the
+   next host-pointer product on the context returns GPU_FFT_SMALL_ETIMEOUT
+   and clears it.  gpu_test_pipe_slot_ctx returns the context behind slot
+   `slot` of a pipeline (the impl of a gpu_mpn_ctx_t), or NULL. */
+GPU_FFT_SMALL_API int gpu_test_crt_lookback_timeout(gpu_mpn_ctx_t R);
+GPU_FFT_SMALL_API int gpu_test_set_device_error(gpu_mpn_ctx_t R);
+GPU_FFT_SMALL_API void *gpu_test_pipe_slot_ctx(gpu_mpn_pipe_t P, int slot);
+
 /* Integer-pipe calibration (no counterpart in the reference): the rate, in
    butterflies per second, of the transforms' 31-bit modular butterfly run
    from registers only on every SM (median of five timed launches of about a
