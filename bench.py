@@ -377,9 +377,51 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
         B.run(s)
         h_out.copy_(d_out, non_blocking=True)
 
-    ms_e2e = time_on_stream(torch, stream, e2e, max(3, steps // 2), 2)
+    ms_e2e_whole = time_on_stream(torch, stream, e2e, max(3, steps // 2), 2)
     B.check(s)
     e2e_ok = bool(np.array_equal(h_out.numpy().view(np.uint64), out))
+
+    # end to end, overlapped: the requests in E2E_CHUNKS runs of consecutive
+    # requests (contiguous operand and product ranges), one planned batch
+    # each; chunk c's upload, batch and download go on an upload, the compute
+    # and a download stream, so one chunk's download, the next one's batch and
+    # a later one's upload overlap.  A step starts after the previous one has
+    # finished (its first upload waits for the step's start on `stream`).
+    E2E_CHUNKS = 8
+    cuts = [len(reqs) * c // E2E_CHUNKS for c in range(E2E_CHUNKS + 1)]
+    parts = []
+    for c in range(E2E_CHUNKS):
+        r0, r1 = cuts[c], cuts[c + 1]
+        lo, hi = spans[r0][0], spans[r1 - 1][2] + spans[r1 - 1][3]   # operands and products share offsets
+        parts.append((lo, hi, FB.MpnBatch(ctx, reqs[r0:r1], configs=configs[r0:r1])))
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def e2e_overlapped():
+        start = torch.cuda.Event()
+        start.record(stream)
+        up.wait_event(start)
+        for lo, hi, Bc in parts:
+            with torch.cuda.stream(up):
+                d_in[lo:hi].copy_(h_in[lo:hi], non_blocking=True)
+            e_in = torch.cuda.Event()
+            e_in.record(up)
+            stream.wait_event(e_in)
+            Bc.run(s)
+            e_run = torch.cuda.Event()
+            e_run.record(stream)
+            down.wait_event(e_run)
+            with torch.cuda.stream(down):
+                h_out[lo:hi].copy_(d_out[lo:hi], non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(down)
+        stream.wait_event(done)
+
+    h_out.zero_()
+    ms_e2e = time_on_stream(torch, stream, e2e_overlapped, max(3, steps // 2), 2)
+    for _, _, Bc in parts:
+        Bc.check(s)
+        Bc.close()
+    e2e_ok = e2e_ok and bool(np.array_equal(h_out.numpy().view(np.uint64), out))
     res = {
         "workload": "%d uneven products, an = round(2^U), U~U[10,18], bn = max(1, round(an/2^V)), "
                     "V~U[0,4], seed %d" % (BATCH_N, BATCH_SEED),
@@ -397,7 +439,11 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
                                "basecase": sum(c.route == 1 for c in configs)},
                     "held_out_regret_vs_exhaustive": reg},
         "e2e": {"value": bits / ms_e2e / 1e6, "unit": "Gbit/s", "ms_per_step": ms_e2e,
-                "h2d_bytes_per_step": 8 * total, "d2h_bytes_per_step": 8 * total},
+                "h2d_bytes_per_step": 8 * total, "d2h_bytes_per_step": 8 * total,
+                "schedule": "%d chunks of consecutive requests, upload / batch / download overlapped "
+                            "on three streams" % E2E_CHUNKS},
+        "e2e_unchunked": {"value": bits / ms_e2e_whole / 1e6, "unit": "Gbit/s", "ms_per_step": ms_e2e_whole,
+                          "schedule": "whole batch: upload, batch, download in turn"},
         "exact_vs_per_instance": exact, "fingerprints_ok": bool(fp_ok), "e2e_matches": e2e_ok,
         "roofline": {"bound": "hbm", "alg_bytes": 208 * total,
                      "achieved": 208 * total / ms_batch / 1e6},
