@@ -840,6 +840,16 @@ def main():
     bfly = 3 * logM * (M // 2) * np_
     rate = ctx.butterfly_rate()
     t_bound = bfly / rate * 1e3
+    # the same per kernel: its share of the butterflies (forward columns: two
+    # operands x logR levels; rows: three transforms x logC levels; inverse
+    # columns: logR levels) at that rate, over its measured launch time
+    logC_ = FB.resolve_config(0, an, bn).logC
+    logR_ = logM - logC_
+    kb = {"k_fwd_cols": 2 * logR_, "k_rows": 3 * logC_, "k_inv_cols": logR_}
+    for name, v in kern.items():
+        if name in kb:
+            v["butterflies"] = kb[name] * (M // 2) * np_
+            v["int_pipe_frac"] = v["butterflies"] / rate * 1e3 / v["ms_per_launch"]
     int_pipe = {"butterflies": bfly, "rate_per_s": rate, "t_bound_ms": t_bound,
                 "frac": t_bound / ms_step,
                 "note": "31-bit modular butterfly from registers on every SM (gpu_butterfly_rate); "
