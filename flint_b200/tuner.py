@@ -15,7 +15,7 @@ Every valid configuration gives the same exact product; only time differs.
 * ``candidates`` enumerates the configurations of a request;
 * ``Autotuner`` measures them on the device (gpu_mul_time_config, CUDA
   events, median of a few runs) -- the exhaustive tuner, which is both the
-  fallback and the judge of the learned model;
+  fallback and the yardstick of the learned model (its regret);
 * ``CostModel`` is the learned part: an MLP (16 inputs -> 3 x 64 -> 1, fp32,
   the library's own CUDA training and inference kernels) that predicts the
   log device time of (request, configuration); ``choose`` takes the argmin
