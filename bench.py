@@ -474,6 +474,75 @@ def batch_cpu_baseline(sizes, host, spans, seconds):
             "sample": "first %d of the %d products, one mpn_ctx_mpn_mul each" % (k, len(spans))}
 
 
+def bench_configs(torch, FB, ctx, dev, stream, steps, cpu):
+    """The other measured configurations: 2^16 x 2^16 and 2^24 x 2^20 limbs
+    (mpn_mul), and the nmod window product (coefficients [2^19, 3 2^19) of
+    two 2^20-coefficient polynomials mod an odd n in [2^61, 2^62)), each
+    device-resident (CUDA events) against its algorithmic byte model, with
+    the compiled reference timed on the host and its output compared."""
+    import oracle
+    L = ref_library()[0] if cpu else None
+    peak = load_peaks()[0]
+    s = stream.cuda_stream
+    out = []
+
+    def ref_time(fn, reps):
+        fn()
+        ts = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            r = fn()
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts), r
+
+    for name, an, bn, seed in [("1: mpn_mul 2^16 x 2^16", 1 << 16, 1 << 16, 11),
+                               ("2b: mpn_mul 2^24 x 2^20", 1 << 24, 1 << 20, 12)]:
+        a, b = splitmix_limbs(seed, an), splitmix_limbs(seed + 1, bn)
+        da = torch.from_numpy(a.view(np.int64)).to(dev)
+        db = torch.from_numpy(b.view(np.int64)).to(dev)
+        dz = torch.empty(an + bn, dtype=torch.int64, device=dev)
+        k = max(steps, 50 if an < (1 << 20) else 10)
+        ms = time_on_stream(torch, stream, lambda: ctx.mpn_mul_device(dz.data_ptr(), da.data_ptr(), an,
+                                                                    db.data_ptr(), bn, s), k, 3)
+        z = dz.cpu().numpy().view(np.uint64)
+        alg = 208 * (an + bn)
+        r = {"workload": name, "ms": ms, "value": NS_LIMB_BITS * (an + bn) / ms / 1e6, "unit": "Gbit/s",
+             "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved": alg / ms / 1e6, "peak": peak,
+                          "frac": alg / ms / 1e6 / peak}}
+        if L is not None:
+            t, zr = ref_time(lambda: oracle.ref_mpn_mul(a, b), 5 if an < (1 << 20) else 2)
+            r.update(cpu_ms=t * 1e3, speedup_vs_cpu=t * 1e3 / ms, identical_to_reference=bool(np.array_equal(z, zr)))
+        out.append(r)
+    # nmod window product
+    n_ = (int(splitmix_limbs(21, 1)[0]) >> 2 | (1 << 61)) | 1
+    an = bn = 1 << 20
+    zl, zh = 1 << 19, 3 << 19
+    a = splitmix_limbs(22, an) % np.uint64(n_)     # inputs reduced mod n, as the call requires
+    b = splitmix_limbs(23, bn) % np.uint64(n_)
+    da = torch.from_numpy(a.view(np.int64)).to(dev)
+    db = torch.from_numpy(b.view(np.int64)).to(dev)
+    dz = torch.empty(zh - zl, dtype=torch.int64, device=dev)
+    ms = time_on_stream(torch, stream, lambda: ctx.nmod_poly_mul_mid_device(dz.data_ptr(), zl, zh, da.data_ptr(),
+                                                                          an, db.data_ptr(), bn, n_, s),
+                        max(steps, 50), 3)
+    z = dz.cpu().numpy().view(np.uint64)
+    alg = 200 * (an + bn) + 8 * (zh - zl)
+    r = {"workload": "3: nmod window product, coefficients [2^19, 3 2^19) of two 2^20-coefficient "
+                     "polynomials mod odd n in [2^61, 2^62)", "ms": ms,
+         "value": (zh - zl) / ms / 1e3, "unit": "M coefficients/s",
+         "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved": alg / ms / 1e6, "peak": peak,
+                      "frac": alg / ms / 1e6 / peak,
+                      "note": "the working set is largely L2-resident, so a fraction above 1 is possible"}}
+    if L is not None:
+        t, zr = ref_time(lambda: oracle.ref_nmod_mul_mid(zl, zh, a, b, n_), 3)
+        r.update(cpu_ms=t * 1e3, speedup_vs_cpu=t * 1e3 / ms, identical_to_reference=bool(np.array_equal(z, zr)))
+    out.append(r)
+    if L is not None:
+        for r in out:
+            r["cpu_note"] = "compiled reference on all host threads, median of a few calls"
+    return out
+
+
 def bench_precomp(torch, FB, ctx, dev, stream, steps):
     """Transformed-operand reuse (the reference's op API): b of 2^22 limbs
     transformed once, then for each a of 2^22 limbs: forward transform of a,
@@ -662,6 +731,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mpn24", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 2^16, 2^24 x 2^20 and nmod window measurements")
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the 4096-product uneven batch")
     ap.add_argument("--no-negacyclic", action="store_true",
@@ -795,11 +866,13 @@ def main():
     pipelined.update(value=world * gbits_step / pipe_s, ms_per_step=pipe_s * 1e3)
     # the batch, stream and transformed-operand legs are single-GPU
     # measurements: run at N = 1 only
-    batch = stream_res = precomp = negacyclic = None
+    batch = stream_res = precomp = negacyclic = other_configs = None
     single = world == 1
     cpu_s = 0.0 if (world > 1 or args.no_cpu_baseline) else 10.0
     if single:
         precomp = bench_precomp(torch, FB, ctx, dev, stream, max(3, args.steps // 2))
+        if not args.no_configs:
+            other_configs = bench_configs(torch, FB, ctx, dev, stream, args.steps, not args.no_cpu_baseline)
         if not args.no_negacyclic:
             negacyclic = bench_negacyclic(torch, FB, ctx, dev, stream, max(3, args.steps // 2),
                                           min(cpu_s, 5.0))
@@ -892,6 +965,7 @@ def main():
         "batch": batch,
         "stream": stream_res,
         "transformed_operand": precomp,
+        "other_configs": other_configs,
         "negacyclic": negacyclic,
     }
     print(json.dumps(line), flush=True)

@@ -104,6 +104,7 @@ SIGNATURES = {
     "gpu_mpn_mulmid_default_mpn_ctx": (None, [_P, _P, _S, _P, _S, _S, _S]),
     "_gpu_nmod_poly_mul_mid_mpn_ctx": (None, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_mul_mid_status": (ctypes.c_int, [_P, _U, _U, _P, _U, _P, _U, _Nmod, _CTX]),
+    "gpu_nmod_poly_mul_mid_device": (ctypes.c_int, [_CTX, _P, _U, _U, _P, _U, _P, _U, _Nmod, _P]),
     "_gpu_nmod_poly_divrem_mpn_ctx": (None, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "_gpu_nmod_poly_divrem_status": (ctypes.c_int, [_P, _P, _P, _U, _P, _U, _Nmod, _CTX]),
     "gpu_get_default_mpn_ctx": (_CTX, []),
@@ -415,6 +416,11 @@ class MpnCtx:
         """Queue the raw-form window product on device pointers."""
         _check(lib().gpu_fmpz_poly_mul_mid_device(self.ptr, z_ptr, zw, zl, zh, a_ptr, aw, an,
                                                   b_ptr, bw, bn, stream))
+
+    def nmod_poly_mul_mid_device(self, z_ptr, zl, zh, a_ptr, an, b_ptr, bn, n, stream=None):
+        """Queue coefficients [zl, zh) of a * b mod n on device pointers (ints)."""
+        _check(lib().gpu_nmod_poly_mul_mid_device(self.ptr, z_ptr, zl, zh, a_ptr, an, b_ptr, bn,
+                                                  _Nmod(n, 0, 0), stream))
 
     def mpn_mul_device_config(self, z_ptr, a_ptr, an, b_ptr, bn, cfg, stream=None):
         """mpn_mul_device under an explicit MulConfig."""

@@ -1283,6 +1283,27 @@ int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, gpu_ulong zh,
     return nmod_mul_mid_host(get_ctx(R), z, zl, zh, a, an, b, bn, mod.n);
 }
 
+int gpu_nmod_poly_mul_mid_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zl, gpu_ulong zh,
+                                 const uint64_t *a_dev, gpu_ulong an, const uint64_t *b_dev, gpu_ulong bn,
+                                 gpu_nmod_t mod, void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (an == 0 || bn == 0) return set_error(GPU_FFT_SMALL_EINVAL, "empty operand");
+    if (mod.n == 0) return set_error(GPU_FFT_SMALL_EINVAL, "modulus must be nonzero");
+    if (zl >= zh) return 0;
+    int rc = bind_device(X);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const gpu_ulong zn = an + bn - 1;
+    // coefficients at or beyond the product's length are zero, as is
+    // everything mod 1
+    const gpu_ulong top = mod.n == 1 ? zl : std::min<gpu_ulong>(zh, std::max<gpu_ulong>(zn, zl));
+    if (zh > top) CU(cudaMemsetAsync(z_dev + (top - zl), 0, (zh - top) * 8, st));
+    if (top > zl) rc = nmod_mul_mid_enqueue(X, z_dev, zl, top, a_dev, an, b_dev, bn, mod.n, st);
+    return rc;
+}
+
 int _gpu_nmod_poly_divrem_status(gpu_ulong *q, gpu_ulong *r, const gpu_ulong *a, gpu_ulong an,
                                  const gpu_ulong *b, gpu_ulong bn, gpu_nmod_t mod, gpu_mpn_ctx_t R)
 {

@@ -181,6 +181,15 @@ GPU_FFT_SMALL_API int _gpu_nmod_poly_mul_mid_status(gpu_ulong *z, gpu_ulong zl, 
                                   const gpu_ulong *b, gpu_ulong bn,
                                   gpu_nmod_t mod, gpu_mpn_ctx_t R);
 
+/* Device-pointer twin of _gpu_nmod_poly_mul_mid_mpn_ctx: coefficients
+   [zl, zh) of a * b mod n into z_dev[0, zh - zl) (zero where the product has
+   no coefficient), a and b reduced mod n, all device addresses; queued on
+   `stream` (a cudaStream_t), returns without synchronising. */
+GPU_FFT_SMALL_API int gpu_nmod_poly_mul_mid_device(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zl, gpu_ulong zh,
+                                                   const uint64_t *a_dev, gpu_ulong an,
+                                                   const uint64_t *b_dev, gpu_ulong bn,
+                                                   gpu_nmod_t mod, void *stream);
+
 /* q[0, an-bn+1) and r[0, bn-1): quotient and remainder of a by b mod n
    (an >= bn > 1, b's leading coefficient a unit mod n, inputs reduced mod n).
    Replaces _nmod_poly_divrem_mpn_ctx (src/fft_small.h:776-782,

@@ -74,3 +74,43 @@ def test_wraparound_window(ctx):
     a, b = O.rand_below(10, 6000, n), O.rand_below(11, 2000, n)
     got = ctx.nmod_poly_mul_mid(3905, 4096, a, b, n)
     assert (got == O.port_nmod_mul_mid(3905, 4096, a, b, n)).all()
+
+
+def _device_mul_mid(ctx, zl, zh, a, b, n, fill=0x5A5A5A5A5A5A5A5A):
+    torch = pytest.importorskip("torch")
+    da = torch.from_numpy(np.ascontiguousarray(a, np.uint64).view(np.int64)).cuda()
+    db = da if b is a else torch.from_numpy(np.ascontiguousarray(b, np.uint64).view(np.int64)).cuda()
+    dz = torch.full((max(zh - zl, 1),), fill - (1 << 64) if fill >= 1 << 63 else fill,
+                    dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream()
+    ctx.nmod_poly_mul_mid_device(dz.data_ptr(), zl, zh, da.data_ptr(), len(a), db.data_ptr(), len(b), n,
+                                 s.cuda_stream)
+    s.synchronize()
+    return dz.cpu().numpy().view(np.uint64)[:zh - zl]
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_device_twin_matches_host_call(ctx, seed):
+    """gpu_nmod_poly_mul_mid_device gives the host call's coefficients,
+    windows beyond the product zero-filled (the output starts as garbage)."""
+    rng = np.random.default_rng(100 + seed)
+    an, bn = int(rng.integers(1, 5000)), int(rng.integers(1, 5000))
+    bits = int(rng.integers(2, 65))
+    n = (int(O.rand_limbs(seed + 50, 1, False)[0]) >> (64 - bits)) | (1 << (bits - 1)) | 1
+    a, b = O.rand_below(seed + 1, an, n), O.rand_below(seed + 2, bn, n)
+    zl = int(rng.integers(0, an + bn))
+    zh = zl + int(rng.integers(1, an + bn + 20))
+    assert (_device_mul_mid(ctx, zl, zh, a, b, n) == ctx.nmod_poly_mul_mid(zl, zh, a, b, n)).all()
+
+
+def test_device_twin_edges(ctx, golden):
+    # the 2^20 window product of the golden fixtures, squaring, modulus 1,
+    # a window entirely beyond the product, and an empty window
+    case = next(c for c in golden["nmod"] if c["name"] == "config3_2^20_mulmid")
+    n, a, b = nmod_inputs(case)
+    _check_record(case, _device_mul_mid(ctx, case["zl"], case["zh"], a, b, n))
+    a2 = O.rand_below(3, 3000, n)
+    assert (_device_mul_mid(ctx, 100, 6100, a2, a2, n) == ctx.nmod_poly_mul_mid(100, 6100, a2, a2, n)).all()
+    assert (_device_mul_mid(ctx, 0, 500, a2, a2, 1) == 0).all()
+    assert (_device_mul_mid(ctx, 7000, 7010, a2, a2, n) == 0).all()
+    assert len(_device_mul_mid(ctx, 5, 5, a2, a2, n)) == 0
