@@ -319,7 +319,7 @@ static int ctx_build_tables(Ctx *X)
 // kernel dispatch by transform shape (column length 2^logR, row length 2^logC)
 typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t,
                             uint32_t *, uint32_t *, int, int, const InstDesc *, int, FzShape);
-typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int, const InstDesc *);
+typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int, const InstDesc *, ChunkOut);
 typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, const uint32_t *,
                         int, const InstDesc *, int, int);
 
@@ -421,12 +421,14 @@ static LaunchShape make_shape(int logM, int logC = -1)
 
 // the three transform launches shared by every product type; with a batch
 // descriptor array (ninst products of this shape) a, b, ra, rb are ignored;
-// with fz the operands are integer polynomials (an, bn coefficients)
+// with fz the operands are integer polynomials (an, bn coefficients); with co
+// the inverse column pass writes a split product's chunk (ChunkOut)
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
                               TimingRecord *tr, const InstDesc *desc = nullptr, int ninst = 1,
-                              const FzShape *fz = nullptr, cudaEvent_t b_ready = nullptr);
+                              const FzShape *fz = nullptr, cudaEvent_t b_ready = nullptr,
+                              const ChunkOut *co = nullptr);
 
 static int upload_scales(Ctx *X);
 
@@ -692,7 +694,7 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
                               TimingRecord *tr, const InstDesc *desc, int ninst, const FzShape *fz,
-                              cudaEvent_t b_ready)
+                              cudaEvent_t b_ready, const ChunkOut *co)
 {
     const MulShape &S = L.S;
     const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
@@ -718,7 +720,7 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     timing_mark(tr, 2, st);
     if (S.logR > 0)
         INV_COLS[S.logR]<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
-            X->T, ra, S.logC, S.G, desc);
+            X->T, ra, S.logC, S.G, desc, co ? *co : ChunkOut{nullptr, 0, 0, 0, 0});
     timing_mark(tr, 3, st);
 }
 
@@ -788,6 +790,32 @@ struct CrtChunks {
     void *arg = nullptr;
 };
 
+// Chunk transform length for an unbalanced whole product (0: one transform).
+// Chunks of the long operand of c = 2^Lc - yn + 1 limbs each multiply the
+// short operand in a 2^Lc-point transform; with k chunks the butterfly work
+// is k 3 Lc 2^(Lc-1) against 3 logM 2^(logM-1) for the single transform.
+// Splitting is taken when it saves at least 15% of that work, for products
+// of 2^20 points or more (smaller ones are launch-bound) and chunks of at
+// least 2^20 points.  (The reference truncates its transforms instead,
+// src/fft_small/sd_fft.c:1230-1274.)
+static int split_plan(uint64_t an, uint64_t bn, int logM)
+{
+    const uint64_t xn = std::max(an, bn), yn = std::min(an, bn);
+    if (logM < 20) return 0;
+    const double full = 3.0 * logM * (double)((uint64_t)1 << logM);
+    int best = 0;
+    double best_cost = 0.85 * full;
+    for (int Lc = 20; Lc < logM; Lc++) {
+        const uint64_t Mc = (uint64_t)1 << Lc;
+        if (Mc < 2 * yn) continue;
+        const uint64_t c = Mc - yn + 1;
+        const uint64_t k = (xn + c - 1) / c;
+        const double cost = (double)k * 3.0 * Lc * (double)Mc;
+        if (cost < best_cost) { best_cost = cost; best = Lc; }
+    }
+    return best;
+}
+
 static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
                            const uint64_t *b, uint64_t bn, cudaStream_t st,
                            const gpu_mul_config *cfg = nullptr, uint64_t lo = 0, uint64_t hi = ~0ull,
@@ -820,7 +848,13 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     const bool sq = (a == b) && (an == bn);
     const int np = P.np, logM = P.logM;
     const size_t M = (size_t)1 << logM;
-    const size_t res_bytes = (sq ? 1 : 2) * (size_t)np * M * sizeof(uint32_t);
+    // an unbalanced whole product may run as chunks of the long operand
+    // against the short one (split_plan): their residues are summed into
+    // one array of the full length, then a single CRT/carry pass follows
+    const int Lc = (!cfg && !window && !sq) ? split_plan(an, bn, logM) : 0;
+    const size_t Mc = Lc ? (size_t)1 << Lc : 0;
+    const size_t res_bytes = Lc ? (size_t)np * (M + 2 * Mc) * sizeof(uint32_t)
+                                : (sq ? 1 : 2) * (size_t)np * M * sizeof(uint32_t);
     rc = grow((void **)&X->d_res, &X->res_cap, res_bytes);
     if (rc) return rc;
     uint32_t *ra = X->d_res, *rb = X->d_res + (size_t)np * M;
@@ -838,8 +872,32 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
 
     int launches = 3;
     TimingRecord *tr = timing_begin(X, st);
-    launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr, nullptr, 1,
-                      nullptr, b_ready);
+    if (Lc) {
+        // chunk i: x[i c, i c + c) times y, c = 2^Lc - yn + 1 (the chunk's
+        // product fills the 2^Lc-point transform without wrapping); its
+        // residues land at i c in ra, added where chunk i - 1's end
+        const uint64_t *x = a, *y = b;
+        uint64_t xn = an, yn = bn;
+        if (yn > xn) { std::swap(x, y); std::swap(xn, yn); }
+        const uint64_t c = Mc - yn + 1;
+        uint32_t *ca = ra + (size_t)np * M, *cb = ca + (size_t)np * Mc;
+        const LaunchShape Ls = make_shape(Lc);
+        if (b_ready) CU(cudaStreamWaitEvent(st, b_ready, 0));
+        launches = 0;
+        for (uint64_t i = 0; i * c < xn; i++) {
+            const uint64_t xi = std::min(c, xn - i * c);
+            const ChunkOut co{ra, logM, i * c, i ? yn - 1 : 0, xi + yn - 1};
+            launch_transforms(X, Ls, np, x + i * c, xi, y, yn, ca, cb, false, scale_ptr(X, np, Lc), st, nullptr,
+                              nullptr, 1, nullptr, nullptr, &co);
+            launches += 3;
+        }
+        timing_mark(tr, 1, st);
+        timing_mark(tr, 2, st);
+        timing_mark(tr, 3, st);
+    } else {
+        launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr, nullptr, 1,
+                          nullptr, b_ready);
+    }
     // tiles take their index from the ticket counter, so consecutive launches
     // with the same ticket base continue one carry chain: tile k's look-back
     // finds tile k - 1 finished by an earlier launch

@@ -489,13 +489,25 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
     cp_async_wait<0>();
 }
 
+// Destination of one chunk of a split product (a long operand cut into
+// chunks, each multiplied by the short one): the inverse column pass writes
+// the chunk's residues into acc (prime stride 2^logMf) at offset shift
+// instead of back in place, adds them mod p below `overlap` (where the
+// previous chunk's product ends), and skips positions at or beyond nvalid
+// (past the chunk's product).  acc == nullptr: in place.
+struct ChunkOut {
+    uint32_t* acc;
+    int logMf;
+    uint64_t shift, overlap, nvalid;
+};
+
 // ---------------------------------------------------------------------------
 // Column pass, inverse: untwist in registers + length-R inverse transforms,
-// in place.  grid = (C / G, np, instances); smem = padw(R * G) words.
+// in place (or into a split product's residues, ChunkOut).  grid = (C / G, np, instances); smem = padw(R * G) words.
 template <int LOGR, int G>
 __global__ void __launch_bounds__(512)
 k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
-           const InstDesc* __restrict__ desc)
+           const InstDesc* __restrict__ desc, ChunkOut co)
 {
     extern __shared__ uint32_t sm[];
     constexpr int R = 1 << LOGR;
@@ -534,10 +546,23 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
         const int t = threadIdx.x;
         const int u_t = t / G, c = t & (G - 1);
         const size_t step = (size_t)(512 / G) * C;
-        uint32_t* dst = buf + (size_t)u_t * C + i0 + c;
         const uint32_t* s_ = sm + padw(u_t * G) + c;
+        if (!co.acc) {
+            uint32_t* dst = buf + (size_t)u_t * C + i0 + c;
 #pragma unroll 8
-        for (int k = 0; k < R * G / 512; k++) dst[k * step] = s_[k * 528];
+            for (int k = 0; k < R * G / 512; k++) dst[k * step] = s_[k * 528];
+        } else {
+            uint32_t* __restrict__ out = co.acc + ((size_t)j << co.logMf) + co.shift;
+            const uint64_t n0 = (uint64_t)u_t * C + i0 + c;
+#pragma unroll 8
+            for (int k = 0; k < R * G / 512; k++) {
+                const uint64_t n = n0 + (uint64_t)k * step;
+                if (n < co.nvalid) {
+                    const uint32_t v = s_[k * 528];
+                    out[n] = n < co.overlap ? add_mod(out[n], v, p) : v;
+                }
+            }
+        }
     } else if constexpr (LOGR > 0) {
         for (int v = threadIdx.x; v < GR; v += blockDim.x) {
             const uint32_t col = (uint32_t)(i0 + v);
