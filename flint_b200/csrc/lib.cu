@@ -792,25 +792,32 @@ struct CrtChunks {
 
 // Chunk transform length for an unbalanced whole product (0: one transform).
 // Chunks of the long operand of c = 2^Lc - yn + 1 limbs each multiply the
-// short operand in a 2^Lc-point transform; with k chunks the butterfly work
-// is k 3 Lc 2^(Lc-1) against 3 logM 2^(logM-1) for the single transform.
-// Splitting is taken when it saves at least 15% of that work, for products
-// of 2^20 points or more (smaller ones are launch-bound) and chunks of at
-// least 2^20 points.  (The reference truncates its transforms instead,
-// src/fft_small/sd_fft.c:1230-1274.)
+// short operand in a 2^Lc-point transform; the short operand is transformed
+// once, so k chunks cost 2k + 1 transforms of Lc levels on 2^Lc points
+// against 3 of logM levels on 2^logM, plus a fixed cost per chunk (its
+// three launches and their tails: about 24 2^20 level-points, measured as
+// ~0.04 ms per 2^20-point chunk on the B200).  Splitting is taken when that
+// is at most 75% of the single transform's work (the margin covers the
+// separate spectrum pass and the CRT, which costs the same either way), for
+// products of 2^20 points or more and chunks of at least 2^20 points.
+// Measured (split / single transform): 2^24 x 2^20 0.66, 2^22 x 3000 0.71,
+// 2^23 x 7 10^5 0.70, 5 10^6 x 3 10^5 0.77, 2^24 x 2^22 0.90; without the
+// chunk cost term 2^23 x 1 (8 chunks) 1.06 and 3 2^20 x 2^16 1.10, which
+// now take the single transform.  (The reference truncates its transforms
+// instead, src/fft_small/sd_fft.c:1230-1274.)
 static int split_plan(uint64_t an, uint64_t bn, int logM)
 {
     const uint64_t xn = std::max(an, bn), yn = std::min(an, bn);
     if (logM < 20) return 0;
     const double full = 3.0 * logM * (double)((uint64_t)1 << logM);
     int best = 0;
-    double best_cost = 0.85 * full;
+    double best_cost = 0.75 * full;
     for (int Lc = 20; Lc < logM; Lc++) {
         const uint64_t Mc = (uint64_t)1 << Lc;
         if (Mc < 2 * yn) continue;
         const uint64_t c = Mc - yn + 1;
         const uint64_t k = (xn + c - 1) / c;
-        const double cost = (double)k * 3.0 * Lc * (double)Mc;
+        const double cost = (double)(2 * k + 1) * Lc * (double)Mc + (double)k * (24u << 20);
         if (cost < best_cost) { best_cost = cost; best = Lc; }
     }
     return best;
@@ -874,21 +881,35 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     TimingRecord *tr = timing_begin(X, st);
     if (Lc) {
         // chunk i: x[i c, i c + c) times y, c = 2^Lc - yn + 1 (the chunk's
-        // product fills the 2^Lc-point transform without wrapping); its
-        // residues land at i c in ra, added where chunk i - 1's end
+        // product fills the 2^Lc-point transform without wrapping); y's
+        // spectrum is computed once (column pass, k_rows_fwd) and every
+        // chunk's row pass transforms only its x part (squaring mode 2); the
+        // chunk's residues land at i c in ra, added where chunk i - 1's end
         const uint64_t *x = a, *y = b;
         uint64_t xn = an, yn = bn;
         if (yn > xn) { std::swap(x, y); std::swap(xn, yn); }
         const uint64_t c = Mc - yn + 1;
         uint32_t *ca = ra + (size_t)np * M, *cb = ca + (size_t)np * Mc;
         const LaunchShape Ls = make_shape(Lc);
+        const MulShape &S = Ls.S;
+        const FzShape one{1, 1, 1};
         if (b_ready) CU(cudaStreamWaitEvent(st, b_ready, 0));
-        launches = 0;
+        FWD_COLS[S.logR]<<<dim3(np, Ls.col_grid, 1), Ls.col_threads, Ls.col_smem, st>>>(
+            X->T, y, yn, y, yn, cb, cb, S.logC, S.G, nullptr, np, one);
+        ROWS_FWD[S.logC]<<<((1 << S.logR) / Ls.nv) * np, Ls.nv * (1 << S.logC) / 32,
+                           Ls.nv * padw(1 << S.logC) * sizeof(uint32_t), st>>>(X->T, cb, S.logR, Ls.nv, np,
+                                                                              1 << S.logR);
+        launches = 2;
+        const int items = Ls.row_grid * np;
         for (uint64_t i = 0; i * c < xn; i++) {
             const uint64_t xi = std::min(c, xn - i * c);
             const ChunkOut co{ra, logM, i * c, i ? yn - 1 : 0, xi + yn - 1};
-            launch_transforms(X, Ls, np, x + i * c, xi, y, yn, ca, cb, false, scale_ptr(X, np, Lc), st, nullptr,
-                              nullptr, 1, nullptr, nullptr, &co);
+            FWD_COLS[S.logR]<<<dim3(np, Ls.col_grid, 1), Ls.col_threads, Ls.col_smem, st>>>(
+                X->T, x + i * c, xi, x + i * c, xi, ca, ca, S.logC, S.G, nullptr, np, one);
+            ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(Ls)), Ls.row_threads, Ls.row_smem, st>>>(
+                X->T, ca, cb, S.logR, Ls.nv, np, scale_ptr(X, np, Lc), 2, nullptr, 1, 1 << S.logR);
+            INV_COLS[S.logR]<<<dim3(Ls.col_grid, np, 1), Ls.col_threads, Ls.col_smem, st>>>(X->T, ca, S.logC, S.G,
+                                                                                          nullptr, co);
             launches += 3;
         }
         timing_mark(tr, 1, st);

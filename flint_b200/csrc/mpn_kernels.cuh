@@ -406,7 +406,8 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         const uint32_t* B;
         decode(g, j, u0, A, B);
         rows_prefetch<LOGC, LOGE, true>(sa_buf(0), A + ((size_t)j << logM), u0, nv, R);
-        if (!squaring) rows_prefetch<LOGC, LOGE, true>(sb, B + ((size_t)j << logM), u0, nv, R);
+        if (squaring == 0) rows_prefetch<LOGC, LOGE, true>(sb, B + ((size_t)j << logM), u0, nv, R);
+        else if (squaring == 2) rows_prefetch<LOGC, LOGE, false>(sb, B + ((size_t)j << logM), u0, nv, R);
         else cp_async_commit();
     }
     int cur = 0;
@@ -432,7 +433,7 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
 
         uint32_t xr[E];
         uint32_t breg[E];
-        if (!squaring) {
+        if (squaring == 0) {
             if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all2<LOGC, QMAX, LOGE, true>(sa, sb, nv, twf, p);
             else gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
 #pragma unroll
@@ -445,17 +446,27 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
             if (g2 < total) rows_prefetch<LOGC, LOGE, true>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
             else cp_async_commit();
         } else {
+            // a squaring, or b's rows already hold its spectrum in this
+            // kernel's order (squaring == 2: k_rows_fwd output, landed padded)
             if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all<LOGC, 0, QMAX, LOGE, true>(sa, nv, twf, p);
             else gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
 #pragma unroll
             for (int m = 0; m < E; m++) xr[m] = sa[pb + m];
             gs_contig<LOGE, ROW_GS_FMA_ADDS>(xr, c_w32[j], p);
-            cp_async_commit();
+            if (squaring == 2) {
+#pragma unroll
+                for (int m = 0; m < E; m++) breg[m] = sb[pb + m];
+                __syncthreads();   // b fully read: refill it for the next item
+                if (g2 < total) rows_prefetch<LOGC, LOGE, false>(sb, B2 + ((size_t)j2 << logM), u2, nv, R);
+                else cp_async_commit();
+            } else {
+                cp_async_commit();
+            }
         }
         const uint32_t sc = scale[j];
 #pragma unroll
         for (int m = 0; m < E; m++) {
-            const uint32_t y = squaring ? xr[m] : breg[m];
+            const uint32_t y = squaring == 1 ? xr[m] : breg[m];
             xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
         }
         ct_contig<LOGE, ROW_CT_FMA_ADDS>(xr, c_w32[j], p);

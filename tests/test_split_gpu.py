@@ -2,10 +2,10 @@
 operand is cut into chunks, each multiplied by the short one in a shorter
 transform, the chunks' residues summed into one array of the full length and
 recombined by a single CRT/carry pass.  Every case is compared limb for limb
-with GMP's mpn_mul; the sizes cover several chunk lengths (2^20 to 2^22
-points), a last chunk of one limb, a one-limb short operand (no overlap
-between chunks), the operands in either order, and products near the size at
-which splitting stops paying (which take the single transform).
+with GMP's mpn_mul; the sizes cover several chunk lengths (2^20 to 2^23
+points), short last chunks, a one-limb short operand (no overlap between
+chunks), the operands in either order, and products for which splitting
+does not pay (they take the single transform).
 """
 import numpy as np
 import pytest
@@ -21,13 +21,15 @@ SIZES = [
     (1 << 24, 1 << 20),            # 6 chunks of 2^22 points
     (1 << 22, 3000),               # 5 chunks of 2^20 points
     (3000, 1 << 22),               # the same with the operands swapped
-    (5 * C20 + 1, 3000),           # last chunk of one limb
-    ((1 << 23) + (1 << 20), 1),    # one-limb short operand: chunks do not overlap
+    (5 * C20 + 1, 3000),           # 3 chunks of 2^21 points
+    ((1 << 23) + (1 << 20), 1),    # one-limb short operand: 5 chunks that do not overlap
     (5_000_000, 300_000),          # 3 chunks of 2^21 points
     (1 << 23, 700_000),            # 3 chunks of 2^22 points
-    (1 << 21, 1 << 17),            # 3 chunks of 2^20 points
-    ((1 << 23), 1),                # not split (a single transform is cheaper)
+    (1 << 21, 1 << 17),            # not split
+    (1 << 24, 1 << 22),            # 4 chunks of 2^23 points
+    ((1 << 23), 1),                # not split: eight 2^20-point chunks cost more
     (3 << 20, 1 << 16),            # not split
+    ((1 << 22) - (1 << 20), 1 << 20),  # not split
 ]
 
 
@@ -42,7 +44,7 @@ def test_split_product_all_ones_and_device_entry(ctx):
     """Longest carry chains across chunk boundaries, through the
     device-pointer entry point."""
     torch = pytest.importorskip("torch")
-    an, bn = 5 * C20 + 17, 3000          # 6 chunks of 2^20 points
+    an, bn = 5 * C20 + 17, 3000          # 3 chunks of 2^21 points
     ones = np.full(an, (1 << 64) - 1, dtype=np.uint64)
     b = np.full(bn, (1 << 64) - 1, dtype=np.uint64)
     da = torch.from_numpy(ones.view(np.int64)).cuda()
