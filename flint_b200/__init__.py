@@ -195,6 +195,7 @@ SIGNATURES = {
     "gpu_fft_small_last_error": (ctypes.c_char_p, []),
     "gpu_mpn_mul_plan": (ctypes.c_int, [_U, _U, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]),
+    "gpu_mpn_mul_split_plan": (ctypes.c_int, [_U, _U, ctypes.POINTER(ctypes.c_int)]),
     "gpu_fft_small_prime": (_U, [ctypes.c_int]),
     "gpu_mpn_ctx_last_launches": (ctypes.c_int, [_CTX]),
     "gpu_mpn_ctx_set_timing": (ctypes.c_int, [_CTX, ctypes.c_int]),
@@ -238,6 +239,13 @@ def mpn_mul_plan(an, bn):
     np_, lm = ctypes.c_int(), ctypes.c_int()
     _check(lib().gpu_mpn_mul_plan(an, bn, ctypes.byref(np_), ctypes.byref(lm)))
     return np_.value, lm.value
+
+
+def mpn_mul_split_plan(an, bn):
+    """log2 chunk transform length of a split an x bn product, 0 if not split."""
+    lc = ctypes.c_int()
+    _check(lib().gpu_mpn_mul_split_plan(an, bn, ctypes.byref(lc)))
+    return lc.value
 
 
 def prime(i):

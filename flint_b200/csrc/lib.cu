@@ -1796,6 +1796,15 @@ int gpu_mpn_mul_plan(gpu_ulong an, gpu_ulong bn, int *np, int *logM)
     return 0;
 }
 
+int gpu_mpn_mul_split_plan(gpu_ulong an, gpu_ulong bn, int *chunk_logM)
+{
+    MulPlan P;
+    int rc = plan_mpn(an, bn, &P);
+    if (rc) return rc;
+    *chunk_logM = P.route == GPU_MUL_ROUTE_NTT ? split_plan(an, bn, P.logM) : 0;
+    return 0;
+}
+
 gpu_ulong gpu_fft_small_prime(int i)
 {
     return (i >= 0 && i < MAX_NP) ? PRIMES[i] : 0;

@@ -695,6 +695,11 @@ GPU_FFT_SMALL_API const char *gpu_fft_small_last_error(void);
 /* Number of primes the GPU path would use and the transform length 2^logM
    for an an x bn product; returns 0 on success. */
 GPU_FFT_SMALL_API int gpu_mpn_mul_plan(gpu_ulong an, gpu_ulong bn, int *np, int *logM);
+/* For a whole non-squaring an x bn product under the default plan: the
+   log2 transform length of the chunks it is split into (chunks of the long
+   operand against one transform of the short one), or 0 when it runs as a
+   single transform; returns 0 on success. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_split_plan(gpu_ulong an, gpu_ulong bn, int *chunk_logM);
 /* The i-th prime of the GPU prime set (0 if out of range). */
 GPU_FFT_SMALL_API gpu_ulong gpu_fft_small_prime(int i);
 /* Kernel launches issued by the most recent call on this context. */

@@ -1,0 +1,52 @@
+"""Host logic of split products (no GPU): which unbalanced products the
+default plan cuts into chunks of the long operand, and with which chunk
+transform length (gpu_mpn_mul_split_plan).  The decisions on the shapes
+measured on the B200 are pinned; random shapes check the rule's invariants.
+"""
+import numpy as np
+import pytest
+
+import flint_b200 as FB
+
+
+@pytest.mark.parametrize("an,bn,want", [
+    (1 << 24, 1 << 20, 22),          # 0.66 of the single transform's time
+    (1 << 22, 3000, 20),             # 0.71
+    (3000, 1 << 22, 20),             # operand order does not matter
+    ((1 << 23) + (1 << 20), 1, 21),  # 0.60
+    (5_000_000, 300_000, 21),        # 0.77
+    (1 << 23, 700_000, 22),          # 0.70
+    (1 << 24, 1 << 22, 23),          # 0.90
+    (1 << 23, 1, 0),                 # eight 2^20-point chunks measured 1.06: single transform
+    (3 << 20, 1 << 16, 0),           # measured 1.10: single transform
+    (1 << 21, 1 << 17, 0),
+    (1 << 24, 1 << 24, 0),           # balanced
+    (1 << 24, 1 << 23, 0),
+    (1000, 3, 0),                    # small products are never split
+])
+def test_measured_shapes(an, bn, want):
+    assert FB.mpn_mul_split_plan(an, bn) == want
+
+
+def test_invariants_on_random_shapes():
+    rng = np.random.default_rng(7)
+    for _ in range(400):
+        an = int(2 ** rng.uniform(10, 25))
+        bn = int(2 ** rng.uniform(0, np.log2(an)))
+        if an + bn - 1 > 1 << 25:
+            continue
+        lc = FB.mpn_mul_split_plan(an, bn)
+        logM = FB.mpn_mul_plan(an, bn)[1]
+        if lc:
+            assert 20 <= lc < logM
+            assert (1 << lc) >= 2 * min(an, bn)          # chunks at least twice the short operand
+            assert max(an, bn) > 2 * min(an, bn)          # only unbalanced products
+        assert FB.mpn_mul_split_plan(bn, an) == lc
+
+
+def test_errors_match_the_plan():
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.mpn_mul_split_plan(0, 5)
+    with pytest.raises(FB.GpuFftSmallError) as e:
+        FB.mpn_mul_split_plan(1 << 25, (1 << 25) + 1)
+    assert e.value.code == FB.ETOOBIG
