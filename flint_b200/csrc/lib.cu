@@ -805,22 +805,55 @@ struct CrtChunks {
 // chunk cost term 2^23 x 1 (8 chunks) 1.06 and 3 2^20 x 2^16 1.10, which
 // now take the single transform.  (The reference truncates its transforms
 // instead, src/fft_small/sd_fft.c:1230-1274.)
-static int split_plan(uint64_t an, uint64_t bn, int logM)
+static int split_search(uint64_t xn, uint64_t yn, int Lmax, double *best_cost)
 {
-    const uint64_t xn = std::max(an, bn), yn = std::min(an, bn);
-    if (logM < 20) return 0;
-    const double full = 3.0 * logM * (double)((uint64_t)1 << logM);
     int best = 0;
-    double best_cost = 0.75 * full;
-    for (int Lc = 20; Lc < logM; Lc++) {
+    for (int Lc = 20; Lc <= Lmax; Lc++) {
         const uint64_t Mc = (uint64_t)1 << Lc;
         if (Mc < 2 * yn) continue;
         const uint64_t c = Mc - yn + 1;
         const uint64_t k = (xn + c - 1) / c;
         const double cost = (double)(2 * k + 1) * Lc * (double)Mc + (double)k * (24u << 20);
-        if (cost < best_cost) { best_cost = cost; best = Lc; }
+        if (cost < *best_cost) { *best_cost = cost; best = Lc; }
     }
     return best;
+}
+
+static int split_plan(uint64_t an, uint64_t bn, int logM)
+{
+    if (logM < 20) return 0;
+    double cost = 0.75 * 3.0 * logM * (double)((uint64_t)1 << logM);
+    return split_search(std::max(an, bn), std::min(an, bn), logM - 1, &cost);
+}
+
+// Whole products beyond the longest transform (an + bn - 1 > 2^25 limbs)
+// run split when the short operand leaves room for chunks of at most 2^25
+// points: the chunk length is the cheapest by the same count, the residues
+// of the whole product take 2^logM words per prime (logM <= LOG_MAX_SPLIT),
+// and the prime count is the one the coefficient bound of the short operand
+// asks for, as for any product.
+constexpr int LOG_MAX_SPLIT = 30;
+
+static int plan_mpn_oversize(uint64_t an, uint64_t bn, MulPlan *P, int *Lc)
+{
+    const uint64_t L = an + bn - 1, yn = std::min(an, bn);
+    const int logM = ceil_log2_u64(L);
+    if (logM > LOG_MAX_SPLIT)
+        return set_error(GPU_FFT_SMALL_ETOOBIG, "product of %llu coefficients exceeds 2^%d",
+                         (unsigned long long)L, LOG_MAX_SPLIT);
+    double cost = 1e300;
+    const int lc = split_search(std::max(an, bn), yn, LOG_MAXM, &cost);
+    if (!lc)
+        return set_error(GPU_FFT_SMALL_ETOOBIG, "product of %llu coefficients with a %llu-limb short operand "
+                         "exceeds a 2^%d transform", (unsigned long long)L, (unsigned long long)yn, LOG_MAXM);
+    MulPlan Q;
+    int rc = plan_mpn(yn, yn, &Q);   // the prime count for a short operand of yn limbs
+    if (rc) return rc;
+    P->np = Q.np;
+    P->logM = logM;
+    P->route = GPU_MUL_ROUTE_NTT;
+    *Lc = lc;
+    return 0;
 }
 
 static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
@@ -830,11 +863,15 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
 {
     MulPlan P;
     int rc = plan_mpn_cfg(an, bn, cfg, &P);
-    if (rc) return rc;
     const uint64_t zfull = an + bn;
     hi = std::min(hi, zfull);
-    if (lo >= hi) return 0;
     const bool window = lo > 0 || hi < zfull;
+    // beyond the longest transform: a whole unbalanced product may still run split
+    int Lover = 0;
+    if (rc == GPU_FFT_SMALL_ETOOBIG && !cfg && !window && !(a == b && an == bn))
+        rc = plan_mpn_oversize(an, bn, &P, &Lover);
+    if (rc) return rc;
+    if (lo >= hi) return 0;
     if (P.route == GPU_MUL_ROUTE_BASECASE) {
         if (window) return set_error(GPU_FFT_SMALL_EINVAL, "the basecase route computes whole products only");
         if (b_ready) CU(cudaStreamWaitEvent(st, b_ready, 0));
@@ -858,7 +895,7 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     // an unbalanced whole product may run as chunks of the long operand
     // against the short one (split_plan): their residues are summed into
     // one array of the full length, then a single CRT/carry pass follows
-    const int Lc = (!cfg && !window && !sq) ? split_plan(an, bn, logM) : 0;
+    const int Lc = Lover ? Lover : (!cfg && !window && !sq) ? split_plan(an, bn, logM) : 0;
     const size_t Mc = Lc ? (size_t)1 << Lc : 0;
     const size_t res_bytes = Lc ? (size_t)np * (M + 2 * Mc) * sizeof(uint32_t)
                                 : (sq ? 1 : 2) * (size_t)np * M * sizeof(uint32_t);
@@ -1800,6 +1837,7 @@ int gpu_mpn_mul_split_plan(gpu_ulong an, gpu_ulong bn, int *chunk_logM)
 {
     MulPlan P;
     int rc = plan_mpn(an, bn, &P);
+    if (rc == GPU_FFT_SMALL_ETOOBIG && an != bn) return plan_mpn_oversize(an, bn, &P, chunk_logM);
     if (rc) return rc;
     *chunk_logM = P.route == GPU_MUL_ROUTE_NTT ? split_plan(an, bn, P.logM) : 0;
     return 0;

@@ -77,7 +77,11 @@ GPU_FFT_SMALL_API void gpu_mpn_ctx_clear(gpu_mpn_ctx_t R);
 /* --- integer products ---------------------------------------------------- */
 
 /* z[0, an+bn) = a * b.  Replaces mpn_ctx_mpn_mul (src/fft_small.h:433,
-   src/fft_small/mpn_mul.c:1980-1983).  Requires an, bn >= 1. */
+   src/fft_small/mpn_mul.c:1980-1983).  Requires an, bn >= 1.  Products of
+   up to 2^25 + 1 limbs in all; beyond, an unbalanced product whose short
+   operand leaves room for chunks of at most 2^25 points runs split (up to
+   2^30 limbs), anything else is GPU_FFT_SMALL_ETOOBIG
+   (gpu_mpn_mul_split_plan tells which). */
 GPU_FFT_SMALL_API void gpu_mpn_ctx_mpn_mul(gpu_mpn_ctx_t R, gpu_ulong *z,
                          const gpu_ulong *a, gpu_ulong an,
                          const gpu_ulong *b, gpu_ulong bn);

@@ -56,6 +56,16 @@ def test_split_product_all_ones_and_device_entry(ctx):
     assert (dz.cpu().numpy().view(np.uint64) == O.gmp_mpn_mul(ones, b)).all()
 
 
+@pytest.mark.parametrize("an,bn", [((1 << 25) + (1 << 20), 1000), ((1 << 26) + 12345, 4096)])
+def test_products_beyond_the_longest_transform(ctx, an, bn):
+    """More than 2^25 + 1 limbs in all: no single transform holds the
+    product, chunks of the long operand do."""
+    a = O.rand_limbs(an % 1009 + 1, an)
+    b = O.rand_limbs(bn % 1013 + 3, bn)
+    assert FB.mpn_mul_split_plan(an, bn) > 0
+    assert (ctx.mpn_mul(a, b) == O.gmp_mpn_mul(a, b)).all()
+
+
 def test_split_product_through_the_pipeline():
     a, b = O.rand_limbs(5, 1 << 22), O.rand_limbs(6, 3000)
     with FB.MpnPipe(2) as P:

@@ -48,5 +48,21 @@ def test_errors_match_the_plan():
     with pytest.raises(FB.GpuFftSmallError):
         FB.mpn_mul_split_plan(0, 5)
     with pytest.raises(FB.GpuFftSmallError) as e:
-        FB.mpn_mul_split_plan(1 << 25, (1 << 25) + 1)
+        FB.mpn_mul_split_plan(1 << 25, (1 << 25) + 1)   # too balanced to split
     assert e.value.code == FB.ETOOBIG
+    with pytest.raises(FB.GpuFftSmallError) as e:
+        FB.mpn_mul_split_plan(1 << 30, 5)                # beyond 2^30 coefficients
+    assert e.value.code == FB.ETOOBIG
+
+
+@pytest.mark.parametrize("an,bn,want", [
+    ((1 << 25) + (1 << 20), 1000, 21),
+    ((1 << 26) + 12345, 4096, 22),
+    (1 << 26, 1 << 20, 23),
+    (1 << 28, 1 << 22, 25),
+    (1 << 26, 1 << 24, 25),           # short operand of 2^24 limbs: chunks of 2^25 points
+])
+def test_products_beyond_the_longest_transform_split(an, bn, want):
+    with pytest.raises(FB.GpuFftSmallError):
+        FB.mpn_mul_plan(an, bn)                          # no single transform holds them
+    assert FB.mpn_mul_split_plan(an, bn) == want
