@@ -296,7 +296,9 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
 // a ping-pong pair for a, so the next item's a rows stream in (cp.async)
 // during the whole current item and its b rows as soon as b's spectrum is in
 // registers.  grid = min(items, resident CTAs); block = nv * C / 32;
-// smem = 3 * nv * padw(C) words.
+// smem = 3 * nv * padw(C) words.  `squaring`: 0 a b, 1 a a (b unused), 2 a
+// times a b whose rows already hold its spectrum in this kernel's order
+// (k_rows_fwd output; the chunks of a split product share one).
 __device__ __forceinline__ void cp_async4(uint32_t* dst, const uint32_t* src, bool valid)
 {
     const unsigned s = (unsigned)__cvta_generic_to_shared(dst);
