@@ -10,7 +10,9 @@ functions (src/fft_small.h):
     MpnCtx.nmod_poly_mul_mid(..)   _nmod_poly_mul_mid_mpn_ctx
     MpnCtx.fmpz_poly_mul_mid(..)   _fmpz_poly_mul_mid_mpn_ctx (raw coefficient rows)
     MpnBatch(ctx, reqs)            batches of uneven products (no counterpart)
+    MpnPipe(depth)                 streams of host-pointer products (no counterpart)
     MpnCtx.mpn_mul_device(..)      device-pointer twin (no host copies)
+    mpn_mul_plan, mpn_mul_split_plan   plan introspection
 
 There is no CPU fallback: if the library or a GPU is missing, every call
 raises.
@@ -36,6 +38,11 @@ class GpuFftSmallError(RuntimeError):
 
 
 class _Ctx(ctypes.Structure):
+    _fields_ = [("impl", ctypes.c_void_p)]
+
+
+class _Pipe(ctypes.Structure):
+    """gpu_mpn_pipe_struct"""
     _fields_ = [("impl", ctypes.c_void_p)]
 
 
@@ -84,19 +91,20 @@ _P = ctypes.c_void_p
 _U = ctypes.c_ulong
 _S = ctypes.c_long
 _CTX = ctypes.POINTER(_Ctx)
+_PIPE = ctypes.POINTER(_Pipe)
 SIGNATURES = {
     "gpu_mpn_ctx_init": (None, [_CTX, _U]),
     "gpu_mpn_ctx_init_status": (ctypes.c_int, [_CTX, _U]),
     "gpu_mpn_ctx_clear": (None, [_CTX]),
     "gpu_mpn_ctx_mpn_mul": (None, [_CTX, _P, _P, _U, _P, _U]),
     "gpu_mpn_ctx_mpn_mul_status": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U]),
-    "gpu_mpn_pipe_init": (ctypes.c_int, [_CTX, ctypes.c_int]),
-    "gpu_mpn_pipe_submit": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, ctypes.POINTER(ctypes.c_longlong)]),
-    "gpu_mpn_pipe_wait": (ctypes.c_int, [_CTX, ctypes.c_longlong]),
-    "gpu_mpn_pipe_clear": (None, [_CTX]),
+    "gpu_mpn_pipe_init": (ctypes.c_int, [_PIPE, ctypes.c_int]),
+    "gpu_mpn_pipe_submit": (ctypes.c_int, [_PIPE, _P, _P, _U, _P, _U, ctypes.POINTER(ctypes.c_longlong)]),
+    "gpu_mpn_pipe_wait": (ctypes.c_int, [_PIPE, ctypes.c_longlong]),
+    "gpu_mpn_pipe_clear": (None, [_PIPE]),
     "gpu_test_crt_lookback_timeout": (ctypes.c_int, [_CTX]),
     "gpu_test_set_device_error": (ctypes.c_int, [_CTX]),
-    "gpu_test_pipe_slot_ctx": (ctypes.c_void_p, [_CTX, ctypes.c_int]),
+    "gpu_test_pipe_slot_ctx": (ctypes.c_void_p, [_PIPE, ctypes.c_int]),
     "_gpu_mpn_ctx_mpn_mul_range": (None, [_CTX, _P, _U, _U, _P, _U, _P, _U]),
     "gpu_mpn_mul_device": (ctypes.c_int, [_CTX, _P, _P, _U, _P, _U, _P]),
     "gpu_mpn_mul_device_noalloc": (ctypes.c_int, [_P, _P, _U, _P, _U, _P]),
@@ -499,7 +507,7 @@ class MpnPipe:
     pin_memory()) makes the copies asynchronous."""
 
     def __init__(self, depth=2):
-        self._c = _Ctx()   # same one-pointer layout as the pipeline handle
+        self._c = _Pipe()
         _check(lib().gpu_mpn_pipe_init(ctypes.byref(self._c), depth))
         self.depth = depth
         self._held = {}
