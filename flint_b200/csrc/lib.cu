@@ -19,6 +19,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -72,22 +73,65 @@ static void raise_error(int code)
 
 // ---------------------------------------------------------------------------
 // host number theory
+// Smallest primitive root mod p (no heap use: the allocation-free entry
+// point's set-up calls it too).
 static uint32_t primitive_root(uint32_t p)
 {
-    uint32_t m = p - 1;
-    std::vector<uint32_t> f;
+    uint32_t m = p - 1, f[32];
+    int nf = 0;
     for (uint32_t q = 2; (uint64_t)q * q <= m; q++)
         if (m % q == 0) {
-            f.push_back(q);
+            f[nf++] = q;
             while (m % q == 0) m /= q;
         }
-    if (m > 1) f.push_back(m);
+    if (m > 1) f[nf++] = m;
     for (uint32_t g = 2;; g++) {
         bool ok = true;
-        for (uint32_t q : f)
-            if (h_powmod(g, (p - 1) / q, p) == 1) { ok = false; break; }
+        for (int i = 0; i < nf; i++)
+            if (h_powmod(g, (p - 1) / f[i], p) == 1) { ok = false; break; }
         if (ok) return g;
     }
+}
+
+// Constant-memory tables that every kernel of the module reads: the
+// radix-32 twiddles w_32^k, w_32^-k of all MAX_NP primes (c_w32) and the
+// opaque constants of fadd/fsub (c_one, c_minus_one).  Their values depend on
+// nothing but the prime set, so they are written once per device, by
+// whichever of context creation or the allocation-free entry point's set-up
+// reaches the device first, and never rewritten while kernels may read them.
+// (A cudaDeviceReset would discard them with the module; this library never
+// resets a device.)
+constexpr int CONST_MAX_DEVICES = 64;
+static std::atomic<bool> g_const_ready[CONST_MAX_DEVICES];
+static std::mutex g_const_lock;
+
+static cudaError_t device_constants_ensure(int dev)
+{
+    if (dev >= 0 && dev < CONST_MAX_DEVICES && g_const_ready[dev].load(std::memory_order_acquire))
+        return cudaSuccess;
+    std::lock_guard<std::mutex> guard(g_const_lock);
+    if (dev >= 0 && dev < CONST_MAX_DEVICES && g_const_ready[dev].load(std::memory_order_relaxed))
+        return cudaSuccess;
+    W32Table w32[MAX_NP];
+    for (int j = 0; j < MAX_NP; j++) {
+        const uint32_t p = PRIMES[j];
+        const uint32_t w = h_powmod(primitive_root(p), (p - 1) >> LOG_MAXM, p);   // order 2^25
+        const uint32_t w32f = h_powmod(w, 1u << (LOG_MAXM - 5), p), w32i = h_invmod(w32f, p);
+        uint32_t x = 1, xi = 1;
+        for (int k = 0; k < 16; k++) {
+            w32[j].f[k] = make_uint2(x, shoup_companion(x, p));
+            w32[j].i[k] = make_uint2(xi, shoup_companion(xi, p));
+            x = h_mulmod(x, w32f, p);
+            xi = h_mulmod(xi, w32i, p);
+        }
+    }
+    const uint32_t one = 1, minus_one = 0xffffffffu;
+    cudaError_t e = cudaMemcpyToSymbol(c_w32, w32, sizeof w32);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_one, &one, sizeof one);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_minus_one, &minus_one, sizeof minus_one);
+    if (e == cudaSuccess && dev >= 0 && dev < CONST_MAX_DEVICES)
+        g_const_ready[dev].store(true, std::memory_order_release);
+    return e;
 }
 
 static uint2 shoup_pair(uint32_t w, uint32_t p)
@@ -206,7 +250,6 @@ static int ctx_build_tables(Ctx *X)
     const size_t n_tl = (size_t)MAX_NP * TL_SZ;
     std::vector<PrimeInfo> pi(MAX_NP);
     std::vector<uint2> twf(n_twf), twi(n_twf), th(n_th), tl(n_tl), thi(n_th), tli(n_tl);
-    std::vector<W32Table> w32tab(MAX_NP);
     for (int j = 0; j < MAX_NP; j++) {
         const uint32_t p = PRIMES[j];
         PrimeInfo &P = pi[j];
@@ -234,19 +277,6 @@ static int ctx_build_tables(Ctx *X)
                 twi[(size_t)j * TW_SZ + h + jj] = shoup_pair(xi, p);
                 x = h_mulmod(x, r, p);
                 xi = h_mulmod(xi, ri, p);
-            }
-        }
-        // uniform twiddles of the radix-32 pass: w_32^k, w_32^-k
-        {
-            const uint32_t w32 = h_powmod(w, 1u << (LOG_MAXM - 5), p);
-            const uint32_t w32i = h_invmod(w32, p);
-            W32Table &C = w32tab[j];
-            uint32_t x = 1, xi = 1;
-            for (int k = 0; k < 16; k++) {
-                C.f[k] = shoup_pair(x, p);
-                C.i[k] = shoup_pair(xi, p);
-                x = h_mulmod(x, w32, p);
-                xi = h_mulmod(xi, w32i, p);
             }
         }
         // twist tables
@@ -307,10 +337,7 @@ static int ctx_build_tables(Ctx *X)
     X->T.thi = (const uint2 *)(base + o_thi);
     X->T.tli = (const uint2 *)(base + o_tli);
     // constant memory belongs to the current device's module instance
-    CU(cudaMemcpyToSymbol(c_w32, w32tab.data(), sizeof(W32Table) * MAX_NP));
-    const uint32_t one = 1, minus_one = 0xffffffffu;
-    CU(cudaMemcpyToSymbol(c_one, &one, sizeof one));
-    CU(cudaMemcpyToSymbol(c_minus_one, &minus_one, sizeof minus_one));
+    CU(device_constants_ensure(X->device));
     CU(cudaDeviceGetAttribute(&X->nsm, cudaDevAttrMultiProcessorCount, X->device));
     return 0;
 }
@@ -1900,6 +1927,16 @@ int gpu_mpn_ctx_kernel_times(gpu_mpn_ctx_t R, double *ms, long *count, int max)
 // scratch, which keeps the last call's contents, so calls whose work overlaps on
 // the GPU (different streams, or different host threads) race and must be
 // serialised by the caller.
+//
+// The first call on a device sets the device up: it writes the module's
+// constant tables unless a context did so already, launches the table kernel
+// on CUDA's legacy default stream and synchronises the device.  Make that
+// first call before any stream capture.  Later calls only queue kernels on
+// the caller's stream and return; a device-side error (the carry look-back's
+// bounded wait running out, which takes a GPU that stops scheduling the
+// earlier tiles) is recorded in the scratch's error word but cannot be
+// reported by the return code, which only covers argument checks, the set-up
+// and the launches.
 constexpr int NA_LOG_MAXM = 18;
 constexpr uint64_t NA_MAX_LIMBS = ((uint64_t)1 << NA_LOG_MAXM) + 1;
 constexpr int NA_NP = 5;
@@ -1963,7 +2000,7 @@ __global__ void k_na_tables(uint2* twf, uint2* twi, uint2* th, uint2* tl, uint2*
 }
 
 struct NaDevice {
-    bool ready = false;
+    std::atomic<bool> ready{false};   // stored (release) after every field below is set
     Ctx ctx;                       // only T and nsm are used by the launches
     uint32_t *res = nullptr, *status = nullptr, *scale = nullptr;
     unsigned long long *ticket = nullptr;
@@ -2015,27 +2052,10 @@ static int na_setup(int dev, NaDevice &D)
     // order-2^25 roots of unity (forward, inverse) per prime
     uint2 roots[NA_NP];
     PrimeInfo pi[MAX_NP];
-    W32Table w32[MAX_NP];
     memset(pi, 0, sizeof pi);
-    memset(w32, 0, sizeof w32);
     for (int j = 0; j < NA_NP; j++) {
         const uint32_t p = PRIMES[j];
-        uint32_t m = p - 1, f[16];
-        int nf = 0;
-        for (uint32_t q = 2; (uint64_t)q * q <= m; q++)
-            if (m % q == 0) {
-                f[nf++] = q;
-                while (m % q == 0) m /= q;
-            }
-        if (m > 1) f[nf++] = m;
-        uint32_t g = 2;
-        for (;; g++) {
-            bool ok = true;
-            for (int i = 0; i < nf; i++)
-                if (h_powmod(g, (p - 1) / f[i], p) == 1) { ok = false; break; }
-            if (ok) break;
-        }
-        const uint32_t w = h_powmod(g, (p - 1) >> LOG_MAXM, p), wi = h_invmod(w, p);
+        const uint32_t w = h_powmod(primitive_root(p), (p - 1) >> LOG_MAXM, p), wi = h_invmod(w, p);
         roots[j] = make_uint2(w, wi);
         PrimeInfo &P = pi[j];
         P.p = p;
@@ -2045,14 +2065,6 @@ static int na_setup(int dev, NaDevice &D)
         P.c32 = (uint32_t)((1ull << 32) % p);
         P.r2 = h_mulmod(P.c32, P.c32, p);
         P.finv = 1.0f / (float)p;
-        const uint32_t w32f = h_powmod(w, 1u << (LOG_MAXM - 5), p), w32i = h_invmod(w32f, p);
-        uint32_t x = 1, xi = 1;
-        for (int k = 0; k < 16; k++) {
-            w32[j].f[k] = make_uint2(x, shoup_companion(x, p));
-            w32[j].i[k] = make_uint2(xi, shoup_companion(xi, p));
-            x = h_mulmod(x, w32f, p);
-            xi = h_mulmod(xi, w32i, p);
-        }
     }
     // device addresses of the image's arrays, taken with this device current
     void *scr = nullptr, *twf, *twi, *th, *tl, *thi, *tli, *pip, *sc;
@@ -2073,10 +2085,9 @@ static int na_setup(int dev, NaDevice &D)
         NA_CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     NA_CU(cudaMemcpyToSymbol(c_na_primes, PRIMES, sizeof(uint32_t) * NA_NP));
     NA_CU(cudaMemcpyToSymbol(c_na_roots, roots, sizeof roots));
-    NA_CU(cudaMemcpyToSymbol(c_w32, w32, sizeof(W32Table) * MAX_NP));
-    const uint32_t one = 1, minus_one = 0xffffffffu;
-    NA_CU(cudaMemcpyToSymbol(c_one, &one, sizeof one));
-    NA_CU(cudaMemcpyToSymbol(c_minus_one, &minus_one, sizeof minus_one));
+    // the module-wide constant tables (all MAX_NP primes), unless a context
+    // or an earlier set-up on this device has written them already
+    NA_CU(device_constants_ensure(dev));
     NA_CU(cudaMemcpyToSymbol(na_pi, pi, sizeof pi));
     k_na_tables<<<256, 256>>>((uint2 *)twf, (uint2 *)twi, (uint2 *)th, (uint2 *)tl, (uint2 *)thi,
                               (uint2 *)tli);
@@ -2111,7 +2122,7 @@ static int na_setup(int dev, NaDevice &D)
     D.ticket = (unsigned long long *)(D.status + NA_TILES + (NA_TILES & 1));   // 8-byte aligned
     D.err = (int *)(D.ticket + 1);
     D.scale = (uint32_t *)sc;
-    D.ready = true;
+    D.ready.store(true, std::memory_order_release);
     return 0;
 }
 
@@ -2121,14 +2132,15 @@ int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev, gpu_ulong
                                const uint64_t *b_dev, gpu_ulong bn, void *stream)
 {
     if (an == 0 || bn == 0 || !z_dev || !a_dev || !b_dev) return GPU_FFT_SMALL_EINVAL;
-    if (an + bn > NA_MAX_LIMBS) return GPU_FFT_SMALL_ETOOBIG;
+    if (an > NA_MAX_LIMBS || bn > NA_MAX_LIMBS - an) return GPU_FFT_SMALL_ETOOBIG;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES)
         return GPU_FFT_SMALL_ECUDA;
     NaDevice &D = g_na[dev];
-    if (!D.ready) {
+    if (!D.ready.load(std::memory_order_acquire)) {
         std::lock_guard<std::mutex> guard(g_na_lock);
-        if (!D.ready && na_setup(dev, D) != 0) return GPU_FFT_SMALL_ECUDA;
+        if (!D.ready.load(std::memory_order_relaxed) && na_setup(dev, D) != 0)
+            return GPU_FFT_SMALL_ECUDA;
     }
     const cudaStream_t st = (cudaStream_t)stream;
     const uint64_t L = an + bn - 1;
