@@ -23,7 +23,9 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libflint_b200.so")
+# FLINT_B200_LIB selects another build of the library (same C ABI), e.g. one
+# compiled with different options; the default is the in-tree build.
+LIB_PATH = os.environ.get("FLINT_B200_LIB") or os.path.join(_HERE, "libflint_b200.so")
 DEFAULT_PRIME = 0x0003F00000000001
 
 OK, EINVAL, ETOOBIG, ECUDA, ETIMEOUT, ENOPRIMES = 0, 1, 2, 3, 4, 5

@@ -345,7 +345,8 @@ static int ctx_build_tables(Ctx *X)
 // ---------------------------------------------------------------------------
 // kernel dispatch by transform shape (column length 2^logR, row length 2^logC)
 typedef void (*fwd_cols_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t,
-                            uint32_t *, uint32_t *, int, int, const InstDesc *, int, FzShape);
+                            uint32_t *, uint32_t *, int, int, const InstDesc *, int, FzShape,
+                            const uint32_t *, int);
 typedef void (*inv_cols_fn)(DevTables, uint32_t *, int, int, const InstDesc *, ChunkOut);
 typedef void (*rows_fn)(DevTables, uint32_t *, const uint32_t *, int, int, int, const uint32_t *,
                         int, const InstDesc *, int, int);
@@ -362,6 +363,34 @@ constexpr int tmpl_cols() { return LOGR >= 5 ? cols_per_tile(LOGR) : 0; }
 static const fwd_cols_fn FWD_COLS[12] = {FB_COLS(k_fwd_cols, , false)};
 static const fwd_cols_fn FWD_COLS_FZ[12] = {FB_COLS(k_fwd_cols, , true)};
 static const inv_cols_fn INV_COLS[12] = {FB_COLS(k_inv_cols)};
+// constant-stride instances: 2^13-point rows under 2^9..2^11-point columns
+// (index logR - 9) and 2^14-point rows under 2^11-point columns
+static const fwd_cols_fn FWD_COLS_C13[3] = {k_fwd_cols<9, tmpl_cols<9>(), false, 13>,
+                                            k_fwd_cols<10, tmpl_cols<10>(), false, 13>,
+                                            k_fwd_cols<11, tmpl_cols<11>(), false, 13>};
+static const fwd_cols_fn FWD_COLS_FZ_C13[3] = {k_fwd_cols<9, tmpl_cols<9>(), true, 13>,
+                                               k_fwd_cols<10, tmpl_cols<10>(), true, 13>,
+                                               k_fwd_cols<11, tmpl_cols<11>(), true, 13>};
+static const inv_cols_fn INV_COLS_C13[3] = {k_inv_cols<9, tmpl_cols<9>(), 13>,
+                                            k_inv_cols<10, tmpl_cols<10>(), 13>,
+                                            k_inv_cols<11, tmpl_cols<11>(), 13>};
+static const fwd_cols_fn FWD_COLS_C14 = k_fwd_cols<11, tmpl_cols<11>(), false, 14>;
+static const fwd_cols_fn FWD_COLS_FZ_C14 = k_fwd_cols<11, tmpl_cols<11>(), true, 14>;
+static const inv_cols_fn INV_COLS_C14 = k_inv_cols<11, tmpl_cols<11>(), 14>;
+
+// the column kernels for a transform shape
+static fwd_cols_fn fwd_cols_kernel(int logR, int logC, bool fz = false)
+{
+    if (logR == 11 && logC == 14) return fz ? FWD_COLS_FZ_C14 : FWD_COLS_C14;
+    if (logR >= 9 && logR <= 11 && logC == 13) return (fz ? FWD_COLS_FZ_C13 : FWD_COLS_C13)[logR - 9];
+    return (fz ? FWD_COLS_FZ : FWD_COLS)[logR];
+}
+static inv_cols_fn inv_cols_kernel(int logR, int logC)
+{
+    if (logR == 11 && logC == 14) return INV_COLS_C14;
+    if (logR >= 9 && logR <= 11 && logC == 13) return INV_COLS_C13[logR - 9];
+    return INV_COLS[logR];
+}
 // Rows run with 32 elements per thread (k_rows<LOGC, 5>).  The kernel also
 // builds with 16 per thread (k_rows<14, 4>: 1024 threads, 32 warps per SM, 64
 // registers); measured on the 2^24 product that is slower (1.88 against
@@ -468,6 +497,14 @@ static int configure_kernels()
         CU(cudaFuncSetAttribute(FWD_COLS_FZ[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
         CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
+    for (int r = 0; r < 3; r++) {
+        CU(cudaFuncSetAttribute(FWD_COLS_C13[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(FWD_COLS_FZ_C13[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(INV_COLS_C13[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    }
+    CU(cudaFuncSetAttribute(FWD_COLS_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    CU(cudaFuncSetAttribute(FWD_COLS_FZ_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    CU(cudaFuncSetAttribute(INV_COLS_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     for (int c = 5; c <= LOG_MAXC; c++) {
         CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         CU(cudaFuncSetAttribute(ROWS_FWD[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
@@ -726,27 +763,32 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     const MulShape &S = L.S;
     const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
     const FzShape shape = fz ? *fz : FzShape{1, 1, 1};
+    // Products of two operands whose columns are long enough for the
+    // per-thread twist (2^5 points or more) fold the pointwise scale into
+    // b's twist factors, so the row pass multiplies the spectra once instead
+    // of twice; squarings keep the scale in the row pass.
+    const bool fold = !(sq && !desc) && S.logR >= 5;
     if (b_ready && !desc && !sq) {
         // b is still arriving: a's column pass first, b's after its copy
-        (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
-            X->T, a, an, a, an, ra, ra, S.logC, S.G, nullptr, np, shape);
+        fwd_cols_kernel(S.logR, S.logC, fz != nullptr)<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
+            X->T, a, an, a, an, ra, ra, S.logC, S.G, nullptr, np, shape, d_scale, 0);
         cudaStreamWaitEvent(st, b_ready, 0);
         const FzShape shb = fz ? FzShape{shape.S, shape.wb, shape.wb} : shape;
-        (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
-            X->T, b, bn, b, bn, rb, rb, S.logC, S.G, nullptr, np, shb);
+        fwd_cols_kernel(S.logR, S.logC, fz != nullptr)<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
+            X->T, b, bn, b, bn, rb, rb, S.logC, S.G, nullptr, np, shb, d_scale, fold ? 1 : 0);
     } else {
         if (b_ready) cudaStreamWaitEvent(st, b_ready, 0);
-        (fz ? FWD_COLS_FZ : FWD_COLS)[S.logR]<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
-            X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np, shape);
+        fwd_cols_kernel(S.logR, S.logC, fz != nullptr)<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
+            X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np, shape, d_scale, fold ? 2 : 0);
     }
     timing_mark(tr, 1, st);
     const int items = L.row_grid * np * (desc ? ninst : 1);
     ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
-        X->T, ra, rb, S.logR, L.nv, np, d_scale, (sq && !desc) ? 1 : 0, desc, desc ? ninst : 1,
-        1 << S.logR);
+        X->T, ra, rb, S.logR, L.nv, np, fold ? nullptr : d_scale, (sq && !desc) ? 1 : 0, desc,
+        desc ? ninst : 1, 1 << S.logR);
     timing_mark(tr, 2, st);
     if (S.logR > 0)
-        INV_COLS[S.logR]<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
+        inv_cols_kernel(S.logR, S.logC)<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
             X->T, ra, S.logC, S.G, desc, co ? *co : ChunkOut{nullptr, 0, 0, 0, 0});
     timing_mark(tr, 3, st);
 }
@@ -958,8 +1000,8 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
         const MulShape &S = Ls.S;
         const FzShape one{1, 1, 1};
         if (b_ready) CU(cudaStreamWaitEvent(st, b_ready, 0));
-        FWD_COLS[S.logR]<<<dim3(np, Ls.col_grid, 1), Ls.col_threads, Ls.col_smem, st>>>(
-            X->T, y, yn, y, yn, cb, cb, S.logC, S.G, nullptr, np, one);
+        fwd_cols_kernel(S.logR, S.logC)<<<dim3(np, Ls.col_grid, 1), Ls.col_threads, Ls.col_smem, st>>>(
+            X->T, y, yn, y, yn, cb, cb, S.logC, S.G, nullptr, np, one, nullptr, 0);
         ROWS_FWD[S.logC]<<<((1 << S.logR) / Ls.nv) * np, Ls.nv * (1 << S.logC) / 32,
                            Ls.nv * padw(1 << S.logC) * sizeof(uint32_t), st>>>(X->T, cb, S.logR, Ls.nv, np,
                                                                               1 << S.logR);
@@ -968,11 +1010,11 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
         for (uint64_t i = 0; i * c < xn; i++) {
             const uint64_t xi = std::min(c, xn - i * c);
             const ChunkOut co{ra, logM, i * c, i ? yn - 1 : 0, xi + yn - 1};
-            FWD_COLS[S.logR]<<<dim3(np, Ls.col_grid, 1), Ls.col_threads, Ls.col_smem, st>>>(
-                X->T, x + i * c, xi, x + i * c, xi, ca, ca, S.logC, S.G, nullptr, np, one);
+            fwd_cols_kernel(S.logR, S.logC)<<<dim3(np, Ls.col_grid, 1), Ls.col_threads, Ls.col_smem, st>>>(
+                X->T, x + i * c, xi, x + i * c, xi, ca, ca, S.logC, S.G, nullptr, np, one, nullptr, 0);
             ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(Ls)), Ls.row_threads, Ls.row_smem, st>>>(
                 X->T, ca, cb, S.logR, Ls.nv, np, scale_ptr(X, np, Lc), 2, nullptr, 1, 1 << S.logR);
-            INV_COLS[S.logR]<<<dim3(Ls.col_grid, np, 1), Ls.col_threads, Ls.col_smem, st>>>(X->T, ca, S.logC, S.G,
+            inv_cols_kernel(S.logR, S.logC)<<<dim3(Ls.col_grid, np, 1), Ls.col_threads, Ls.col_smem, st>>>(X->T, ca, S.logC, S.G,
                                                                                           nullptr, co);
             launches += 3;
         }
@@ -2080,6 +2122,10 @@ static int na_setup(int dev, NaDevice &D)
     for (int r = 0; r < 12; r++) {
         NA_CU(cudaFuncSetAttribute(FWD_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
         NA_CU(cudaFuncSetAttribute(INV_COLS[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    }
+    for (int r = 0; r < 3; r++) {
+        NA_CU(cudaFuncSetAttribute(FWD_COLS_C13[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        NA_CU(cudaFuncSetAttribute(INV_COLS_C13[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
     for (int c = 5; c <= LOG_MAXC; c++)
         NA_CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));

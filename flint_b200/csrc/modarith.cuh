@@ -114,62 +114,92 @@ __constant__ uint32_t c_minus_one;  // 0xffffffff
 __device__ __forceinline__ uint32_t fadd(uint32_t x, uint32_t y) { return x * c_one + y; }
 __device__ __forceinline__ uint32_t fsub(uint32_t x, uint32_t y) { return y * c_minus_one + x; }
 
+// min(x + y, x + y - p) style reductions use the fused add-and-minimum
+// (VIADDMNMX on sm_100, one ALU instruction for the add and the unsigned
+// minimum): viaddmin(x, y, z) = min(x + y, z).
+__device__ __forceinline__ uint32_t viaddmin(uint32_t x, uint32_t y, uint32_t z) { return __viaddmin_u32(x, y, z); }
+
+// Butterfly forms.  F selects how the additions and reductions issue:
+//   F = -1  fused add-and-minimum (VIADDMNMX) for every reduction, twiddle-1
+//           butterflies on the ALU only: the fewest instructions;
+//   F = -2  fused reductions, twiddle-1 butterflies as for F = 0;
+//   F =  0  separate add and minimum, twiddle-1 butterflies with their add
+//           and subtract on the FMA pipe (fadd / fsub);
+//   F >= 1  as 0 with F of the additions on the FMA pipe.
+// On sm_100 the three multiplications of Shoup's product hold the FMA pipe
+// for 8 cycles per warp (the high-half multiply takes 4).  Which form runs
+// fastest depends on the kernel around it (register budget and what else
+// competes for the pipes); the choices are measured per pass kind
+// (ntt_smem.cuh).
+
 // Gentleman-Sande butterfly, inputs and outputs in [0, p):
 // (a, b) -> (a + b, (a - b) w).
-// F (0, 1 or 2) is the number of additions sent to the FMA pipe: 2 for
-// kernels whose other work is ALU-heavy, fewer for kernels whose other work
-// is multiplication-heavy.  The high-half multiply occupies the FMA pipe for
-// two issue slots.
-template <int F = 2>
+template <int F = 0>
 __device__ __forceinline__ void bfly_gs(uint32_t& a, uint32_t& b, uint32_t w, uint32_t wq, uint32_t p)
 {
-    const uint32_t s = F >= 1 ? fadd(a, b) : a + b;
-    const uint32_t s1 = a + b - p;          // ALU
     const uint32_t d = a - b + p;           // ALU, in [1, 2p)
     const uint32_t q = __umulhi(d, wq);
     const uint32_t r = d * w - q * p;       // [0, 2p)
-    const uint32_t r1 = F >= 2 ? fadd(r, 0u - p) : r - p;
-    a = min(s, s1);
-    b = min(r, r1);
+    if constexpr (F < 0) {
+        a = viaddmin(a, b, a + b - p);      // min(a + b, a + b - p)
+        b = viaddmin(r, 0u - p, r);         // min(r - p, r)
+    } else {
+        const uint32_t s = F >= 1 ? fadd(a, b) : a + b;
+        const uint32_t s1 = a + b - p;
+        const uint32_t r1 = F >= 2 ? fadd(r, 0u - p) : r - p;
+        a = min(s, s1);
+        b = min(r, r1);
+    }
 }
 
 // Gentleman-Sande butterfly with twiddle 1
+template <int F = 0>
 __device__ __forceinline__ void bfly_gs1(uint32_t& a, uint32_t& b, uint32_t p)
 {
-    const uint32_t s = fadd(a, b);
-    const uint32_t s1 = a + b - p;
-    const uint32_t d = a - b + p;
-    const uint32_t d1 = fsub(a, b);
-    a = min(s, s1);
-    b = min(d, d1);
+    if constexpr (F == -1) {
+        const uint32_t s1 = a + b - p;
+        const uint32_t d = a - b;
+        a = viaddmin(a, b, s1);             // min(a + b, a + b - p)
+        b = viaddmin(d, p, d);              // min(a - b + p, a - b)
+    } else {
+        const uint32_t s = fadd(a, b);
+        const uint32_t s1 = a + b - p;
+        const uint32_t d = a - b + p;
+        const uint32_t d1 = fsub(a, b);
+        a = min(s, s1);
+        b = min(d, d1);
+    }
 }
 
 // Cooley-Tukey butterfly, inputs and outputs in [0, p):
-// (x, y) -> (x + y w, x - y w); F as for bfly_gs (up to 3 here)
-template <int F = 2>
+// (x, y) -> (x + y w, x - y w)
+template <int F = 0>
 __device__ __forceinline__ void bfly_ct(uint32_t& x, uint32_t& y, uint32_t w, uint32_t wq, uint32_t p)
 {
     const uint32_t q = __umulhi(y, wq);
     uint32_t t = y * w - q * p;             // [0, 2p)
-    t = min(t, F >= 3 ? fadd(t, 0u - p) : t - p);
-    const uint32_t s = F >= 1 ? fadd(x, t) : x + t;
-    const uint32_t s1 = x + t - p;
-    const uint32_t d = x - t + p;
-    const uint32_t d1 = F >= 2 ? fsub(x, t) : x - t;
-    x = min(s, s1);
-    y = min(d, d1);
+    if constexpr (F < 0) {
+        t = viaddmin(t, 0u - p, t);         // [0, p)
+        const uint32_t s1 = x + t - p;
+        const uint32_t d = x - t;
+        x = viaddmin(x, t, s1);
+        y = viaddmin(d, p, d);
+    } else {
+        t = min(t, F >= 3 ? fadd(t, 0u - p) : t - p);
+        const uint32_t s = F >= 1 ? fadd(x, t) : x + t;
+        const uint32_t s1 = x + t - p;
+        const uint32_t d = x - t + p;
+        const uint32_t d1 = F >= 2 ? fsub(x, t) : x - t;
+        x = min(s, s1);
+        y = min(d, d1);
+    }
 }
 
-// Cooley-Tukey butterfly with twiddle 1
+// Cooley-Tukey butterfly with twiddle 1 (the same arithmetic as bfly_gs1)
+template <int F = 0>
 __device__ __forceinline__ void bfly_ct1(uint32_t& x, uint32_t& y, uint32_t p)
 {
-    const uint32_t t = y;
-    const uint32_t s = fadd(x, t);
-    const uint32_t s1 = x + t - p;
-    const uint32_t d = x - t + p;
-    const uint32_t d1 = fsub(x, t);
-    x = min(s, s1);
-    y = min(d, d1);
+    bfly_gs1<F>(x, y, p);
 }
 #endif
 

@@ -96,10 +96,12 @@ __device__ __forceinline__ uint32_t shoup_companion_dev(uint32_t w, uint32_t p)
 // beta = w^(col 2^(r-5)).  They are generated by a Shoup chain in Montgomery
 // form (F_(k+1) = F_k beta) and applied with one Montgomery product each,
 // so no table is read per element.
+// fsc != 0 multiplies every factor by fsc (a pointwise scale folded into
+// this operand's transform; one extra product per thread).
 template <int LOGR>
 __device__ __forceinline__ void twist32(uint32_t (&x)[32], uint32_t col, int s, int logM,
                                         const uint2* __restrict__ th, const uint2* __restrict__ tl,
-                                        const PrimeInfo& P)
+                                        const PrimeInfo& P, uint32_t fsc = 0)
 {
     const uint32_t p = P.p;
     const uint32_t mmask = (1u << logM) - 1;
@@ -110,6 +112,7 @@ __device__ __forceinline__ void twist32(uint32_t (&x)[32], uint32_t col, int s, 
     const uint32_t beta = table_power(e1, th, tl, p);
     const uint32_t bq = shoup_companion_dev(beta, p);
     uint32_t F = mul_mont(alpha, P.r2, p, P.pneg_inv);   // alpha in Montgomery form
+    if (fsc) F = mul_mont(F, fsc, p, P.pneg_inv);         // alpha fsc, Montgomery form
 #pragma unroll
     for (int k = 0; k < 32; k++) {
         const int m = (int)(__brev((unsigned)k) >> 27);
@@ -166,15 +169,19 @@ __device__ __forceinline__ uint32_t load_residue(const uint64_t* __restrict__ x,
 // with a batch descriptor, grid.z = 2 * instance + operand.  FZ selects the
 // integer-polynomial source (an, bn count coefficients, shape in fz).
 // smem = padw(R * G) words.
-template <int LOGR, int G, bool FZ>
-__global__ void __launch_bounds__(512)
-k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
-           const uint64_t* __restrict__ b, uint64_t bn,
-           uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols,
-           const InstDesc* __restrict__ desc, int np, FzShape fz)
+// LC != 0: the row length 2^LC is a compile-time constant (logC == LC), so
+// the strided stores take immediate offsets instead of address arithmetic.
+template <int LOGR, int G, bool FZ, int LC>
+__device__ __forceinline__ void
+fwd_cols_body(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
+              const uint64_t* __restrict__ b, uint64_t bn,
+              uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols,
+              const InstDesc* __restrict__ desc, int np, FzShape fz, const uint32_t* __restrict__ fscale,
+              int fmask)
 {
     extern __shared__ uint32_t sm[];
     constexpr int R = 1 << LOGR;
+    if constexpr (LC != 0) logC = LC;
     const int C = 1 << logC;
     const int logM = LOGR + logC;
     const int GR = G ? G : gcols;          // runtime tile width for short columns
@@ -248,6 +255,9 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     const int sh = LOG_MAXM - logM;
     const uint32_t mmask = (uint32_t)(M - 1);
     if constexpr (LOGR >= 5) {
+        // pointwise scale folded into this operand's twist (fmask bit 0: the
+        // first operand, bit 1: the second)
+        const uint32_t fsc = (fmask >> (opb ? 1 : 0)) & 1 ? fscale[j] : 0u;
         gs_strided_all<LOGR, G>(sm, 1, T.twf + (size_t)j * TW_SZ, p);
         constexpr int NS = R / 32;
         for (int f = threadIdx.x; f < G * NS; f += blockDim.x) {
@@ -258,13 +268,18 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             for (int m = 0; m < 32; m++) xr[m] = sm[pb + padw(m * G)];
             gs_contig<5, COL_FMA_ADDS>(xr, c_w32[j], p);
             const uint32_t col = (uint32_t)(i0 + v);
-            twist32<LOGR>(xr, col, s, logM, th, tl, P);
+            twist32<LOGR>(xr, col, s, logM, th, tl, P, fsc);
             // rows 32 s .. 32 s + 31 of column col: a pointer bump per row keeps
             // the address arithmetic on the ALU pipe (the FMA pipe is this
             // kernel's busiest unit)
             uint32_t* o = out + ((size_t)(32 * s) << logC) + col;
+            if constexpr (LC != 0) {
 #pragma unroll
-            for (int m = 0; m < 32; m++, o += C) *o = xr[m];
+                for (int m = 0; m < 32; m++) o[m * (1 << LC)] = xr[m];
+            } else {
+#pragma unroll
+                for (int m = 0; m < 32; m++, o += C) *o = xr[m];
+            }
         }
     } else {
         // short columns: one thread owns a whole column
@@ -285,6 +300,27 @@ k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             }
         }
     }
+}
+
+// Kernel instances: LC = 0 takes the row length at run time; LC = 14 serves
+// 2^14-point rows under 2^11-point columns (2^25 points) and LC = 13 2^13-point
+// rows under 2^9- to 2^11-point columns, with constant strides (measured on
+// the 2^25-point forward pass: 1.28 -> 1.13 ms).  An LC instance also holds
+// the run-time body behind a branch that never takes it for its shape: with
+// that second body the compiler schedules the constant-stride one better
+// (1.21 ms alone, 1.13 ms with it; three bodies in one kernel: 1.24 ms).
+template <int LOGR, int G, bool FZ, int LC = 0>
+__global__ void __launch_bounds__(512)
+k_fwd_cols(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
+           const uint64_t* __restrict__ b, uint64_t bn,
+           uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logC, int gcols,
+           const InstDesc* __restrict__ desc, int np, FzShape fz, const uint32_t* __restrict__ fscale,
+           int fmask)
+{
+    if (LC != 0 && logC == LC)
+        fwd_cols_body<LOGR, G, FZ, LC>(T, a, an, b, bn, ra, rb, logC, gcols, desc, np, fz, fscale, fmask);
+    else
+        fwd_cols_body<LOGR, G, FZ, 0>(T, a, an, b, bn, ra, rb, logC, gcols, desc, np, fz, fscale, fmask);
 }
 
 // ---------------------------------------------------------------------------
@@ -465,11 +501,17 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
                 cp_async_commit();
             }
         }
-        const uint32_t sc = scale[j];
+        if (scale) {
+            const uint32_t sc = scale[j];
 #pragma unroll
-        for (int m = 0; m < E; m++) {
-            const uint32_t y = squaring == 1 ? xr[m] : breg[m];
-            xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
+            for (int m = 0; m < E; m++) {
+                const uint32_t y = squaring == 1 ? xr[m] : breg[m];
+                xr[m] = mul_mont(mul_mont(xr[m], y, p, P.pneg_inv), sc, p, P.pneg_inv);
+            }
+        } else {
+            // the scale was folded into b's forward transform (k_fwd_cols)
+#pragma unroll
+            for (int m = 0; m < E; m++) xr[m] = mul_mont(xr[m], breg[m], p, P.pneg_inv);
         }
         ct_contig<LOGE, ROW_CT_FMA_ADDS>(xr, c_w32[j], p);
 #pragma unroll
@@ -517,13 +559,14 @@ struct ChunkOut {
 // ---------------------------------------------------------------------------
 // Column pass, inverse: untwist in registers + length-R inverse transforms,
 // in place (or into a split product's residues, ChunkOut).  grid = (C / G, np, instances); smem = padw(R * G) words.
-template <int LOGR, int G>
-__global__ void __launch_bounds__(512)
-k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
-           const InstDesc* __restrict__ desc, ChunkOut co)
+template <int LOGR, int G, int LC>
+__device__ __forceinline__ void
+inv_cols_body(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
+              const InstDesc* __restrict__ desc, ChunkOut co)
 {
     extern __shared__ uint32_t sm[];
     constexpr int R = 1 << LOGR;
+    if constexpr (LC != 0) logC = LC;
     const int C = 1 << logC;
     const int logM = LOGR + logC;
     const int GR = G ? G : gcols;
@@ -544,10 +587,11 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
             const int v = f & (G - 1), s = f / G;
             const uint32_t col = (uint32_t)(i0 + v);
             uint32_t xr[32];
+            const uint32_t* src = buf + ((size_t)(32 * s) << logC) + col;
 #pragma unroll
-            for (int m = 0; m < 32; m++) xr[m] = buf[(size_t)(32 * s + m) * C + col];
+            for (int m = 0; m < 32; m++) xr[m] = src[(size_t)m * C];
             twist32<LOGR>(xr, col, s, logM, th, tl, P);
-            ct_contig<5, COL_FMA_ADDS>(xr, c_w32[j], p);
+            ct_contig<5, COL_CT_FMA_ADDS>(xr, c_w32[j], p);
             const int pb = 33 * G * s + v;
 #pragma unroll
             for (int m = 0; m < 32; m++) sm[pb + padw(m * G)] = xr[m];
@@ -585,11 +629,19 @@ k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
                 const uint32_t e = ((col * bitrev_bits(m, LOGR)) & mmask) << sh;
                 xr[m] = twist_mul(buf[(size_t)m * C + col], e, th, tl, p);
             }
-            ct_contig<LOGR, COL_FMA_ADDS>(xr, c_w32[j], p);
+            ct_contig<LOGR, COL_CT_FMA_ADDS>(xr, c_w32[j], p);
 #pragma unroll
             for (int m = 0; m < R; m++) buf[(size_t)m * C + col] = xr[m];
         }
     }
+}
+
+template <int LOGR, int G, int LC = 0>
+__global__ void __launch_bounds__(512)
+k_inv_cols(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
+           const InstDesc* __restrict__ desc, ChunkOut co)
+{
+    inv_cols_body<LOGR, G, LC>(T, ra, logC, gcols, desc, co);
 }
 
 // ---------------------------------------------------------------------------

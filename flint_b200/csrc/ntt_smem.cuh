@@ -35,21 +35,31 @@
 namespace fb {
 
 constexpr int MAX_NP = 7;
-// Additions per butterfly sent to the FMA pipe: column passes, row forward
+// Butterfly form per pass kind (bfly_gs's F): column passes, row forward
 // (Gentleman-Sande) passes, row inverse (Cooley-Tukey) passes.  Measured on
-// the B200 (2^24 x 2^24 product): every kernel is fastest with all additions
-// on the ALU pipe (row pass 1.98 ms with 2/3 FMA additions, 1.74 ms with
-// none); the FMA pipe is left to the multiplications.
+// the B200 (2^24 x 2^24 product): the row pass is fastest with the fused
+// add-and-minimum form (F = -1: 1.500 -> 1.474 ms with the twiddle-1
+// butterflies off the FMA pipe); the column passes, whose kernels run at 64
+// registers, are fastest with separate adds and minima (F = 0; the fused
+// form took the forward column pass from 1.28 to 1.56 ms); FMA-pipe
+// additions (F >= 1) were slower everywhere (row pass 1.98 ms with 2/3 of
+// them, 1.74 ms with none).
 #ifndef FB_COL_FMA_ADDS
 #define FB_COL_FMA_ADDS 0
 #endif
+// inverse column passes: fused reductions with FMA-pipe twiddle-1 butterflies
+// (F = -2: 0.561 -> 0.539 ms against F = 0)
+#ifndef FB_COL_CT_FMA_ADDS
+#define FB_COL_CT_FMA_ADDS (-2)
+#endif
 #ifndef FB_ROW_GS_FMA_ADDS
-#define FB_ROW_GS_FMA_ADDS 0
+#define FB_ROW_GS_FMA_ADDS (-1)
 #endif
 #ifndef FB_ROW_CT_FMA_ADDS
-#define FB_ROW_CT_FMA_ADDS 0
+#define FB_ROW_CT_FMA_ADDS (-1)
 #endif
 constexpr int COL_FMA_ADDS = FB_COL_FMA_ADDS;
+constexpr int COL_CT_FMA_ADDS = FB_COL_CT_FMA_ADDS;
 // unroll factor of the strided passes' sub-transform loops
 #ifndef FB_PASS_UNROLL
 #define FB_PASS_UNROLL 1
@@ -83,7 +93,7 @@ __device__ __forceinline__ void gs_contig(uint32_t (&x)[1 << Q], const W32Table&
             if ((m & hm) == 0) {
                 const int k = m & (hm - 1);
                 if (k == 0) {
-                    bfly_gs1(x[m], x[m + hm], p);
+                    bfly_gs1<F>(x[m], x[m + hm], p);
                 } else {
                     const uint2 w = W.f[k * (16 / hm)];
                     bfly_gs<F>(x[m], x[m + hm], w.x, w.y, p);
@@ -108,8 +118,8 @@ __device__ __forceinline__ void gs_contig2(uint32_t (&x)[1 << Q], uint32_t (&y)[
             if ((m & hm) == 0) {
                 const int k = m & (hm - 1);
                 if (k == 0) {
-                    bfly_gs1(x[m], x[m + hm], p);
-                    bfly_gs1(y[m], y[m + hm], p);
+                    bfly_gs1<F>(x[m], x[m + hm], p);
+                    bfly_gs1<F>(y[m], y[m + hm], p);
                 } else {
                     const uint2 w = W.f[k * (16 / hm)];
                     bfly_gs<F>(x[m], x[m + hm], w.x, w.y, p);
@@ -133,7 +143,7 @@ __device__ __forceinline__ void ct_contig(uint32_t (&x)[1 << Q], const W32Table&
             if ((m & hm) == 0) {
                 const int k = m & (hm - 1);
                 if (k == 0) {
-                    bfly_ct1(x[m], x[m + hm], p);
+                    bfly_ct1<F>(x[m], x[m + hm], p);
                 } else {
                     const uint2 w = W.i[k * (16 / hm)];
                     bfly_ct<F>(x[m], x[m + hm], w.x, w.y, p);
@@ -312,7 +322,7 @@ __device__ __forceinline__ void ct_pass_smem(uint32_t* sm, int nv, const uint2* 
         uint32_t x[E];
 #pragma unroll
         for (int m = 0; m < E; m++) x[m] = sm[pb + padw(m * SG)];
-        ct_strided<Q, H, (G == 0 ? ROW_CT_FMA_ADDS : COL_FMA_ADDS)>(x, twi, jj0, p);
+        ct_strided<Q, H, (G == 0 ? ROW_CT_FMA_ADDS : COL_CT_FMA_ADDS)>(x, twi, jj0, p);
 #pragma unroll
         for (int m = 0; m < E; m++) sm[pb + padw(m * SG)] = x[m];
     }
