@@ -138,6 +138,27 @@ def ref_library():
     return None, "port", 1
 
 
+def host_info():
+    """CPU model, host threads and GMP version of this host (the CPU
+    baseline's context)."""
+    import ctypes
+    model = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    gmp_version = "unknown"
+    try:
+        import oracle
+        gmp_version = ctypes.c_char_p.in_dll(oracle.gmp(), "__gmp_version").value.decode()
+    except (OSError, ValueError, AttributeError):
+        pass
+    return {"cpu_model": model, "host_threads": os.cpu_count() or 1, "gmp_version": gmp_version}
+
+
 def cpu_baseline_run(an, bn, steps, warmup, max_seconds=60.0):
     """Time the reference's fft_small mpn_mul (or, when it is not built, the
     oracle's C restatement on a smaller sample) on this host."""
@@ -171,7 +192,7 @@ def cpu_baseline_run(an, bn, steps, warmup, max_seconds=60.0):
     return {"value": bits / med / 1e9, "unit": "Gbit/s", "cores": cores, "kind": kind,
             "sample": sample + ", median of %d, host threads available %d" %
             (len(times), os.cpu_count() or 1),
-            "ms_per_step": med * 1e3, "steps_timed": len(times)}
+            "ms_per_step": med * 1e3, "steps_timed": len(times), **host_info()}
 
 
 BATCH_N, BATCH_SEED = 4096, 4096
@@ -237,11 +258,14 @@ def train_cost_model(ctx):
 STREAM_SEED = 5005
 
 
-def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds):
+def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_held=1000):
     """The mixed request stream (half mpn products, an log-uniform in
     [2^6, 2^22], ratio log-uniform in [1, 64]; half integer-polynomial
     products, lengths log-uniform in [2^8, 2^16], coefficient bits uniform in
-    [64, 4096]) under the learned schedule and under the fixed rule."""
+    [64, 4096]) under the learned schedule and under the fixed rule.  Every
+    product of the two runs is compared by a 64-bit device digest; a
+    stratified subsample is compared limb for limb with the reference's own
+    products (and timed on the host)."""
     from flint_b200 import tuner
     from flint_b200.stream import run_stream
     from flint_b200.workload import request_stream
@@ -250,27 +274,38 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds):
     learned = model.choose(reqs)
     t_choose = time.perf_counter() - t0
     default = [tuner.default_config(r) for r in reqs]
-    keep = set(range(0, n_req, max(1, n_req // 24)))
-    rl = run_stream(ctx, torch, reqs, learned, 17, stream, dev, keep=keep, check_against=default)
+    keep = stream_subsample(reqs)
+    t0 = time.perf_counter()
+    rl = run_stream(ctx, torch, reqs, learned, 17, stream, dev, keep=keep)
+    t1 = time.perf_counter()
     rd = run_stream(ctx, torch, reqs, default, 17, stream, dev)
-    held = request_stream(STREAM_SEED + 2, 32)
+    t2 = time.perf_counter()
+    same = rl["digests"] == rd["digests"]
+    held = request_stream(STREAM_SEED + 2, n_held)
+    t0 = time.perf_counter()
     reg = tuner.regret(tun, held, model.choose(held))
+    reg["seconds"] = time.perf_counter() - t0
     bits_mpn = NS_LIMB_BITS * rl["mpn_limbs"]
     res = {
         "workload": "%d requests: half mpn_mul (an log-uniform [2^6, 2^22], an/bn log-uniform "
                     "[1, 64]), half fmpz_poly_mul (lengths log-uniform [2^8, 2^16], coefficient "
                     "bits uniform [64, 4096]), seed %d; mpn products in planned batches, "
-                    "integer polynomials one call each" % (n_req, STREAM_SEED),
+                    "integer polynomials in list calls (gpu_fmpz_poly_mul_mid_device_list)"
+                    % (n_req, STREAM_SEED),
         "requests": n_req, "mpn_requests": rl["mpn_requests"], "fmpz_requests": rl["fmpz_requests"],
+        "mpn_limbs": rl["mpn_limbs"], "fmpz_coeff_limbs": rl["fmpz_coeff_limbs"],
         "learned": {"total_ms": rl["total_ms"], "mpn_ms": rl["mpn_ms"], "fmpz_ms": rl["fmpz_ms"],
                     "mpn_Gbit_s": bits_mpn / rl["mpn_ms"] / 1e6},
         "default_rule": {"total_ms": rd["total_ms"], "mpn_ms": rd["mpn_ms"], "fmpz_ms": rd["fmpz_ms"],
                          "mpn_Gbit_s": bits_mpn / rd["mpn_ms"] / 1e6},
         "gain_over_default_rule": rd["total_ms"] / rl["total_ms"],
-        "choose_s": t_choose,
+        "choose_s": t_choose, "wall_s": {"learned_run": t1 - t0, "default_run": t2 - t1},
         "routes": {"transform": sum(c.route == 0 for c in learned),
                    "basecase": sum(c.route == 1 for c in learned)},
-        "identical_to_default_rule": rl["identical"],
+        "identical_to_default_rule": bool(same.all()),
+        "digests_compared": int(len(same)), "digests_equal": int(same.sum()),
+        "digest_note": "per product: sum of its limbs times fixed pseudo-random 64-bit weights, "
+                       "mod 2^64, computed on the device, learned run against default-rule run",
         "held_out_regret_vs_exhaustive": reg,
     }
     if cpu_seconds > 0:
@@ -278,15 +313,30 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds):
     return res
 
 
+def stream_subsample(reqs, per_kind=24, mpn_cap=1 << 20, fmpz_cap=1 << 22):
+    """Indices of a stratified subsample of the stream: for each kind, requests
+    spread evenly over the kind's size order, up to a size cap so the
+    reference's host products stay within seconds."""
+    out = set()
+    for kind, cap in ((0, mpn_cap), (1, fmpz_cap)):
+        idx = [k for k, r in enumerate(reqs) if r[0] == kind]
+        size = (lambda r: r[1] + r[2]) if kind == 0 else (lambda r: (r[1] + r[2]) * (r[3] + r[4]))
+        idx = sorted((k for k in idx if size(reqs[k]) <= cap), key=lambda k: size(reqs[k]))
+        if idx:
+            step = max(1, len(idx) // per_kind)
+            out.update(idx[::step][:per_kind])
+    return out
+
+
 def stream_cpu_check(reqs, kept, seconds):
-    """The reference's own products for a subsample of the stream, timed on
-    the host, each compared limb for limb with the GPU's product."""
+    """The reference's own products for the stream's subsample, timed on the
+    host, each compared limb for limb with the GPU's product."""
     import oracle
     L, kind, nthreads = ref_library()
     if L is None:
         return None
     t0 = time.perf_counter()
-    done, same, t_ref = 0, 0, 0.0
+    done, same, t_ref, bits = 0, 0, 0.0, 0
     for k in sorted(kept):
         if time.perf_counter() - t0 > seconds:
             break
@@ -297,6 +347,7 @@ def stream_cpu_check(reqs, kept, seconds):
             t = time.perf_counter()
             want = oracle.ref_mpn_mul(ops[:an], ops[an:an + bn])
             t_ref += time.perf_counter() - t
+            bits += NS_LIMB_BITS * (an + bn)
         else:
             a, b, z = kept[k]
             _, an, bn, aw, bw = r
@@ -308,9 +359,10 @@ def stream_cpu_check(reqs, kept, seconds):
         done += 1
         same += int(np.array_equal(np.asarray(want).reshape(-1), np.asarray(z).reshape(-1)))
     return {"checked": done, "identical": same, "ref_seconds": t_ref, "cores": min(nthreads, 8),
-            "kind": kind,
-            "sample": "every %d-th request of the stream, reference product vs GPU product" %
-            max(1, len(reqs) // 24)}
+            "kind": kind, **host_info(),
+            "sample": "stratified subsample: up to 24 mpn products (an + bn <= 2^20 limbs) and 24 "
+                      "integer-polynomial products (<= 2^22 coefficient limbs), spread over each "
+                      "kind's size order; reference product vs GPU product, limb for limb"}
 
 
 def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, tun, train_info):
@@ -758,7 +810,8 @@ def main():
                 "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (splitmix64 limbs)",
                 "config": dict(config, parallelism="host threads"),
-                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model",
+                                                    "gmp_version")},
                 "e2e": {"value": cb["value"], "unit": "Gbit/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
@@ -943,7 +996,7 @@ def main():
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline_run(an, bn, steps=2, warmup=1, max_seconds=30.0)
-        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample", "cpu_model", "gmp_version")}
     line = {
         "metric": METRIC, "value": value, "unit": "Gbit/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,

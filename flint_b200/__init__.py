@@ -67,6 +67,15 @@ class MulReq(ctypes.Structure):
                 ("b", ctypes.c_void_p), ("bn", ctypes.c_ulong)]
 
 
+class FmpzMulReq(ctypes.Structure):
+    """gpu_fmpz_mul_req: one integer-polynomial window product of a list
+    (device pointers; raw two's complement coefficient rows)."""
+    _fields_ = [("z", ctypes.c_void_p), ("zw", ctypes.c_ulong), ("zl", ctypes.c_ulong),
+                ("zh", ctypes.c_ulong), ("a", ctypes.c_void_p), ("aw", ctypes.c_ulong),
+                ("an", ctypes.c_ulong), ("b", ctypes.c_void_p), ("bw", ctypes.c_ulong),
+                ("bn", ctypes.c_ulong)]
+
+
 class MulConfig(ctypes.Structure):
     """gpu_mul_config: route, prime count, log2 transform length, log2 row length."""
     _fields_ = [("route", ctypes.c_int), ("np", ctypes.c_int), ("logM", ctypes.c_int),
@@ -157,6 +166,7 @@ SIGNATURES = {
     "gpu_fmpz_poly_mul_config_resolve": (ctypes.c_int, [_U, _U, _U, _U, ctypes.POINTER(MulConfig)]),
     "gpu_fmpz_poly_mul_mid_device_config": (ctypes.c_int, [_CTX, _P, _U, _U, _U, _P, _U, _U, _P, _U,
                                                            _U, ctypes.POINTER(MulConfig), _P]),
+    "gpu_fmpz_poly_mul_mid_device_list": (ctypes.c_int, [_CTX, _P, ctypes.c_size_t, _P, _P]),
     "gpu_mul_time_config": (ctypes.c_int, [_CTX, ctypes.c_int, _U, _U, _U, _U,
                                            ctypes.POINTER(MulConfig), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double)]),
@@ -450,6 +460,15 @@ class MpnCtx:
         _check(lib().gpu_fmpz_poly_mul_mid_device_config(self.ptr, z_ptr, zw, zl, zh, a_ptr, aw,
                                                          an, b_ptr, bw, bn, ctypes.byref(cfg),
                                                          stream))
+
+    def fmpz_poly_mul_device_list(self, reqs, cfgs=None, stream=None):
+        """Queue a list of integer-polynomial window products (FmpzMulReq,
+        device pointers) with one call; cfgs: None or one MulConfig per
+        request."""
+        n = len(reqs)
+        arr = (FmpzMulReq * n)(*reqs)
+        carr = (MulConfig * n)(*cfgs) if cfgs is not None else None
+        _check(lib().gpu_fmpz_poly_mul_mid_device_list(self.ptr, arr, n, carr, stream))
 
     def time_config(self, kind, an, bn, cfg=None, aw=1, bw=1, reps=3):
         """Median device milliseconds of a product under cfg (autotuner probe)."""

@@ -229,7 +229,13 @@ struct Ctx {
     // the kernels, and events to order the two
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_copy[9] = {nullptr};
+    // configuration timing (autotuner): operand buffer and events kept
+    // between calls, so a timing costs launches only
+    uint64_t *d_time = nullptr;
+    size_t time_cap = 0;                  // bytes
+    cudaEvent_t ev_time[2] = {nullptr, nullptr};
 };
+
 
 static int grow(void **ptr, size_t *cap, size_t need)
 {
@@ -240,6 +246,17 @@ static int grow(void **ptr, size_t *cap, size_t need)
     size_t sz = std::max(need, *cap + *cap / 8);
     CU(cudaMalloc(ptr, sz));
     *cap = sz;
+    return 0;
+}
+
+// the timing buffer (at least `bytes`) and the two timing events
+static int timing_scratch(Ctx *X, size_t bytes, uint64_t **buf)
+{
+    int rc = grow((void **)&X->d_time, &X->time_cap, bytes);
+    if (rc) return rc;
+    for (auto &e : X->ev_time)
+        if (!e) CU(cudaEventCreate(&e));
+    *buf = X->d_time;
     return 0;
 }
 
@@ -616,6 +633,9 @@ static void ctx_destroy(Ctx *X)
     }
     for (auto &e : X->ev_copy)
         if (e) cudaEventDestroy(e);
+    for (auto &e : X->ev_time)
+        if (e) cudaEventDestroy(e);
+    cudaFree(X->d_time);
     delete X;
 }
 
@@ -1584,6 +1604,40 @@ int gpu_fmpz_poly_mul_config_resolve(gpu_ulong an, gpu_ulong aw, gpu_ulong bn, g
     return 0;
 }
 
+int gpu_fmpz_poly_mul_mid_device_list(gpu_mpn_ctx_t R, const gpu_fmpz_mul_req *reqs, size_t n,
+                                      const gpu_mul_config *cfgs, void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (n && !reqs) return set_error(GPU_FFT_SMALL_EINVAL, "null request list");
+    size_t need = 0;
+    for (size_t i = 0; i < n; i++) {
+        const gpu_fmpz_mul_req &q = reqs[i];
+        int rc = fmpz_check_args(q.zw, q.aw, q.an, q.bw, q.bn);
+        if (!rc && (q.zl >= q.zh || q.zh > q.an + q.bn - 1))
+            rc = set_error(GPU_FFT_SMALL_EINVAL, "window must lie inside the product");
+        FmpzPlan P;
+        if (!rc) rc = plan_fmpz_cfg(q.an, q.aw, q.bn, q.bw, cfgs ? &cfgs[i] : nullptr, &P);
+        if (rc) {
+            const std::string msg = g_last_error;
+            return set_error(rc, "request %zu: %s", i, msg.c_str());
+        }
+        const bool sq = (q.a == q.b) && (q.an == q.bn) && (q.aw == q.bw);
+        need = std::max(need, (sq ? 1 : 2) * (size_t)P.np * ((size_t)1 << P.logM) * sizeof(uint32_t));
+    }
+    int rc = bind_device(X);
+    if (rc) return rc;
+    rc = grow((void **)&X->d_res, &X->res_cap, need);
+    if (rc) return rc;
+    for (size_t i = 0; i < n; i++) {
+        const gpu_fmpz_mul_req &q = reqs[i];
+        rc = fmpz_mul_mid_enqueue(X, q.z, q.zw, q.zl, q.zh, q.a, q.aw, q.an, q.b, q.bw, q.bn,
+                                  (cudaStream_t)stream, cfgs ? &cfgs[i] : nullptr);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
 int gpu_fmpz_poly_mul_mid_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, gpu_ulong zw, gpu_ulong zl,
                                         gpu_ulong zh, const uint64_t *a_dev, gpu_ulong aw, gpu_ulong an,
                                         const uint64_t *b_dev, gpu_ulong bw, gpu_ulong bn,
@@ -1713,7 +1767,8 @@ int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw, g
     const uint64_t zn = an + bn, zw = kind == 0 ? 1 : aw + bw + 1;
     const size_t na = an * aw, nb = bn * bw, nz = zn * zw;
     uint64_t *buf = nullptr;
-    CU(cudaMalloc(&buf, (na + nb + nz) * sizeof(uint64_t)));
+    rc = timing_scratch(X, (na + nb + nz) * sizeof(uint64_t), &buf);
+    if (rc) return rc;
     uint64_t *da = buf, *db = buf + na, *dz = buf + na + nb;
     cudaStream_t st = X->stream;
     k_fill_limbs<<<X->nsm * 4, 256, 0, st>>>(da, na, 0x1234567ull + an);
@@ -1723,10 +1778,8 @@ int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw, g
                          : fmpz_mul_mid_enqueue(X, dz, zw, 0, an + bn - 1, da, aw, an, db, bw, bn, st, cfg);
     };
     std::vector<float> t(reps);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = X->ev_time[0], e1 = X->ev_time[1];
     rc = call();   // warm-up (allocations, first launch)
-    if (!rc && cudaEventCreate(&e0) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
-    if (!rc && cudaEventCreate(&e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
     for (int r = 0; r < reps && !rc; r++) {
         cudaEventRecord(e0, st);
         rc = call();
@@ -1735,10 +1788,7 @@ int gpu_mul_time_config(gpu_mpn_ctx_t R, int kind, gpu_ulong an, gpu_ulong aw, g
         if (!rc) cudaEventElapsedTime(&t[r], e0, e1);
     }
     if (!rc) rc = check_device_error(X);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
     cudaStreamSynchronize(st);
-    cudaFree(buf);
     if (rc) return rc;
     std::sort(t.begin(), t.end());
     *ms = t[reps / 2];
@@ -1758,7 +1808,8 @@ int gpu_mpn_mul_time_batched(gpu_mpn_ctx_t R, gpu_ulong an, gpu_ulong bn, const 
     if (rc) return rc;
     const size_t per = an + bn + (an + bn);
     uint64_t *buf = nullptr;
-    CU(cudaMalloc(&buf, per * copies * sizeof(uint64_t)));
+    rc = timing_scratch(X, per * copies * sizeof(uint64_t), &buf);
+    if (rc) return rc;
     cudaStream_t st = X->stream;
     std::vector<gpu_mpn_mul_req> reqs(copies);
     std::vector<gpu_mul_config> cfgs(copies, cfg ? *cfg : gpu_mul_config{0, 0, 0, 0});
@@ -1772,10 +1823,8 @@ int gpu_mpn_mul_time_batched(gpu_mpn_ctx_t R, gpu_ulong an, gpu_ulong bn, const 
     gpu_mpn_batch_options opt = {0, 4, 1};
     rc = batch_plan(B, reqs.data(), cfgs.data(), copies, &opt);
     std::vector<float> t(reps);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = X->ev_time[0], e1 = X->ev_time[1];
     if (!rc) rc = batch_run(B, st);   // warm-up and graph capture
-    if (!rc && cudaEventCreate(&e0) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
-    if (!rc && cudaEventCreate(&e1) != cudaSuccess) rc = set_error(GPU_FFT_SMALL_ECUDA, "cudaEventCreate");
     for (int r = 0; r < reps && !rc; r++) {
         cudaEventRecord(e0, st);
         rc = batch_run(B, st);
@@ -1784,11 +1833,8 @@ int gpu_mpn_mul_time_batched(gpu_mpn_ctx_t R, gpu_ulong an, gpu_ulong bn, const 
         if (!rc) cudaEventElapsedTime(&t[r], e0, e1);
     }
     if (!rc) rc = check_device_error(X);
-    if (e0) cudaEventDestroy(e0);
-    if (e1) cudaEventDestroy(e1);
     cudaStreamSynchronize(st);
     batch_destroy(B);
-    cudaFree(buf);
     if (rc) return rc;
     std::sort(t.begin(), t.end());
     *ms_per_product = t[reps / 2] / copies;

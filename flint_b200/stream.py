@@ -8,55 +8,79 @@ the configuration a chooser gives it:
 * mpn requests go in chunks (at most ``chunk_limbs`` operand limbs each) into
   planned batches (gpu_mpn_batch_init_config), so products that share a
   configuration share launches;
-* integer-polynomial requests run one device call each
-  (gpu_fmpz_poly_mul_mid_device_config).
+* integer-polynomial requests go in chunks through one list call each
+  (gpu_fmpz_poly_mul_mid_device_list): every product of a chunk is queued by
+  native code on one stream, with the scratch sized before the timing.
 
 Operands are generated on the device from a seed (torch's CUDA generator),
 outside the timed region; the device time of the products is measured with
-CUDA events on the launching stream.  ``outputs`` lets a caller keep or
-compare the products (e.g. a learned schedule against the fixed rule: the
-products must be identical).
+CUDA events on the launching stream.  Every product also gets a 64-bit
+digest (a weighted sum of its limbs with fixed pseudo-random weights,
+computed on the device), so two runs under different schedules can be
+compared product by product without copying them to the host; ``keep`` lets
+a caller copy selected products (with their operands) to the host.
 """
 import numpy as np
 
-from . import MpnBatch
+from . import FmpzMulReq, MpnBatch
 
 
-def _fill_fmpz(torch, n, w, bits, gen, dev):
-    """n coefficients of w limbs, uniform in (-2^bits, 2^bits), two's complement."""
-    x = torch.randint(-(1 << 63), (1 << 63) - 1, (n, w), dtype=torch.int64, device=dev, generator=gen)
-    t = bits - 64 * (w - 1) + 1            # significant bits of the top limb, sign included
-    x[:, -1] = x[:, -1] >> (64 - t) if t < 64 else x[:, -1]
-    return x
+def _weights(torch, n, dev):
+    """Fixed pseudo-random int64 weights for product digests."""
+    g = torch.Generator(device=dev)
+    g.manual_seed(0x5EED)
+    return torch.randint(-(1 << 63), (1 << 63) - 1, (n,), dtype=torch.int64, device=dev, generator=g)
 
 
-def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 26, keep=None,
-               check_against=None):
+def _digests(torch, out, starts, lens, weights):
+    """Per-product digests sum_i out[s + i] * weights[i] (mod 2^64) for the
+    products at out[starts[k] : starts[k] + lens[k]]."""
+    dev = out.device
+    st = torch.tensor(starts, dtype=torch.int64, device=dev)
+    ln = torch.tensor(lens, dtype=torch.int64, device=dev)
+    # position of every limb inside its product
+    owner = torch.repeat_interleave(torch.arange(len(starts), device=dev), ln)
+    local = torch.arange(out.numel(), device=dev) - torch.repeat_interleave(st, ln)
+    prod = out[:owner.numel()] * weights[local]
+    d = torch.zeros(len(starts), dtype=torch.int64, device=dev)
+    d.index_add_(0, owner, prod)
+    return d
+
+
+def _chunks(idx, size_of, limit):
+    out, cur, size = [], [], 0
+    for k in idx:
+        n = size_of(k)
+        if cur and size + n > limit:
+            out.append(cur)
+            cur, size = [], 0
+        cur.append(k)
+        size += n
+    if cur:
+        out.append(cur)
+    return out
+
+
+def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27, keep=None):
     """Execute reqs under configs (one per request).  Returns a dict of device
-    milliseconds (mpn, fmpz, total), limbs/bits processed, and, when
-    check_against is another config list, whether every product equals the
-    product under those configurations.  keep: optional set of request
-    indices whose products are returned (host arrays) in 'kept'."""
+    milliseconds (mpn, fmpz, total), limbs processed, a per-request digest
+    array ('digests', int64, in request order) and, for the request indices
+    in `keep`, host copies of operands and products in 'kept'."""
     gen = torch.Generator(device=dev)
     s = stream.cuda_stream
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     res = {"mpn_ms": 0.0, "fmpz_ms": 0.0, "mpn_limbs": 0, "fmpz_coeff_limbs": 0,
-           "mpn_requests": 0, "fmpz_requests": 0, "identical": True, "kept": {}}
+           "mpn_requests": 0, "fmpz_requests": 0, "kept": {}}
+    digests = np.zeros(len(reqs), dtype=np.int64)
     mpn = [k for k, r in enumerate(reqs) if r[0] == 0]
     fz = [k for k, r in enumerate(reqs) if r[0] == 1]
-    # mpn requests: chunks of bounded operand size
-    chunks, cur, size = [], [], 0
-    for k in mpn:
-        n = reqs[k][1] + reqs[k][2]
-        if cur and size + n > chunk_limbs:
-            chunks.append(cur)
-            cur, size = [], 0
-        cur.append(k)
-        size += n
-    if cur:
-        chunks.append(cur)
-    for ci, idx in enumerate(chunks):
+    wmax = 1
+    for r in reqs:
+        wmax = max(wmax, r[1] + r[2] if r[0] == 0 else (r[1] + r[2] - 1) * (r[3] + r[4] + 1))
+    weights = _weights(torch, wmax, dev)
+
+    for ci, idx in enumerate(_chunks(mpn, lambda k: reqs[k][1] + reqs[k][2], chunk_limbs)):
         tot = sum(reqs[k][1] + reqs[k][2] for k in idx)
         gen.manual_seed(seed * 1000003 + ci)
         d_in = torch.randint(-(1 << 63), (1 << 63) - 1, (tot,), dtype=torch.int64, device=dev,
@@ -77,13 +101,8 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 26
             ev1.record(stream)
             B.check(s)
             res["mpn_ms"] += ev0.elapsed_time(ev1)
-        if check_against is not None:
-            d_ref = torch.empty_like(d_out)
-            rq2 = [(d_ref.data_ptr() + 8 * o, a, an, b, bn) for o, (_, a, an, b, bn) in zip(offs, rq)]
-            with MpnBatch(ctx, rq2, configs=[check_against[k] for k in idx]) as B2:
-                B2.run(s)
-                B2.check(s)
-            res["identical"] &= bool(torch.equal(d_out, d_ref))
+        dg = _digests(torch, d_out, offs, [reqs[k][1] + reqs[k][2] for k in idx], weights)
+        digests[idx] = dg.cpu().numpy()
         if keep:
             for k, o in zip(idx, offs):
                 if k in keep:
@@ -92,36 +111,63 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 26
                                       d_out[o:o + an + bn].cpu().numpy().view(np.uint64).copy())
         res["mpn_limbs"] += tot
         res["mpn_requests"] += len(idx)
-    # integer-polynomial requests, one call each
-    for k in fz:
-        _, an, bn, aw, bw = reqs[k]
-        bits = 64 * aw - 1
-        gen.manual_seed(seed * 1000003 + 7919 * (k + 1))
-        a = _fill_fmpz(torch, an, aw, bits, gen, dev)
-        b = _fill_fmpz(torch, bn, bw, bits, gen, dev)
-        zw = aw + bw + 1
-        zn = an + bn - 1
-        z = torch.empty((zn, zw), dtype=torch.int64, device=dev)
-        ctx.fmpz_poly_mul_device_config(z.data_ptr(), zw, 0, zn, a.data_ptr(), aw, an, b.data_ptr(),
-                                        bw, bn, configs[k], s)    # warm-up (scratch growth)
+
+    if fz:
+        # size the context's scratch for the stream's largest integer-polynomial
+        # product outside the timing (one untimed product)
+        big = max(fz, key=lambda k: (reqs[k][1] + reqs[k][2] - 1) * (reqs[k][3] + reqs[k][4] - 1))
+        _, an, bn, aw, bw = reqs[big]
+        ta = torch.zeros(an * aw + bn * bw, dtype=torch.int64, device=dev)
+        tz = torch.empty((an + bn - 1) * (aw + bw + 1), dtype=torch.int64, device=dev)
+        ctx.fmpz_poly_mul_device_list(
+            [FmpzMulReq(tz.data_ptr(), aw + bw + 1, 0, an + bn - 1, ta.data_ptr(), aw, an,
+                        ta.data_ptr() + 8 * an * aw, bw, bn)], [configs[big]], s)
         stream.synchronize()
+        del ta, tz
+
+    def fz_size(k):
+        _, an, bn, aw, bw = reqs[k]
+        return an * aw + bn * bw + (an + bn - 1) * (aw + bw + 1)
+
+    for ci, idx in enumerate(_chunks(fz, fz_size, chunk_limbs)):
+        tin = sum(reqs[k][1] * reqs[k][3] + reqs[k][2] * reqs[k][4] for k in idx)
+        tout = sum((reqs[k][1] + reqs[k][2] - 1) * (reqs[k][3] + reqs[k][4] + 1) for k in idx)
+        gen.manual_seed(seed * 1000003 + 500009 + ci)
+        # coefficients of w limbs uniform in (-2^(64w-1), 2^(64w-1)): bits = 64w - 1
+        d_in = torch.randint(-(1 << 63), (1 << 63) - 1, (tin,), dtype=torch.int64, device=dev,
+                             generator=gen)
+        d_out = torch.empty(tout, dtype=torch.int64, device=dev)
+        lst, ins, outs, zlens = [], [], [], []
+        oi = oo = 0
+        for k in idx:
+            _, an, bn, aw, bw = reqs[k]
+            zw, zn = aw + bw + 1, an + bn - 1
+            pa = d_in.data_ptr() + 8 * oi
+            lst.append(FmpzMulReq(d_out.data_ptr() + 8 * oo, zw, 0, zn, pa, aw, an,
+                                  pa + 8 * an * aw, bw, bn))
+            ins.append(oi)
+            outs.append(oo)
+            zlens.append(zn * zw)
+            oi += an * aw + bn * bw
+            oo += zn * zw
         ev0.record(stream)
-        ctx.fmpz_poly_mul_device_config(z.data_ptr(), zw, 0, zn, a.data_ptr(), aw, an, b.data_ptr(),
-                                        bw, bn, configs[k], s)
+        ctx.fmpz_poly_mul_device_list(lst, [configs[k] for k in idx], s)
         ev1.record(stream)
         ev1.synchronize()
         res["fmpz_ms"] += ev0.elapsed_time(ev1)
-        if check_against is not None:
-            z2 = torch.empty_like(z)
-            ctx.fmpz_poly_mul_device_config(z2.data_ptr(), zw, 0, zn, a.data_ptr(), aw, an,
-                                            b.data_ptr(), bw, bn, check_against[k], s)
-            stream.synchronize()
-            res["identical"] &= bool(torch.equal(z, z2))
-        if keep and k in keep:
-            res["kept"][k] = (a.cpu().numpy().view(np.uint64).copy(),
-                              b.cpu().numpy().view(np.uint64).copy(),
-                              z.cpu().numpy().view(np.uint64).copy())
-        res["fmpz_coeff_limbs"] += an * aw + bn * bw
-        res["fmpz_requests"] += 1
+        dg = _digests(torch, d_out, outs, zlens, weights)
+        digests[idx] = dg.cpu().numpy()
+        if keep:
+            for k, i0, o0 in zip(idx, ins, outs):
+                if k in keep:
+                    _, an, bn, aw, bw = reqs[k]
+                    zw, zn = aw + bw + 1, an + bn - 1
+                    res["kept"][k] = (
+                        d_in[i0:i0 + an * aw].cpu().numpy().view(np.uint64).copy(),
+                        d_in[i0 + an * aw:i0 + an * aw + bn * bw].cpu().numpy().view(np.uint64).copy(),
+                        d_out[o0:o0 + zn * zw].cpu().numpy().view(np.uint64).copy())
+        res["fmpz_coeff_limbs"] += tin
+        res["fmpz_requests"] += len(idx)
     res["total_ms"] = res["mpn_ms"] + res["fmpz_ms"]
+    res["digests"] = digests
     return res

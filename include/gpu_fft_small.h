@@ -409,6 +409,29 @@ GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device_config(gpu_mpn_ctx_t R, uint6
                                                           gpu_ulong bw, gpu_ulong bn,
                                                           const gpu_mul_config *cfg, void *stream);
 
+/* A list of integer-polynomial products queued by one call (no counterpart
+   in the reference, whose callers multiply one polynomial pair per
+   _fmpz_poly_mul call, src/fmpz_poly/mul.c:100-186): coefficients [zl, zh)
+   of a * b into z (zh - zl rows of zw limbs), raw two's complement rows as
+   for gpu_fmpz_poly_mul_mid_device_config, all device pointers.  Every
+   request is planned first (any invalid one fails the call before anything
+   is queued; the message names its index), the context's scratch is sized
+   once for the largest, and the products are queued in order on `stream`
+   without a host synchronisation.  cfgs: NULL or one configuration per
+   request.  Requests run one after another on the stream, so they may share
+   operands but must not write overlapping z. */
+typedef struct {
+    uint64_t *z;
+    gpu_ulong zw, zl, zh;
+    const uint64_t *a;
+    gpu_ulong aw, an;
+    const uint64_t *b;
+    gpu_ulong bw, bn;
+} gpu_fmpz_mul_req;
+GPU_FFT_SMALL_API int gpu_fmpz_poly_mul_mid_device_list(gpu_mpn_ctx_t R, const gpu_fmpz_mul_req *reqs,
+                                                        size_t n, const gpu_mul_config *cfgs,
+                                                        void *stream);
+
 /* Test hooks for the failure paths of the bounded device waits, which valid
    inputs do not reach (no counterpart in the reference).
    gpu_test_crt_lookback_timeout runs one CRT/carry tile whose carry

@@ -22,7 +22,7 @@ no ``gmp.h``), so this recipe
 
 Nothing is written outside ``oracle/_ref``.  Usage::
 
-    python oracle/build_ref.py [--ref /root/reference] [-j 8]
+    python oracle/build_ref.py [--ref DIR] [-j 8]   (DIR defaults to $FLINT_REFERENCE or /root/reference)
 """
 import argparse
 import os
@@ -231,7 +231,10 @@ REQUIRED = ["mpn_ctx_init", "mpn_ctx_clear", "mpn_ctx_mpn_mul",
             "sd_fft_trunc", "sd_ifft_trunc", "sd_fft_ctx_init_prime"]
 
 
-def build(ref="/root/reference", jobs=None, quiet=False):
+DEFAULT_REF = os.environ.get("FLINT_REFERENCE", "/root/reference")
+
+
+def build(ref=DEFAULT_REF, jobs=None, quiet=False):
     lib = os.path.join(OUT, "libflint_ref.so")
     if not os.path.isdir(os.path.join(ref, "src", "fft_small")):
         raise SystemExit("reference tree not found at %s" % ref)
@@ -273,7 +276,7 @@ def build(ref="/root/reference", jobs=None, quiet=False):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=DEFAULT_REF)
     ap.add_argument("-j", type=int, default=None)
     a = ap.parse_args()
     build(a.ref, a.j)
