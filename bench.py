@@ -275,11 +275,11 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
     t_choose = time.perf_counter() - t0
     default = [tuner.default_config(r) for r in reqs]
     keep = stream_subsample(reqs)
-    t0 = time.perf_counter()
+    w0 = time.perf_counter()
     rl = run_stream(ctx, torch, reqs, learned, 17, stream, dev, keep=keep)
-    t1 = time.perf_counter()
+    w1 = time.perf_counter()
     rd = run_stream(ctx, torch, reqs, default, 17, stream, dev)
-    t2 = time.perf_counter()
+    w2 = time.perf_counter()
     same = rl["digests"] == rd["digests"]
     held = request_stream(STREAM_SEED + 2, n_held)
     t0 = time.perf_counter()
@@ -299,7 +299,7 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
         "default_rule": {"total_ms": rd["total_ms"], "mpn_ms": rd["mpn_ms"], "fmpz_ms": rd["fmpz_ms"],
                          "mpn_Gbit_s": bits_mpn / rd["mpn_ms"] / 1e6},
         "gain_over_default_rule": rd["total_ms"] / rl["total_ms"],
-        "choose_s": t_choose, "wall_s": {"learned_run": t1 - t0, "default_run": t2 - t1},
+        "choose_s": t_choose, "wall_s": {"learned_run": w1 - w0, "default_run": w2 - w1},
         "routes": {"transform": sum(c.route == 0 for c in learned),
                    "basecase": sum(c.route == 1 for c in learned)},
         "identical_to_default_rule": bool(same.all()),
@@ -386,13 +386,26 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
     delta = d_ref.data_ptr() - d_out.data_ptr()
     s = stream.cuda_stream
 
-    def per_instance():
+    def per_instance_python():
         for (z, a, an, b, bn) in reqs:
             ctx.mpn_mul_device(z + delta, a, an, b, bn, s)
+
+    # the per-instance path without the interpreter: one native call queues
+    # every product as gpu_mpn_mul_device would (gpu_mpn_mul_device_list)
+    list_reqs = [FB.MulReq(z + delta, a, an, b, bn) for (z, a, an, b, bn) in reqs]
+
+    def per_instance():
+        ctx.mpn_mul_device_list(list_reqs, None, s)
 
     bits = NS_LIMB_BITS * total
     k_plain = max(2, steps // 3)
     ms_plain = time_on_stream(torch, stream, per_instance, k_plain, 3)
+    stream.synchronize()
+    t0 = time.perf_counter()
+    per_instance()
+    host_issue_ms = (time.perf_counter() - t0) * 1e3
+    stream.synchronize()
+    ms_plain_py = time_on_stream(torch, stream, per_instance_python, max(2, k_plain // 2), 1)
     B0 = FB.MpnBatch(ctx, reqs)
     ms_default = time_on_stream(torch, stream, lambda: B0.run(s), steps, warmup)
     B0.check(s)
@@ -481,7 +494,12 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
         "schedule": "learned (cost model per request, batched by configuration)",
         "value": bits / ms_batch / 1e6, "unit": "Gbit/s", "ms_per_step": ms_batch,
         "per_instance": {"value": bits / ms_plain / 1e6, "ms_per_step": ms_plain,
-                         "launches_per_step": 4 * BATCH_N},
+                         "launches_per_step": 4 * BATCH_N,
+                         "api": "gpu_mpn_mul_device_list: one native call queues the products one by "
+                                "one, as gpu_mpn_mul_device runs them",
+                         "host_issue_ms_per_step": host_issue_ms},
+        "per_instance_python_loop": {"value": bits / ms_plain_py / 1e6, "ms_per_step": ms_plain_py,
+                                     "api": "gpu_mpn_mul_device called from a Python loop"},
         "plain_batched": {"value": bits / ms_default / 1e6, "ms_per_step": ms_default,
                           "schedule": "default configuration for every request"},
         "speedup_vs_per_instance": ms_plain / ms_batch,
@@ -527,8 +545,9 @@ def batch_cpu_baseline(sizes, host, spans, seconds):
 
 
 def bench_configs(torch, FB, ctx, dev, stream, steps, cpu):
-    """The other measured configurations: 2^16 x 2^16 and 2^24 x 2^20 limbs
-    (mpn_mul), and the nmod window product (coefficients [2^19, 3 2^19) of
+    """The other measured configurations: 2^16 x 2^16, 2^24 x 2^20 and
+    3 2^22 x 3 2^22 limbs (mpn_mul; the last on a 3 2^23-point transform), and
+    the nmod window product (coefficients [2^19, 3 2^19) of
     two 2^20-coefficient polynomials mod an odd n in [2^61, 2^62)), each
     device-resident (CUDA events) against its algorithmic byte model, with
     the compiled reference timed on the host and its output compared."""
@@ -548,7 +567,9 @@ def bench_configs(torch, FB, ctx, dev, stream, steps, cpu):
         return statistics.median(ts), r
 
     for name, an, bn, seed in [("1: mpn_mul 2^16 x 2^16", 1 << 16, 1 << 16, 11),
-                               ("2b: mpn_mul 2^24 x 2^20", 1 << 24, 1 << 20, 12)]:
+                               ("2b: mpn_mul 2^24 x 2^20", 1 << 24, 1 << 20, 12),
+                               ("2c: mpn_mul 3 2^22 x 3 2^22 (a 3 2^23-point truncated transform)",
+                                3 << 22, 3 << 22, 13)]:
         a, b = splitmix_limbs(seed, an), splitmix_limbs(seed + 1, bn)
         da = torch.from_numpy(a.view(np.int64)).to(dev)
         db = torch.from_numpy(b.view(np.int64)).to(dev)
@@ -559,6 +580,7 @@ def bench_configs(torch, FB, ctx, dev, stream, steps, cpu):
         z = dz.cpu().numpy().view(np.uint64)
         alg = 208 * (an + bn)
         r = {"workload": name, "ms": ms, "value": NS_LIMB_BITS * (an + bn) / ms / 1e6, "unit": "Gbit/s",
+             "transform_points": FB.mpn_mul_transform_points(an, bn),
              "roofline": {"bound": "hbm", "alg_bytes": alg, "achieved": alg / ms / 1e6, "peak": peak,
                           "frac": alg / ms / 1e6 / peak}}
         if L is not None:

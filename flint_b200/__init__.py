@@ -167,6 +167,7 @@ SIGNATURES = {
     "gpu_fmpz_poly_mul_mid_device_config": (ctypes.c_int, [_CTX, _P, _U, _U, _U, _P, _U, _U, _P, _U,
                                                            _U, ctypes.POINTER(MulConfig), _P]),
     "gpu_fmpz_poly_mul_mid_device_list": (ctypes.c_int, [_CTX, _P, ctypes.c_size_t, _P, _P]),
+    "gpu_mpn_mul_device_list": (ctypes.c_int, [_CTX, _P, ctypes.c_size_t, _P, _P]),
     "gpu_mul_time_config": (ctypes.c_int, [_CTX, ctypes.c_int, _U, _U, _U, _U,
                                            ctypes.POINTER(MulConfig), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double)]),
@@ -216,6 +217,7 @@ SIGNATURES = {
     "gpu_mpn_mul_plan": (ctypes.c_int, [_U, _U, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_int)]),
     "gpu_mpn_mul_split_plan": (ctypes.c_int, [_U, _U, ctypes.POINTER(ctypes.c_int)]),
+    "gpu_mpn_mul_transform_points": (ctypes.c_int, [_U, _U, ctypes.c_int, ctypes.POINTER(_U)]),
     "gpu_fft_small_prime": (_U, [ctypes.c_int]),
     "gpu_mpn_ctx_last_launches": (ctypes.c_int, [_CTX]),
     "gpu_mpn_ctx_set_timing": (ctypes.c_int, [_CTX, ctypes.c_int]),
@@ -266,6 +268,15 @@ def mpn_mul_split_plan(an, bn):
     lc = ctypes.c_int()
     _check(lib().gpu_mpn_mul_split_plan(an, bn, ctypes.byref(lc)))
     return lc.value
+
+
+def mpn_mul_transform_points(an, bn, square=False):
+    """Points of the cyclic transform a whole an x bn product runs under the
+    default plan (2^logM, 3 2^(logM-2), a split chunk's length, or 0 for the
+    basecase route)."""
+    v = _U()
+    _check(lib().gpu_mpn_mul_transform_points(an, bn, 1 if square else 0, ctypes.byref(v)))
+    return v.value
 
 
 def prime(i):
@@ -460,6 +471,14 @@ class MpnCtx:
         _check(lib().gpu_fmpz_poly_mul_mid_device_config(self.ptr, z_ptr, zw, zl, zh, a_ptr, aw,
                                                          an, b_ptr, bw, bn, ctypes.byref(cfg),
                                                          stream))
+
+    def mpn_mul_device_list(self, reqs, cfgs=None, stream=None):
+        """Queue a list of whole products (MulReq or (z, a, an, b, bn) tuples of
+        device pointers) with one call, each as mpn_mul_device would run it."""
+        n = len(reqs)
+        arr = (MulReq * n)(*[r if isinstance(r, MulReq) else MulReq(*r) for r in reqs])
+        carr = (MulConfig * n)(*cfgs) if cfgs is not None else None
+        _check(lib().gpu_mpn_mul_device_list(self.ptr, arr, n, carr, stream))
 
     def fmpz_poly_mul_device_list(self, reqs, cfgs=None, stream=None):
         """Queue a list of integer-polynomial window products (FmpzMulReq,

@@ -11,6 +11,7 @@
 #include "mlp_kernels.cuh"
 #include "op_kernels.cuh"
 #include "neg_kernels.cuh"
+#include "mpn3_kernels.cuh"
 
 #include <cuda_runtime.h>
 #include <math.h>
@@ -315,6 +316,47 @@ static int ctx_build_tables(Ctx *X)
             }
         }
     }
+    // tables of the 3 2^k-point transforms (first NP3 primes): twist powers
+    // of w3 of order 3 2^25, radix-3 stage twiddles omega^(+-e) / 2 with omega
+    // of order 3 2^11, and the stage constants w - w^2, w^-1 - w^-2 (w of
+    // order 3)
+    const size_t n_th3 = (size_t)NP3 * TH3_SZ, n_tl3 = (size_t)NP3 * TL_SZ, n_tw3 = (size_t)NP3 * TW3_SZ;
+    std::vector<uint2> th3(n_th3), tl3(n_tl3), th3i(n_th3), tl3i(n_tl3), tw3f(n_tw3), tw3i(n_tw3),
+        w3c((size_t)NP3 * 2);
+    for (int j = 0; j < NP3; j++) {
+        const uint32_t p = PRIMES[j];
+        const uint32_t w3 = h_powmod(primitive_root(p), (p - 1) / (3u << LOG_MAXM), p);
+        const uint32_t w3i = h_invmod(w3, p);
+        const uint32_t inv2 = (p + 1) / 2;
+        uint32_t x = 1, xi = 1;
+        const uint32_t st = h_powmod(w3, 1u << 13, p), sti = h_powmod(w3i, 1u << 13, p);
+        for (int t = 0; t < TH3_SZ; t++) {
+            th3[(size_t)j * TH3_SZ + t] = shoup_pair(x, p);
+            th3i[(size_t)j * TH3_SZ + t] = shoup_pair(xi, p);
+            x = h_mulmod(x, st, p);
+            xi = h_mulmod(xi, sti, p);
+        }
+        x = 1; xi = 1;
+        for (int t = 0; t < TL_SZ; t++) {
+            tl3[(size_t)j * TL_SZ + t] = shoup_pair(x, p);
+            tl3i[(size_t)j * TL_SZ + t] = shoup_pair(xi, p);
+            x = h_mulmod(x, w3, p);
+            xi = h_mulmod(xi, w3i, p);
+        }
+        const uint32_t om = h_powmod(w3, 1u << (LOG_MAXM - LOG_R3), p), omi = h_invmod(om, p);
+        x = inv2; xi = inv2;
+        for (int e = 0; e < TW3_SZ; e++) {
+            tw3f[(size_t)j * TW3_SZ + e] = shoup_pair(x, p);
+            tw3i[(size_t)j * TW3_SZ + e] = shoup_pair(xi, p);
+            x = h_mulmod(x, om, p);
+            xi = h_mulmod(xi, omi, p);
+        }
+        const uint32_t w = h_powmod(w3, 1u << LOG_MAXM, p), wi = h_invmod(w, p);
+        const uint32_t c = (uint32_t)(((uint64_t)w + p - h_mulmod(w, w, p)) % p);
+        const uint32_t ci = (uint32_t)(((uint64_t)wi + p - h_mulmod(wi, wi, p)) % p);
+        w3c[(size_t)j * 2] = shoup_pair(c, p);
+        w3c[(size_t)j * 2 + 1] = shoup_pair(ci, p);
+    }
     // CRT constants for every prime count
     for (int np = 1; np <= MAX_NP; np++) {
         CrtConst &K = X->crt[np];
@@ -337,6 +379,10 @@ static int ctx_build_tables(Ctx *X)
     const size_t o_twf = place(sizeof(uint2) * n_twf), o_twi = place(sizeof(uint2) * n_twf);
     const size_t o_th = place(sizeof(uint2) * n_th), o_tl = place(sizeof(uint2) * n_tl);
     const size_t o_thi = place(sizeof(uint2) * n_th), o_tli = place(sizeof(uint2) * n_tl);
+    const size_t o_th3 = place(sizeof(uint2) * n_th3), o_tl3 = place(sizeof(uint2) * n_tl3);
+    const size_t o_th3i = place(sizeof(uint2) * n_th3), o_tl3i = place(sizeof(uint2) * n_tl3);
+    const size_t o_tw3f = place(sizeof(uint2) * n_tw3), o_tw3i = place(sizeof(uint2) * n_tw3);
+    const size_t o_w3c = place(sizeof(uint2) * NP3 * 2);
     CU(cudaMalloc(&X->d_tables, off));
     char *base = (char *)X->d_tables;
     CU(cudaMemcpy(base + o_pi, pi.data(), sizeof(PrimeInfo) * MAX_NP, cudaMemcpyHostToDevice));
@@ -346,6 +392,13 @@ static int ctx_build_tables(Ctx *X)
     CU(cudaMemcpy(base + o_tl, tl.data(), sizeof(uint2) * n_tl, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(base + o_thi, thi.data(), sizeof(uint2) * n_th, cudaMemcpyHostToDevice));
     CU(cudaMemcpy(base + o_tli, tli.data(), sizeof(uint2) * n_tl, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_th3, th3.data(), sizeof(uint2) * n_th3, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_tl3, tl3.data(), sizeof(uint2) * n_tl3, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_th3i, th3i.data(), sizeof(uint2) * n_th3, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_tl3i, tl3i.data(), sizeof(uint2) * n_tl3, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_tw3f, tw3f.data(), sizeof(uint2) * n_tw3, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_tw3i, tw3i.data(), sizeof(uint2) * n_tw3, cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(base + o_w3c, w3c.data(), sizeof(uint2) * NP3 * 2, cudaMemcpyHostToDevice));
     X->T.pi = (const PrimeInfo *)(base + o_pi);
     X->T.twf = (const uint2 *)(base + o_twf);
     X->T.twi = (const uint2 *)(base + o_twi);
@@ -353,6 +406,13 @@ static int ctx_build_tables(Ctx *X)
     X->T.tl = (const uint2 *)(base + o_tl);
     X->T.thi = (const uint2 *)(base + o_thi);
     X->T.tli = (const uint2 *)(base + o_tli);
+    X->T.th3 = (const uint2 *)(base + o_th3);
+    X->T.tl3 = (const uint2 *)(base + o_tl3);
+    X->T.th3i = (const uint2 *)(base + o_th3i);
+    X->T.tl3i = (const uint2 *)(base + o_tl3i);
+    X->T.tw3f = (const uint2 *)(base + o_tw3f);
+    X->T.tw3i = (const uint2 *)(base + o_tw3i);
+    X->T.w3c = (const uint2 *)(base + o_w3c);
     // constant memory belongs to the current device's module instance
     CU(device_constants_ensure(X->device));
     CU(cudaDeviceGetAttribute(&X->nsm, cudaDevAttrMultiProcessorCount, X->device));
@@ -394,6 +454,18 @@ static const inv_cols_fn INV_COLS_C13[3] = {k_inv_cols<9, tmpl_cols<9>(), 13>,
 static const fwd_cols_fn FWD_COLS_C14 = k_fwd_cols<11, tmpl_cols<11>(), false, 14>;
 static const fwd_cols_fn FWD_COLS_FZ_C14 = k_fwd_cols<11, tmpl_cols<11>(), true, 14>;
 static const inv_cols_fn INV_COLS_C14 = k_inv_cols<11, tmpl_cols<11>(), 14>;
+
+// columns of 3 2^r points, r = 5 .. 10 (index r - 5)
+typedef void (*fwd_cols3_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t, uint32_t *,
+                             uint32_t *, int, int, const uint32_t *, int);
+typedef void (*inv_cols3_fn)(DevTables, uint32_t *, int, int);
+constexpr int LOG3_RMIN = 5, LOG3_RMAX = 10;
+static const fwd_cols3_fn FWD_COLS3[6] = {
+    k_fwd_cols3<5, cols_per_tile3(5)>, k_fwd_cols3<6, cols_per_tile3(6)>, k_fwd_cols3<7, cols_per_tile3(7)>,
+    k_fwd_cols3<8, cols_per_tile3(8)>, k_fwd_cols3<9, cols_per_tile3(9)>, k_fwd_cols3<10, cols_per_tile3(10)>};
+static const inv_cols3_fn INV_COLS3[6] = {
+    k_inv_cols3<5, cols_per_tile3(5)>, k_inv_cols3<6, cols_per_tile3(6)>, k_inv_cols3<7, cols_per_tile3(7)>,
+    k_inv_cols3<8, cols_per_tile3(8)>, k_inv_cols3<9, cols_per_tile3(9)>, k_inv_cols3<10, cols_per_tile3(10)>};
 
 // the column kernels for a transform shape
 static fwd_cols_fn fwd_cols_kernel(int logR, int logC, bool fz = false)
@@ -522,6 +594,10 @@ static int configure_kernels()
     CU(cudaFuncSetAttribute(FWD_COLS_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     CU(cudaFuncSetAttribute(FWD_COLS_FZ_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     CU(cudaFuncSetAttribute(INV_COLS_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    for (int r = 0; r < 6; r++) {
+        CU(cudaFuncSetAttribute(FWD_COLS3[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(INV_COLS3[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+    }
     for (int c = 5; c <= LOG_MAXC; c++) {
         CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         CU(cudaFuncSetAttribute(ROWS_FWD[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
@@ -547,7 +623,7 @@ static int ctx_create(Ctx **out, gpu_ulong p)
     if (!rc) rc = configure_kernels();
     if (!rc) rc = ctx_build_tables(X);
     if (!rc) {
-        cudaError_t e1 = cudaMalloc(&X->d_scale, sizeof(uint32_t) * (MAX_NP + 1) * (LOG_MAXM + 1) * MAX_NP);
+        cudaError_t e1 = cudaMalloc(&X->d_scale, sizeof(uint32_t) * (MAX_NP + 2) * (LOG_MAXM + 1) * MAX_NP);
         cudaError_t e2 = cudaMalloc(&X->d_err, sizeof(int));
         cudaError_t e3 = cudaMalloc(&X->d_ticket, sizeof(unsigned long long));
         cudaError_t e4 = cudaHostAlloc(&X->h_err, sizeof(int), cudaHostAllocDefault);
@@ -729,6 +805,18 @@ static void fill_scale(const Ctx *X, int np, int logM, uint32_t *scale, int extr
     }
 }
 
+// pointwise scale of a 3 2^k-point transform: (3 2^k)^-1 (P/p_j)^-1 2^128
+static void fill_scale3(const Ctx *X, int np, int k, uint32_t *scale)
+{
+    for (int j = 0; j < np; j++) {
+        const uint32_t p = PRIMES[j];
+        uint32_t s = h_invmod(h_mulmod(3, h_powmod(2, k, p), p), p);
+        s = h_mulmod(s, h_invmod(X->cof_red[np][j], p), p);
+        s = h_mulmod(s, h_powmod(2, 128, p), p);
+        scale[j] = s;
+    }
+}
+
 static int ensure_status(Ctx *X, size_t tiles)
 {
     if (tiles <= X->status_cap) return 0;
@@ -745,14 +833,21 @@ static const uint32_t *scale_ptr(const Ctx *X, int np, int logM)
 {
     return X->d_scale + ((size_t)np * (LOG_MAXM + 1) + logM) * MAX_NP;
 }
+// scales of the 3 2^k-point transforms (NP3 primes), after the 2^logM ones
+static const uint32_t *scale3_ptr(const Ctx *X, int k)
+{
+    return X->d_scale + ((size_t)(MAX_NP + 1) * (LOG_MAXM + 1) + k) * MAX_NP;
+}
 
 // pointwise scales for every (np, logM), uploaded once per context
 static int upload_scales(Ctx *X)
 {
-    std::vector<uint32_t> tab((size_t)(MAX_NP + 1) * (LOG_MAXM + 1) * MAX_NP, 0);
+    std::vector<uint32_t> tab((size_t)(MAX_NP + 2) * (LOG_MAXM + 1) * MAX_NP, 0);
     for (int np = 1; np <= MAX_NP; np++)
         for (int lm = 0; lm <= LOG_MAXM; lm++)
             fill_scale(X, np, lm, &tab[((size_t)np * (LOG_MAXM + 1) + lm) * MAX_NP], 4);
+    for (int k = 0; k <= LOG_MAXM; k++)
+        fill_scale3(X, NP3, k, &tab[((size_t)(MAX_NP + 1) * (LOG_MAXM + 1) + k) * MAX_NP]);
     CU(cudaMemcpy(X->d_scale, tab.data(), tab.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     return 0;
 }
@@ -811,6 +906,42 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
         inv_cols_kernel(S.logR, S.logC)<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
             X->T, ra, S.logC, S.G, desc, co ? *co : ChunkOut{nullptr, 0, 0, 0, 0});
     timing_mark(tr, 3, st);
+}
+
+// Transform of M = 3 2^k points (k - 13 in [LOG3_RMIN, LOG3_RMAX]): columns of
+// 3 2^(k - 13) points with a radix-3 stage, 2^13-point rows; residue planes
+// of 2^logMs words (logMs = k + 2).  The pointwise scale is folded into b's
+// twist as in launch_transforms (squarings keep it in the row pass).
+static void launch_transforms3(const Ctx *X, int k, int logMs, const uint64_t *a, uint64_t an,
+                               const uint64_t *b, uint64_t bn, uint32_t *ra, uint32_t *rb, bool sq,
+                               cudaStream_t st, TimingRecord *tr, cudaEvent_t b_ready)
+{
+    const int np = NP3, r = k - LOGC3;
+    const int G = cols_per_tile3(r);
+    const int C = 1 << LOGC3, rows = 3 << r;
+    const size_t smem = (size_t)(padw(3 * (1 << r) * G) + 32) * sizeof(uint32_t);
+    const uint32_t *sc = scale3_ptr(X, k);
+    if (b_ready) cudaStreamWaitEvent(st, b_ready, 0);
+    FWD_COLS3[r - LOG3_RMIN]<<<dim3(np, C / G, sq ? 1 : 2), 512, smem, st>>>(X->T, a, an, b, bn, ra, rb, logMs, k,
+                                                                             sc, sq ? 0 : 2);
+    timing_mark(tr, 1, st);
+    const LaunchShape L = make_shape(logMs, LOGC3);   // row launch shape (one 2^13-point row per item)
+    const int items = rows * np;
+    ROWS[LOGC3]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
+        X->T, ra, rb, logMs - LOGC3, 1, np, sq ? sc : nullptr, sq ? 1 : 0, nullptr, 1, rows);
+    timing_mark(tr, 2, st);
+    INV_COLS3[r - LOG3_RMIN]<<<dim3(C / G, np), 512, smem, st>>>(X->T, ra, logMs, k);
+    timing_mark(tr, 3, st);
+}
+
+// The 3 2^k-point length for a whole product of L coefficients on the
+// default plan (np primes, 2^logM points), or 0 where the power of two stays
+// (beyond 3 2^(logM - 2), other prime counts, sizes outside the kernels').
+static int three_length(uint64_t L, int np, int logM)
+{
+    const int k = logM - 2;
+    if (np != NP3 || k - LOGC3 < LOG3_RMIN || k - LOGC3 > LOG3_RMAX) return 0;
+    return L <= (3ull << k) ? k : 0;
 }
 
 // Schoolbook route: column sums, then the carry kernel's direct mode.
@@ -985,6 +1116,9 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     // against the short one (split_plan): their residues are summed into
     // one array of the full length, then a single CRT/carry pass follows
     const int Lc = Lover ? Lover : (!cfg && !window && !sq) ? split_plan(an, bn, logM) : 0;
+    // whole products between 2^(logM - 1) and 3 2^(logM - 2) coefficients on
+    // the default plan run a 3 2^(logM - 2)-point transform
+    const int k3 = (!cfg && !window && !Lc) ? three_length(an + bn - 1, np, logM) : 0;
     const size_t Mc = Lc ? (size_t)1 << Lc : 0;
     const size_t res_bytes = Lc ? (size_t)np * (M + 2 * Mc) * sizeof(uint32_t)
                                 : (sq ? 1 : 2) * (size_t)np * M * sizeof(uint32_t);
@@ -1041,6 +1175,8 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
         timing_mark(tr, 1, st);
         timing_mark(tr, 2, st);
         timing_mark(tr, 3, st);
+    } else if (k3) {
+        launch_transforms3(X, k3, logM, a, an, b, bn, ra, rb, sq, st, tr, b_ready);
     } else {
         launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr, nullptr, 1,
                           nullptr, b_ready);
@@ -1435,6 +1571,62 @@ int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev, 
     if (rc) return rc;
     // NULL is CUDA's default stream, as everywhere in the runtime API
     return mpn_mul_enqueue(X, z_dev, a_dev, an, b_dev, bn, (cudaStream_t)stream);
+}
+
+// Scratch a whole product needs on the device (residue bytes, CRT tiles),
+// following mpn_mul_enqueue's plan: split products hold the full residue
+// array plus a chunk pair, the basecase route three 64-bit planes.
+static int mpn_mul_scratch_need(uint64_t an, uint64_t bn, const gpu_mul_config *cfg, bool sq,
+                                size_t *bytes, size_t *tiles)
+{
+    MulPlan P;
+    int Lover = 0;
+    int rc = plan_mpn_cfg(an, bn, cfg, &P);
+    if (rc == GPU_FFT_SMALL_ETOOBIG && !cfg && !sq) rc = plan_mpn_oversize(an, bn, &P, &Lover);
+    if (rc) return rc;
+    const uint64_t zn = an + bn;
+    if (P.route == GPU_MUL_ROUTE_BASECASE) {
+        *bytes = 3 * ((size_t)1 << P.logM) * sizeof(uint64_t);
+        *tiles = (zn + 1023) / 1024;
+        return 0;
+    }
+    const size_t M = (size_t)1 << P.logM;
+    const int Lc = Lover ? Lover : (!cfg && !sq) ? split_plan(an, bn, P.logM) : 0;
+    const size_t Mc = Lc ? (size_t)1 << Lc : 0;
+    *bytes = Lc ? (size_t)P.np * (M + 2 * Mc) * sizeof(uint32_t) : (sq ? 1 : 2) * (size_t)P.np * M * sizeof(uint32_t);
+    *tiles = (zn + CRT_TILE - 1) / CRT_TILE;
+    return 0;
+}
+
+int gpu_mpn_mul_device_list(gpu_mpn_ctx_t R, const gpu_mpn_mul_req *reqs, size_t n,
+                            const gpu_mul_config *cfgs, void *stream)
+{
+    Ctx *X = get_ctx(R);
+    if (!X) return set_error(GPU_FFT_SMALL_EINVAL, "context not initialised");
+    if (n && !reqs) return set_error(GPU_FFT_SMALL_EINVAL, "null request list");
+    size_t bytes = 0, tiles = 0;
+    for (size_t i = 0; i < n; i++) {
+        const gpu_mpn_mul_req &q = reqs[i];
+        size_t b = 0, t = 0;
+        int rc = (!q.z || !q.a || !q.b || q.an == 0 || q.bn == 0)
+                     ? set_error(GPU_FFT_SMALL_EINVAL, "null pointer or empty operand")
+                     : mpn_mul_scratch_need(q.an, q.bn, cfgs ? &cfgs[i] : nullptr, q.a == q.b && q.an == q.bn,
+                                            &b, &t);
+        if (rc) {
+            const std::string msg = g_last_error;
+            return set_error(rc, "request %zu: %s", i, msg.c_str());
+        }
+        bytes = std::max(bytes, b);
+        tiles = std::max(tiles, t);
+    }
+    int rc = bind_device(X);
+    if (!rc) rc = grow((void **)&X->d_res, &X->res_cap, bytes);
+    if (!rc) rc = ensure_status(X, tiles);
+    for (size_t i = 0; i < n && !rc; i++) {
+        const gpu_mpn_mul_req &q = reqs[i];
+        rc = mpn_mul_enqueue(X, q.z, q.a, q.an, q.b, q.bn, (cudaStream_t)stream, cfgs ? &cfgs[i] : nullptr);
+    }
+    return rc;
 }
 
 int gpu_mpn_mul_config_resolve(gpu_ulong an, gpu_ulong bn, gpu_mul_config *cfg)
@@ -1955,6 +2147,28 @@ int gpu_mpn_mul_split_plan(gpu_ulong an, gpu_ulong bn, int *chunk_logM)
     if (rc == GPU_FFT_SMALL_ETOOBIG && an != bn) return plan_mpn_oversize(an, bn, &P, chunk_logM);
     if (rc) return rc;
     *chunk_logM = P.route == GPU_MUL_ROUTE_NTT ? split_plan(an, bn, P.logM) : 0;
+    return 0;
+}
+
+int gpu_mpn_mul_transform_points(gpu_ulong an, gpu_ulong bn, int square, gpu_ulong *points)
+{
+    if (!points) return set_error(GPU_FFT_SMALL_EINVAL, "null output");
+    MulPlan P;
+    int Lover = 0;
+    int rc = plan_mpn(an, bn, &P);
+    if (rc == GPU_FFT_SMALL_ETOOBIG && !square) rc = plan_mpn_oversize(an, bn, &P, &Lover);
+    if (rc) return rc;
+    if (P.route != GPU_MUL_ROUTE_NTT) {
+        *points = 0;
+        return 0;
+    }
+    const int Lc = Lover ? Lover : square ? 0 : split_plan(an, bn, P.logM);
+    if (Lc) {
+        *points = (gpu_ulong)1 << Lc;
+        return 0;
+    }
+    const int k3 = three_length(an + bn - 1, P.np, P.logM);
+    *points = k3 ? (gpu_ulong)3 << k3 : (gpu_ulong)1 << P.logM;
     return 0;
 }
 

@@ -31,6 +31,13 @@ constexpr int TW_SZ = 1 << LOG_MAXC;      // local twiddle table entries per pri
 constexpr int TH_SZ = 1 << (LOG_MAXM - 13);   // twist table: w^(t 2^13), t < 2^12
 constexpr int TL_SZ = 1 << 13;            // twist table: w^t, t < 2^13
 
+// Transforms of 3 2^k points (the first NP3 primes have roots of order
+// 3 2^25): twist powers of w3 (order 3 2^25) and radix-3 stage twiddles
+constexpr int NP3 = 5;
+constexpr int TH3_SZ = 3 << (LOG_MAXM - 13);   // w3^(t 2^13), t < 3 2^12
+constexpr int LOG_R3 = 11;                      // radix-3 stage tables serve columns up to 3 2^11
+constexpr int TW3_SZ = 2 << LOG_R3;             // (omega^e / 2), e < 2^12, omega of order 3 2^11
+
 struct DevTables {
     const PrimeInfo* pi;   // [MAX_NP]
     const uint2* twf;      // [MAX_NP][TW_SZ] forward local twiddles
@@ -39,6 +46,13 @@ struct DevTables {
     const uint2* tl;       // [MAX_NP][TL_SZ] w_{2^25}^t
     const uint2* thi;      // inverses of the above
     const uint2* tli;
+    const uint2* th3;      // [NP3][TH3_SZ] w3^(t 2^13)
+    const uint2* tl3;      // [NP3][TL_SZ] w3^t
+    const uint2* th3i;     // inverses of the above
+    const uint2* tl3i;
+    const uint2* tw3f;     // [NP3][TW3_SZ] omega^e / 2, omega = w3^(2^14) of order 3 2^11
+    const uint2* tw3i;     // [NP3][TW3_SZ] omega^-e / 2
+    const uint2* w3c;      // [NP3][2] (w - w^2, w^-1 - w^-2), w = w3^(2^25) of order 3
 };
 
 // w_M^e * x for e in units of the largest transform (e < 2^25)

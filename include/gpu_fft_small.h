@@ -669,6 +669,16 @@ typedef struct {
     gpu_ulong bn;
 } gpu_mpn_mul_req;
 
+/* A list of products queued by one call (no counterpart in the reference):
+   each request runs as gpu_mpn_mul_device would run it (its own launches,
+   under cfgs[i] when cfgs is not NULL), one after another on `stream`,
+   without a host synchronisation; every request is planned and the context's
+   scratch sized for the largest before anything is queued (an invalid
+   request fails the call, naming its index).  The per-product counterpart
+   of a planned batch, without its class merging or graph. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_device_list(gpu_mpn_ctx_t R, const gpu_mpn_mul_req *reqs, size_t n,
+                                              const gpu_mul_config *cfgs, void *stream);
+
 /* Schedule of a batch.  promote_small: products whose (primes, transform
    length) class holds fewer than this many products are run at the next
    longer length together with that class (0 = off).  max_streams: classes run
@@ -727,6 +737,14 @@ GPU_FFT_SMALL_API int gpu_mpn_mul_plan(gpu_ulong an, gpu_ulong bn, int *np, int 
    operand against one transform of the short one), or 0 when it runs as a
    single transform; returns 0 on success. */
 GPU_FFT_SMALL_API int gpu_mpn_mul_split_plan(gpu_ulong an, gpu_ulong bn, int *chunk_logM);
+/* Points of the cyclic transform a whole an x bn product (squaring when
+   square != 0) runs under the default plan: 2^logM, or 3 2^(logM - 2) when
+   the product fits that truncated length (the counterpart of the
+   reference's transform truncation, src/fft_small/sd_fft.c:1230-1274), or
+   the chunk transform of a split product; 0 for the basecase route.
+   Returns 0 on success. */
+GPU_FFT_SMALL_API int gpu_mpn_mul_transform_points(gpu_ulong an, gpu_ulong bn, int square,
+                                                   gpu_ulong *points);
 /* The i-th prime of the GPU prime set (0 if out of range). */
 GPU_FFT_SMALL_API gpu_ulong gpu_fft_small_prime(int i);
 /* Kernel launches issued by the most recent call on this context. */

@@ -66,3 +66,20 @@ def test_products_beyond_the_longest_transform_split(an, bn, want):
     with pytest.raises(FB.GpuFftSmallError):
         FB.mpn_mul_plan(an, bn)                          # no single transform holds them
     assert FB.mpn_mul_split_plan(an, bn) == want
+
+
+def test_transform_points_truncated_lengths():
+    """Whole products between 2^(m-1) and 3 2^(m-2) coefficients (m >= 20)
+    run 3 2^(m-2)-point transforms; elsewhere the power of two stays."""
+    import flint_b200 as FB
+    assert FB.mpn_mul_transform_points(1 << 23, 1 << 23) == 1 << 24        # L = 2^24 - 1: a power of two
+    assert FB.mpn_mul_transform_points((1 << 23) + (1 << 20), (1 << 23) + (1 << 20)) == 3 << 23
+    assert FB.mpn_mul_transform_points(3 << 22, 3 << 22) == 3 << 23
+    assert FB.mpn_mul_transform_points((3 << 22) + 1, 3 << 22) == 3 << 23   # L = 3 2^23 exactly
+    assert FB.mpn_mul_transform_points((3 << 22) + 1, (3 << 22) + 1) == 1 << 25
+    assert FB.mpn_mul_transform_points(1 << 24, 1 << 24) == 1 << 25
+    # below 2^19 coefficients the columns are too short for the radix-3 kernels
+    assert FB.mpn_mul_transform_points(150000, 150000) == 1 << 19
+    assert FB.mpn_mul_transform_points((1 << 18) + 100, (1 << 18) + 7) == 3 << 18
+    # squarings take the same lengths
+    assert FB.mpn_mul_transform_points(3000000, 3000000, square=True) == 3 << 21
