@@ -9,6 +9,7 @@
  *   gpu_shim__mpn_ctx_mpn_mul_range        _mpn_ctx_mpn_mul_range (src/fft_small.h:462)
  *   gpu_shim__nmod_poly_mul_mid_mpn_ctx    _nmod_poly_mul_mid_mpn_ctx (src/fft_small.h:769-774)
  *   gpu_shim__fmpz_poly_mul_mid_mpn_ctx    _fmpz_poly_mul_mid_mpn_ctx (src/fft_small.h:856-860)
+ *   gpu_shim__nmod_poly_divrem_mpn_ctx     _nmod_poly_divrem_mpn_ctx (src/fft_small.h:776-781)
  *
  * A FLINT build can select them with the preprocessor (for example
  * -Dmpn_ctx_mpn_mul=gpu_shim_mpn_ctx_mpn_mul for the translation units that
@@ -92,4 +93,15 @@ int gpu_shim__fmpz_poly_mul_mid_mpn_ctx(fmpz * z, ulong zl, ulong zh, const fmpz
     (void) R;
     return _gpu_fmpz_poly_mul_mid_mpn_ctx((gpu_slong *) z, zl, zh, (const gpu_slong *) a, an,
                                           (const gpu_slong *) b, bn, shim_ctx());
+}
+
+void gpu_shim__nmod_poly_divrem_mpn_ctx(ulong * q, ulong * r, const ulong * a, ulong an,
+                                        const ulong * b, ulong bn, nmod_t mod, mpn_ctx_t R)
+{
+    gpu_nmod_t gm;
+    (void) R;
+    gm.n = mod.n;
+    gm.ninv = mod.ninv;
+    gm.norm = mod.norm;
+    _gpu_nmod_poly_divrem_mpn_ctx(q, r, a, an, b, bn, gm, shim_ctx());
 }

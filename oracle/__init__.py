@@ -80,6 +80,8 @@ def ref():
         L.flint_get_num_threads.restype = ctypes.c_int
         L.n_preinvert_limb.argtypes = [U]
         L.n_preinvert_limb.restype = U
+        L._nmod_poly_divrem_mpn_ctx.argtypes = [P, P, P, U, P, U, NmodT, P]
+        L._nmod_poly_divrem_mpn_ctx.restype = None
         _ref = L
     return _ref
 
@@ -407,13 +409,30 @@ def check_mul_range_contract(a, b, lo, z):
     return d
 
 
+def ref_nmod_divrem(a, b, n):
+    """The reference's own _nmod_poly_divrem_mpn_ctx (src/fft_small/
+    nmod_poly_mul.c:1248-1277) on its default context: (q, r) with
+    a = q b + r mod n, r of bn - 1 coefficients (b's leading coefficient a
+    unit mod n, bn >= 2)."""
+    a = np.ascontiguousarray(a, dtype=np.uint64)
+    b = np.ascontiguousarray(b, dtype=np.uint64)
+    L = ref()
+    norm = 64 - int(n).bit_length()
+    ninv = L.n_preinvert_limb(n << norm)
+    an, bn = len(a), len(b)
+    q = np.zeros(an - bn + 1, dtype=np.uint64)
+    r = np.zeros(bn - 1, dtype=np.uint64)
+    L._nmod_poly_divrem_mpn_ctx(q.ctypes.data, r.ctypes.data, a.ctypes.data, an, b.ctypes.data, bn,
+                                NmodT(n, ninv, norm), L.get_default_mpn_ctx())
+    return q, r
+
+
 def check_nmod_divrem(a, b, n, q, r):
     """a = q b + r mod n with r of bn - 1 coefficients, checked with the
-    reference's own _nmod_poly_mul_mid_mpn_ctx for the product q b (the
-    reference's _nmod_poly_divrem_mpn_ctx reaches _nmod_poly_inv_series,
-    which needs FLINT's generic-ring module, outside the compiled closure).
+    reference's own _nmod_poly_mul_mid_mpn_ctx for the product q b.
     Quotient and remainder are unique when b's leading coefficient is a
-    unit, so the identity pins them."""
+    unit, so the identity pins them (ref_nmod_divrem gives the reference's
+    own division for a direct comparison)."""
     a = np.ascontiguousarray(a, dtype=np.uint64)
     an, bn = len(a), len(b)
     assert len(q) == an - bn + 1 and len(r) == bn - 1

@@ -43,6 +43,10 @@ DIRS = [
     "fft_small", "ulong_extras", "long_extras", "nmod", "nmod_vec", "nmod_poly",
     "fmpz", "fmpz_vec", "fmpz_poly", "mpn_extras", "thread_pool",
     "thread_support", "generic_files", "fft",
+    # generic rings: _nmod_poly_inv_series (behind _nmod_poly_divrem_mpn_ctx,
+    # src/fft_small/nmod_poly_mul.c:1248-1277) hands series longer than 10
+    # terms to _gr_poly_inv_series over the nmod ring (src/nmod_poly/inv_series.c:63-77)
+    "gr", "gr_generic", "gr_poly", "gr_vec",
 ]
 
 # Single files outside the whole directories: the non-reentrant fmpz memory
@@ -228,7 +232,8 @@ REQUIRED = ["mpn_ctx_init", "mpn_ctx_clear", "mpn_ctx_mpn_mul",
             "_fmpz_poly_mul_mid_mpn_ctx", "get_default_mpn_ctx",
             "mpn_mul_default_mpn_ctx", "_fmpz_poly_mul", "flint_set_num_threads",
             "flint_mpn_mul", "_nmod_poly_mul_KS", "_fmpz_poly_mul_KS",
-            "sd_fft_trunc", "sd_ifft_trunc", "sd_fft_ctx_init_prime"]
+            "sd_fft_trunc", "sd_ifft_trunc", "sd_fft_ctx_init_prime",
+            "_nmod_poly_divrem_mpn_ctx", "_nmod_poly_divrem", "_gr_poly_inv_series"]
 
 
 DEFAULT_REF = os.environ.get("FLINT_REFERENCE", "/root/reference")

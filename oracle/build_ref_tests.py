@@ -3,20 +3,21 @@
 from C (test infrastructure only).
 
 The reference's test programs ``src/fft_small/test/t-mul.c``,
-``t-nmod_poly_mul.c`` and ``t-fmpz_poly_mul.c`` are compiled unchanged from the
-reference tree, with the entry points under test renamed by the preprocessor
+``t-nmod_poly_mul.c``, ``t-fmpz_poly_mul.c`` and ``t-nmod_poly_divrem.c`` are
+compiled unchanged from the reference tree, with the entry points under test renamed by the preprocessor
 to the C shim of this repository (``flint_b200/shim/fft_small_gpu_shim.c``):
 
     mpn_ctx_mpn_mul              -> gpu_shim_mpn_ctx_mpn_mul
     _mpn_ctx_mpn_mul_range       -> gpu_shim__mpn_ctx_mpn_mul_range
     _nmod_poly_mul_mid_mpn_ctx   -> gpu_shim__nmod_poly_mul_mid_mpn_ctx
     _fmpz_poly_mul_mid_mpn_ctx   -> gpu_shim__fmpz_poly_mul_mid_mpn_ctx
+    _nmod_poly_divrem_mpn_ctx    -> gpu_shim__nmod_poly_divrem_mpn_ctx
 
 so every product they check comes from libflint_b200.so through its C ABI,
 while their yardsticks (GMP's mpn_mul / mpn_sqr, _nmod_poly_mul_KS,
-_fmpz_poly_mul_KS) and their harness (random states, TEST_MAIN) come from
+_fmpz_poly_mul_KS, the generic _nmod_poly_divrem) and their harness (random states, TEST_MAIN) come from
 the compiled reference (oracle/_ref/libflint_ref.so, build_ref.py).  A small
-generated main file lists the three test functions.  The binary,
+generated main file lists the four test functions.  The binary,
 ``oracle/_ref/t-gpu-fft_small``, finds both libraries through its run path;
 tests/test_c_caller_gpu.py runs it on a GPU.  Nothing is written outside
 oracle/_ref.  Usage::
@@ -40,10 +41,12 @@ RENAMES = {
     "_mpn_ctx_mpn_mul_range": "gpu_shim__mpn_ctx_mpn_mul_range",
     "_nmod_poly_mul_mid_mpn_ctx": "gpu_shim__nmod_poly_mul_mid_mpn_ctx",
     "_fmpz_poly_mul_mid_mpn_ctx": "gpu_shim__fmpz_poly_mul_mid_mpn_ctx",
+    "_nmod_poly_divrem_mpn_ctx": "gpu_shim__nmod_poly_divrem_mpn_ctx",
 }
-TESTS = ["t-mul.c", "t-nmod_poly_mul.c", "t-fmpz_poly_mul.c"]
+TESTS = ["t-mul.c", "t-nmod_poly_mul.c", "t-fmpz_poly_mul.c", "t-nmod_poly_divrem.c"]
 # the test functions those files define (TEST_FUNCTION_START labels)
-LABELS = ["mpn_ctx_mpn_mul", "_nmod_poly_mul_mid_mpn_ctx", "_fmpz_poly_mul_mid_mpn_ctx"]
+LABELS = ["mpn_ctx_mpn_mul", "_nmod_poly_mul_mid_mpn_ctx", "_fmpz_poly_mul_mid_mpn_ctx",
+          "_nmod_poly_divrem_mpn_ctx"]
 
 MAIN = """\
 /* generated by oracle/build_ref_tests.py: the reference's fft_small tests

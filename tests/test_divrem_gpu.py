@@ -42,3 +42,39 @@ def test_divrem_rejects_non_unit_leading_coefficient(ctx):
     with pytest.raises(FB.GpuFftSmallError) as e:
         ctx.nmod_poly_divrem(a, b, 12)
     assert e.value.code == FB.EINVAL
+
+
+def _unit_leading(seed, bn, n):
+    """A divisor whose leading coefficient is a unit mod n."""
+    import math
+    b = O.rand_below(seed, bn, n)
+    k = 0
+    while math.gcd(int(b[-1]), n) != 1:
+        k += 1
+        b[-1] = (int(b[-1]) + k) % n
+    return b
+
+
+# seeded draws in the shape of the reference's own test
+# (src/fft_small/test/t-nmod_poly_divrem.c: bn in [2, 5002), qn in [1, 5001),
+# moduli of 2 to 64 bits), plus larger quotients and divisors
+REF_CASES = [(an_, bn_, bits) for (an_, bn_, bits) in [
+    (2, 2, 2), (12, 11, 3), (300, 7, 17), (5000, 2, 31), (5001, 5000, 40), (9999, 5001, 62),
+    (4200, 3100, 63), (7000, 123, 64), (20000, 9000, 61), (1 << 17, 1 << 15, 64)]]
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference not built")
+@pytest.mark.parametrize("an,bn,bits", REF_CASES)
+def test_divrem_equals_reference(ctx, an, bn, bits):
+    """Quotient and remainder equal the reference's own
+    _nmod_poly_divrem_mpn_ctx (src/fft_small/nmod_poly_mul.c:1248-1277) on the
+    same seeded inputs, coefficient for coefficient."""
+    n = int(O.rand_limbs(an * 7 + bits, 1)[0]) >> (64 - bits) | (1 << (bits - 1))
+    if n < 2:
+        n = 3
+    a = O.rand_below(an + bits, an, n)
+    b = _unit_leading(bn + 3 * bits, bn, n)
+    q, r = ctx.nmod_poly_divrem(a, b, n)
+    qr, rr = O.ref_nmod_divrem(a, b, n)
+    assert np.array_equal(np.asarray(q, dtype=np.uint64), qr)
+    assert np.array_equal(np.asarray(r, dtype=np.uint64), rr)

@@ -219,3 +219,22 @@ def test_negmul_oracle_vs_reference(seed):
         x = O.neg_operand(300 + seed, n, kx)
         y = O.neg_operand(400 + seed, n, ky)
         assert (O.negmul_python(x, y, N) == O.ref_mulmod_2expp1(x, y, N, m)).all()
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="compiled reference not built")
+@pytest.mark.parametrize("an,bn,n", [(30, 7, 1000003), (500, 40, (1 << 61) + 15), (200, 199, 7),
+                                     (3000, 2000, 7340033), (9000, 4000, (1 << 63) + 29)])
+def test_reference_divrem_pinned(an, bn, n):
+    """The reference's own _nmod_poly_divrem_mpn_ctx (compiled with the
+    generic-ring modules its series inverse needs) against schoolbook
+    division in Python at small sizes and the identity a = q b + r above."""
+    import math
+    a = O.rand_below(an + 1, an, n)
+    b = O.rand_below(bn + 2, bn, n)
+    while math.gcd(int(b[-1]), n) != 1:
+        b[-1] = (int(b[-1]) + 1) % n
+    q, r = O.ref_nmod_divrem(a, b, n)
+    assert O.check_nmod_divrem(a, b, n, q, r)
+    if an <= 500:
+        qp, rp = O.nmod_divrem_python(a, b, n)
+        assert [int(x) for x in q] == qp and [int(x) for x in r] == rp
