@@ -251,7 +251,9 @@ def train_cost_model(ctx):
     info = {"train_requests": len(train), "train_rows": int(len(X)), "tuning_s": t_tune,
             "fit_s": time.perf_counter() - t0, "fit_mse_log_ms": loss,
             "decision_margin": model.margin,
-            "network": "16 -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels"}
+            "network": "%d -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels" % tuner.N_FEATURES,
+            "candidates": "route (transform / basecase), primes (min, +1), length (min, x2), rows "
+                          "(longest .. 8x shorter), THREE (3 2^k length) and SPLIT flags for mpn"}
     return model, tun, info
 
 
@@ -274,13 +276,15 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
     learned = model.choose(reqs)
     t_choose = time.perf_counter() - t0
     default = [tuner.default_config(r) for r in reqs]
+    refrule = [tuner.reference_rule(r) for r in reqs]
     keep = stream_subsample(reqs)
     w0 = time.perf_counter()
     rl = run_stream(ctx, torch, reqs, learned, 17, stream, dev, keep=keep)
     w1 = time.perf_counter()
     rd = run_stream(ctx, torch, reqs, default, 17, stream, dev)
     w2 = time.perf_counter()
-    same = rl["digests"] == rd["digests"]
+    rr = run_stream(ctx, torch, reqs, refrule, 17, stream, dev)
+    same = (rl["digests"] == rd["digests"]) & (rl["digests"] == rr["digests"])
     held = request_stream(STREAM_SEED + 2, n_held)
     t0 = time.perf_counter()
     reg = tuner.regret(tun, held, model.choose(held))
@@ -297,12 +301,23 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
         "learned": {"total_ms": rl["total_ms"], "mpn_ms": rl["mpn_ms"], "fmpz_ms": rl["fmpz_ms"],
                     "mpn_Gbit_s": bits_mpn / rl["mpn_ms"] / 1e6},
         "default_rule": {"total_ms": rd["total_ms"], "mpn_ms": rd["mpn_ms"], "fmpz_ms": rd["fmpz_ms"],
-                         "mpn_Gbit_s": bits_mpn / rd["mpn_ms"] / 1e6},
+                         "mpn_Gbit_s": bits_mpn / rd["mpn_ms"] / 1e6,
+                         "rule": "fewest primes, shortest power-of-two transform, longest rows, "
+                                 "every mpn product in a planned batch"},
+        "reference_rule": {"total_ms": rr["total_ms"], "mpn_ms": rr["mpn_ms"], "fmpz_ms": rr["fmpz_ms"],
+                           "mpn_Gbit_s": bits_mpn / rr["mpn_ms"] / 1e6,
+                           "rule": "the reference's mpn_ctx_best_profile score over this library's "
+                                   "configurations (gpu_mul_reference_rule, host C): 3 2^k lengths where "
+                                   "they fit, run per instance"},
         "gain_over_default_rule": rd["total_ms"] / rl["total_ms"],
+        "gain_over_reference_rule": rr["total_ms"] / rl["total_ms"],
+        "flags_chosen": {"three": sum(bool(c.flags & FB.FLAG_THREE) for c in learned),
+                         "split": sum(bool(c.flags & FB.FLAG_SPLIT) for c in learned)},
         "choose_s": t_choose, "wall_s": {"learned_run": w1 - w0, "default_run": w2 - w1},
         "routes": {"transform": sum(c.route == 0 for c in learned),
                    "basecase": sum(c.route == 1 for c in learned)},
         "identical_to_default_rule": bool(same.all()),
+        "identical_note": "learned, fixed-rule and reference-rule runs: every product's digest equal",
         "digests_compared": int(len(same)), "digests_equal": int(same.sum()),
         "digest_note": "per product: sum of its limbs times fixed pseudo-random 64-bit weights, "
                        "mod 2^64, computed on the device, learned run against default-rule run",
@@ -405,6 +420,13 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
     per_instance()
     host_issue_ms = (time.perf_counter() - t0) * 1e3
     stream.synchronize()
+    # GPU-busy time of the per-instance path: the sum of its kernels' own
+    # durations (CUDA events around each launch) over one step
+    ctx.set_timing(True)
+    per_instance()
+    stream.synchronize()
+    busy_ms = sum(v[0] for v in ctx.kernel_times().values())
+    ctx.set_timing(False)
     ms_plain_py = time_on_stream(torch, stream, per_instance_python, max(2, k_plain // 2), 1)
     B0 = FB.MpnBatch(ctx, reqs)
     ms_default = time_on_stream(torch, stream, lambda: B0.run(s), steps, warmup)
@@ -413,10 +435,11 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
     B0.close()
     # learned schedule: one configuration per request of the batch from the
     # cost model; its regret on held-out requests of this distribution
+    # planned batches run plain transforms: the model chooses among those
     held = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 2, 48)]
-    reg = tuner.regret(tun, held, model.choose(held))
+    reg = tuner.regret(tun, held, model.choose(held, flags=False), flags=False)
     t0 = time.perf_counter()
-    configs = model.choose([(0, a, b) for a, b in sizes])
+    configs = model.choose([(0, a, b) for a, b in sizes], flags=False)
     t_choose = time.perf_counter() - t0
     B = FB.MpnBatch(ctx, reqs, configs=configs)
     d_out.fill_(0)
@@ -497,7 +520,9 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
                          "launches_per_step": 4 * BATCH_N,
                          "api": "gpu_mpn_mul_device_list: one native call queues the products one by "
                                 "one, as gpu_mpn_mul_device runs them",
-                         "host_issue_ms_per_step": host_issue_ms},
+                         "host_issue_ms_per_step": host_issue_ms, "gpu_busy_ms_per_step": busy_ms,
+                         "note": "launch-bound: the kernels are busy for gpu_busy_ms of each step, the host "
+                                 "needs host_issue_ms to issue its 4 launches per product"},
         "per_instance_python_loop": {"value": bits / ms_plain_py / 1e6, "ms_per_step": ms_plain_py,
                                      "api": "gpu_mpn_mul_device called from a Python loop"},
         "plain_batched": {"value": bits / ms_default / 1e6, "ms_per_step": ms_default,

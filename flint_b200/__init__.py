@@ -77,18 +77,21 @@ class FmpzMulReq(ctypes.Structure):
 
 
 class MulConfig(ctypes.Structure):
-    """gpu_mul_config: route, prime count, log2 transform length, log2 row length."""
+    """gpu_mul_config: route, prime count, log2 transform length, log2 row
+    length, flags (FLAG_THREE: a 3 2^(logM-2)-point transform; FLAG_SPLIT:
+    chunks of the long operand against the short one)."""
     _fields_ = [("route", ctypes.c_int), ("np", ctypes.c_int), ("logM", ctypes.c_int),
-                ("logC", ctypes.c_int)]
+                ("logC", ctypes.c_int), ("flags", ctypes.c_int)]
 
     def key(self):
-        return (self.route, self.np, self.logM, self.logC)
+        return (self.route, self.np, self.logM, self.logC, self.flags)
 
     def __repr__(self):
-        return "MulConfig(route=%d, np=%d, logM=%d, logC=%d)" % self.key()
+        return "MulConfig(route=%d, np=%d, logM=%d, logC=%d, flags=%d)" % self.key()
 
 
 ROUTE_NTT, ROUTE_BASECASE = 0, 1
+FLAG_THREE, FLAG_SPLIT = 1, 2
 
 
 class BatchOptions(ctypes.Structure):
@@ -168,6 +171,7 @@ SIGNATURES = {
                                                            _U, ctypes.POINTER(MulConfig), _P]),
     "gpu_fmpz_poly_mul_mid_device_list": (ctypes.c_int, [_CTX, _P, ctypes.c_size_t, _P, _P]),
     "gpu_mpn_mul_device_list": (ctypes.c_int, [_CTX, _P, ctypes.c_size_t, _P, _P]),
+    "gpu_mul_reference_rule": (ctypes.c_int, [ctypes.c_int, _U, _U, _U, _U, ctypes.POINTER(MulConfig)]),
     "gpu_mul_time_config": (ctypes.c_int, [_CTX, ctypes.c_int, _U, _U, _U, _U,
                                            ctypes.POINTER(MulConfig), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_double)]),
@@ -286,11 +290,19 @@ def prime(i):
 def resolve_config(kind, an, bn, cfg=None, aw=1, bw=1):
     """The full configuration (defaults filled in) for a product, or raises
     GpuFftSmallError if cfg is invalid for it."""
-    c = MulConfig(*(cfg.key() if cfg is not None else (0, 0, 0, 0)))
+    c = MulConfig(*(cfg.key() if cfg is not None else (0, 0, 0, 0, 0)))
     if kind == 0:
         _check(lib().gpu_mpn_mul_config_resolve(an, bn, ctypes.byref(c)))
     else:
         _check(lib().gpu_fmpz_poly_mul_config_resolve(an, aw, bn, bw, ctypes.byref(c)))
+    return c
+
+
+def reference_rule(kind, an, bn, aw=1, bw=1):
+    """The configuration the reference's profile choice (mpn_ctx_best_profile)
+    makes in this configuration space (gpu_mul_reference_rule)."""
+    c = MulConfig()
+    _check(lib().gpu_mul_reference_rule(kind, an, aw, bn, bw, ctypes.byref(c)))
     return c
 
 

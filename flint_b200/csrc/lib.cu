@@ -735,6 +735,8 @@ static int ceil_log2_u64(uint64_t x)
 // plan_mpn); every choice is checked against the exactness bound and the
 // kernels' shape limits.
 static int plan_mpn(uint64_t an, uint64_t bn, MulPlan *P);
+static int three_length(uint64_t L, int np, int logM);
+static int split_plan(uint64_t an, uint64_t bn, int logM);
 static int plan_mpn_cfg(uint64_t an, uint64_t bn, const gpu_mul_config *cfg, MulPlan *P)
 {
     int rc = plan_mpn(an, bn, P);
@@ -743,7 +745,7 @@ static int plan_mpn_cfg(uint64_t an, uint64_t bn, const gpu_mul_config *cfg, Mul
         if (std::min(an, bn) > (uint64_t)BASECASE_MAX)
             return set_error(GPU_FFT_SMALL_EINVAL, "basecase route needs an operand of at most %d limbs",
                              BASECASE_MAX);
-        if (cfg->np || cfg->logM || cfg->logC)
+        if (cfg->np || cfg->logM || cfg->logC || cfg->flags)
             return set_error(GPU_FFT_SMALL_EINVAL, "basecase route takes no transform parameters");
         P->route = GPU_MUL_ROUTE_BASECASE;
         P->np = 0;
@@ -762,10 +764,24 @@ static int plan_mpn_cfg(uint64_t an, uint64_t bn, const gpu_mul_config *cfg, Mul
                              P->logM, LOG_MAXM);
         P->logM = cfg->logM;
     }
-    const int logC = cfg->logC ? cfg->logC : default_logC(P->logM);
-    if (!valid_logC(P->logM, logC))
+    const int fl = cfg->flags;
+    // a 3 2^k-point transform has rows of 2^LOGC3 points whatever logM is
+    const int logC = (fl & GPU_MUL_FLAG_THREE) ? LOGC3 : cfg->logC ? cfg->logC : default_logC(P->logM);
+    if (!(fl & GPU_MUL_FLAG_THREE) && !valid_logC(P->logM, logC))
         return set_error(GPU_FFT_SMALL_EINVAL, "row length 2^%d invalid for a 2^%d transform", logC, P->logM);
-    P->L = make_shape(P->logM, logC);
+    P->L = make_shape(P->logM, (fl & GPU_MUL_FLAG_THREE) ? -1 : logC);
+    if (fl & ~(GPU_MUL_FLAG_THREE | GPU_MUL_FLAG_SPLIT))
+        return set_error(GPU_FFT_SMALL_EINVAL, "unknown configuration flags 0x%x", fl);
+    if ((fl & GPU_MUL_FLAG_THREE) && (fl & GPU_MUL_FLAG_SPLIT))
+        return set_error(GPU_FFT_SMALL_EINVAL, "THREE and SPLIT exclude each other");
+    if ((fl & GPU_MUL_FLAG_THREE) && !three_length(an + bn - 1, P->np, P->logM))
+        return set_error(GPU_FFT_SMALL_EINVAL, "no 3 2^%d-point transform for a %llu x %llu product with %d primes",
+                         P->logM - 2, (unsigned long long)an, (unsigned long long)bn, P->np);
+    if ((fl & GPU_MUL_FLAG_THREE) && cfg->logC && cfg->logC != LOGC3)
+        return set_error(GPU_FFT_SMALL_EINVAL, "3 2^k-point transforms use 2^%d-point rows", LOGC3);
+    if ((fl & GPU_MUL_FLAG_SPLIT) && !split_plan(an, bn, P->logM))
+        return set_error(GPU_FFT_SMALL_EINVAL, "a %llu x %llu product does not split",
+                         (unsigned long long)an, (unsigned long long)bn);
     return 0;
 }
 
@@ -1115,10 +1131,12 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     // an unbalanced whole product may run as chunks of the long operand
     // against the short one (split_plan): their residues are summed into
     // one array of the full length, then a single CRT/carry pass follows
-    const int Lc = Lover ? Lover : (!cfg && !window && !sq) ? split_plan(an, bn, logM) : 0;
+    const int fl = cfg ? cfg->flags : 0;
+    const int Lc = Lover ? Lover : ((!cfg || (fl & GPU_MUL_FLAG_SPLIT)) && !window && !sq) ? split_plan(an, bn, logM) : 0;
     // whole products between 2^(logM - 1) and 3 2^(logM - 2) coefficients on
-    // the default plan run a 3 2^(logM - 2)-point transform
-    const int k3 = (!cfg && !window && !Lc) ? three_length(an + bn - 1, np, logM) : 0;
+    // the default plan (or under the THREE flag) run a 3 2^(logM - 2)-point
+    // transform
+    const int k3 = ((!cfg || (fl & GPU_MUL_FLAG_THREE)) && !window && !Lc) ? three_length(an + bn - 1, np, logM) : 0;
     const size_t Mc = Lc ? (size_t)1 << Lc : 0;
     const size_t res_bytes = Lc ? (size_t)np * (M + 2 * Mc) * sizeof(uint32_t)
                                 : (sq ? 1 : 2) * (size_t)np * M * sizeof(uint32_t);
@@ -1638,8 +1656,51 @@ int gpu_mpn_mul_config_resolve(gpu_ulong an, gpu_ulong bn, gpu_mul_config *cfg)
     if (P.route == GPU_MUL_ROUTE_NTT) {
         cfg->np = P.np;
         cfg->logM = P.logM;
-        cfg->logC = P.L.S.logC;
+        cfg->logC = (cfg->flags & GPU_MUL_FLAG_THREE) ? LOGC3 : P.L.S.logC;
     }
+    return 0;
+}
+
+// The reference's profile choice (mpn_ctx_best_profile, src/fft_small/
+// mpn_mul.c:1248-1340) in this library's configuration space: among single
+// transforms with the longest rows -- the fewest primes or one more, the
+// shortest power-of-two length or, where the product fits it, the 3 2^k
+// length (the counterpart of its truncated ztrunc) -- the least score
+// (1 - ratio / 4) np depth L_t, with L_t the transform's points,
+// depth = ceil(log2 L_t) and ratio = L_t / 2^depth (ties to fewer primes).
+// The reference scores its own profiles (50-bit primes, chunk bit sizes,
+// 256-point truncation); the formula is the same.
+int gpu_mul_reference_rule(int kind, gpu_ulong an, gpu_ulong aw, gpu_ulong bn, gpu_ulong bw,
+                           gpu_mul_config *cfg)
+{
+    if (!cfg) return set_error(GPU_FFT_SMALL_EINVAL, "null configuration");
+    gpu_mul_config best{0, 0, 0, 0, 0};
+    double best_score = -1.0;
+    int rc = 0;
+    for (int dnp = 0; dnp <= 1; dnp++)
+        for (int fl = 0; fl <= GPU_MUL_FLAG_THREE; fl += GPU_MUL_FLAG_THREE) {
+            if (kind != 0 && fl) continue;
+            gpu_mul_config c{GPU_MUL_ROUTE_NTT, 0, 0, 0, fl};
+            rc = kind == 0 ? gpu_mpn_mul_config_resolve(an, bn, &c)
+                           : gpu_fmpz_poly_mul_config_resolve(an, aw, bn, bw, &c);
+            if (rc) continue;
+            if (dnp) {
+                c.np += 1;
+                c.logC = 0;
+                rc = kind == 0 ? gpu_mpn_mul_config_resolve(an, bn, &c)
+                               : gpu_fmpz_poly_mul_config_resolve(an, aw, bn, bw, &c);
+                if (rc) continue;
+            }
+            const double lt = fl ? 3.0 * ldexp(1.0, c.logM - 2) : ldexp(1.0, c.logM);
+            const int depth = (int)ceil(log2(lt) - 1e-9);
+            const double score = (1.0 - 0.25 * lt / ldexp(1.0, depth)) * c.np * depth * lt;
+            if (best_score < 0 || score < best_score) {
+                best = c;
+                best_score = score;
+            }
+        }
+    if (best_score < 0) return rc ? rc : set_error(GPU_FFT_SMALL_EINVAL, "no transform configuration");
+    *cfg = best;
     return 0;
 }
 

@@ -96,11 +96,28 @@ k_fwd_cols3(DevTables T, const uint64_t* __restrict__ a, uint64_t an, const uint
     const PrimeInfo P = T.pi[j];
     const uint32_t p = P.p;
 
-    // limbs of rows 0 .. 3R' - 1 (element n = u C + i; zero beyond the operand)
-    for (int f = threadIdx.x; f < 3 * RP * G; f += blockDim.x) {
-        const int u = f / G, c = f & (G - 1);
-        const uint64_t n = (uint64_t)u * C + i0 + c;
-        sm[padw(u * G) + c] = n < xn ? limb_redc(x[n], p, P.pneg_inv, P.c32) : 0u;
+    // limbs of rows 0 .. 3R' - 1 (element n = u C + i; zero beyond the operand).
+    // blockDim == 512: thread t loads rows u_t + k 512/G of its column, so its
+    // shared offsets are compile-time constants and its global address a
+    // pointer bump; the in-range loads are counted once (a shift)
+    {
+        constexpr int K = 3 * RP * G / 512;
+        constexpr int ROWS_PER = 512 / G;
+        const int t = threadIdx.x;
+        const int u_t = t / G, c = t & (G - 1);
+        const uint64_t n0 = (uint64_t)u_t * C + i0 + c;
+        static_assert(RP * G == 8192, "tiles of 3 2^13 words");
+        constexpr int lstep = LOGR - 4 + LOGC3;   // log2(ROWS_PER C): ROWS_PER = 2^(LOGR - 4)
+        int kin = 0;
+        if (n0 < xn) {
+            const uint64_t q = ((xn - n0 - 1) >> lstep) + 1;
+            kin = q < (uint64_t)K ? (int)q : K;
+        }
+        const uint64_t* px = x + n0;
+        uint32_t* d = sm + padw(u_t * G) + c;
+#pragma unroll 8
+        for (int k = 0; k < K; k++, px += (size_t)ROWS_PER * C)
+            d[k * (ROWS_PER * G + ROWS_PER * G / 32)] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
     }
     __syncthreads();
     // radix-3 stage: (u1, u1 + R', u1 + 2R') -> t0, t1 omega^u1, t2 omega^(2 u1)

@@ -7,13 +7,17 @@ the configuration a chooser gives it:
 
 * mpn requests go in chunks (at most ``chunk_limbs`` operand limbs each) into
   planned batches (gpu_mpn_batch_init_config), so products that share a
-  configuration share launches;
+  configuration share launches; requests whose configuration carries flags
+  (a 3 2^k-point transform, a split product) go in chunks through the
+  per-instance list call (gpu_mpn_mul_device_list) instead;
 * integer-polynomial requests go in chunks through one list call each
   (gpu_fmpz_poly_mul_mid_device_list): every product of a chunk is queued by
   native code on one stream, with the scratch sized before the timing.
 
-Operands are generated on the device from a seed (torch's CUDA generator),
-outside the timed region; the device time of the products is measured with
+Operands come from one pool of pseudo-random limbs generated on the device
+from the seed (torch's CUDA generator): request k reads the pool at an offset
+hashed from k, so its operands do not depend on how a schedule groups the
+requests.  They are gathered outside the timed region; the device time of the products is measured with
 CUDA events on the launching stream.  Every product also gets a 64-bit
 digest (a weighted sum of its limbs with fixed pseudo-random weights,
 computed on the device), so two runs under different schedules can be
@@ -22,7 +26,7 @@ a caller copy selected products (with their operands) to the host.
 """
 import numpy as np
 
-from . import FmpzMulReq, MpnBatch
+from . import FmpzMulReq, MpnBatch, MulReq
 
 
 def _weights(torch, n, dev):
@@ -45,6 +49,24 @@ def _digests(torch, out, starts, lens, weights):
     d = torch.zeros(len(starts), dtype=torch.int64, device=dev)
     d.index_add_(0, owner, prod)
     return d
+
+
+POOL_LIMBS = 1 << 27
+
+
+def _pool_offset(k, n):
+    """Pool offset of request k's n operand limbs (a fixed hash of k)."""
+    return ((k + 1) * 0x9E3779B97F4A7C15 >> 17) % (POOL_LIMBS - n)
+
+
+def _gather(torch, pool, starts, lens):
+    """The pool slices [starts[k], starts[k] + lens[k]) concatenated."""
+    dev = pool.device
+    st = torch.tensor(starts, dtype=torch.int64, device=dev)
+    ln = torch.tensor(lens, dtype=torch.int64, device=dev)
+    base = torch.repeat_interleave(torch.cumsum(ln, 0) - ln, ln)
+    idx = torch.arange(int(sum(lens)), device=dev) - base + torch.repeat_interleave(st, ln)
+    return pool[idx]
 
 
 def _chunks(idx, size_of, limit):
@@ -73,18 +95,23 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27
     res = {"mpn_ms": 0.0, "fmpz_ms": 0.0, "mpn_limbs": 0, "fmpz_coeff_limbs": 0,
            "mpn_requests": 0, "fmpz_requests": 0, "kept": {}}
     digests = np.zeros(len(reqs), dtype=np.int64)
-    mpn = [k for k, r in enumerate(reqs) if r[0] == 0]
+    mpn = [k for k, r in enumerate(reqs) if r[0] == 0 and not configs[k].flags]
+    mpn_list = [k for k, r in enumerate(reqs) if r[0] == 0 and configs[k].flags]
     fz = [k for k, r in enumerate(reqs) if r[0] == 1]
     wmax = 1
     for r in reqs:
         wmax = max(wmax, r[1] + r[2] if r[0] == 0 else (r[1] + r[2] - 1) * (r[3] + r[4] + 1))
     weights = _weights(torch, wmax, dev)
+    gen.manual_seed(seed)
+    pool = torch.randint(-(1 << 63), (1 << 63) - 1, (POOL_LIMBS,), dtype=torch.int64, device=dev,
+                         generator=gen)
+
+    def operands(idx, size_of):
+        return _gather(torch, pool, [_pool_offset(k, size_of(k)) for k in idx], [size_of(k) for k in idx])
 
     for ci, idx in enumerate(_chunks(mpn, lambda k: reqs[k][1] + reqs[k][2], chunk_limbs)):
         tot = sum(reqs[k][1] + reqs[k][2] for k in idx)
-        gen.manual_seed(seed * 1000003 + ci)
-        d_in = torch.randint(-(1 << 63), (1 << 63) - 1, (tot,), dtype=torch.int64, device=dev,
-                             generator=gen)
+        d_in = operands(idx, lambda k: reqs[k][1] + reqs[k][2])
         d_out = torch.empty(tot, dtype=torch.int64, device=dev)
         rq, off, offs = [], 0, []
         for k in idx:
@@ -112,6 +139,44 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27
         res["mpn_limbs"] += tot
         res["mpn_requests"] += len(idx)
 
+    # flagged mpn requests: one list call per chunk, queued by native code
+    if mpn_list:
+        big = max(mpn_list, key=lambda k: reqs[k][1] + reqs[k][2])
+        an, bn = reqs[big][1], reqs[big][2]
+        ta = torch.zeros(an + bn, dtype=torch.int64, device=dev)
+        tz = torch.empty(an + bn, dtype=torch.int64, device=dev)
+        ctx.mpn_mul_device_list([MulReq(tz.data_ptr(), ta.data_ptr(), an, ta.data_ptr() + 8 * an, bn)],
+                                [configs[big]], s)      # scratch sized outside the timing
+        stream.synchronize()
+        del ta, tz
+    for ci, idx in enumerate(_chunks(mpn_list, lambda k: reqs[k][1] + reqs[k][2], chunk_limbs)):
+        tot = sum(reqs[k][1] + reqs[k][2] for k in idx)
+        d_in = operands(idx, lambda k: reqs[k][1] + reqs[k][2])
+        d_out = torch.empty(tot, dtype=torch.int64, device=dev)
+        lst, offs, off = [], [], 0
+        for k in idx:
+            an, bn = reqs[k][1], reqs[k][2]
+            p = d_in.data_ptr() + 8 * off
+            lst.append(MulReq(d_out.data_ptr() + 8 * off, p, an, p + 8 * an, bn))
+            offs.append(off)
+            off += an + bn
+        ev0.record(stream)
+        ctx.mpn_mul_device_list(lst, [configs[k] for k in idx], s)
+        ev1.record(stream)
+        ev1.synchronize()
+        res["mpn_ms"] += ev0.elapsed_time(ev1)
+        dg = _digests(torch, d_out, offs, [reqs[k][1] + reqs[k][2] for k in idx], weights)
+        digests[idx] = dg.cpu().numpy()
+        if keep:
+            for k, o in zip(idx, offs):
+                if k in keep:
+                    an, bn = reqs[k][1], reqs[k][2]
+                    res["kept"][k] = (d_in[o:o + an + bn].cpu().numpy().view(np.uint64).copy(),
+                                      d_out[o:o + an + bn].cpu().numpy().view(np.uint64).copy())
+        res["mpn_limbs"] += tot
+        res["mpn_requests"] += len(idx)
+        res["mpn_listed_requests"] = res.get("mpn_listed_requests", 0) + len(idx)
+
     if fz:
         # size the context's scratch for the stream's largest integer-polynomial
         # product outside the timing (one untimed product)
@@ -132,10 +197,8 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27
     for ci, idx in enumerate(_chunks(fz, fz_size, chunk_limbs)):
         tin = sum(reqs[k][1] * reqs[k][3] + reqs[k][2] * reqs[k][4] for k in idx)
         tout = sum((reqs[k][1] + reqs[k][2] - 1) * (reqs[k][3] + reqs[k][4] + 1) for k in idx)
-        gen.manual_seed(seed * 1000003 + 500009 + ci)
         # coefficients of w limbs uniform in (-2^(64w-1), 2^(64w-1)): bits = 64w - 1
-        d_in = torch.randint(-(1 << 63), (1 << 63) - 1, (tin,), dtype=torch.int64, device=dev,
-                             generator=gen)
+        d_in = operands(idx, lambda k: reqs[k][1] * reqs[k][3] + reqs[k][2] * reqs[k][4])
         d_out = torch.empty(tout, dtype=torch.int64, device=dev)
         lst, ins, outs, zlens = [], [], [], []
         oi = oo = 0

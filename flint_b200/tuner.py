@@ -9,6 +9,9 @@ choice per request is a gpu_mul_config:
     np      prime count (the minimum, or one more)
     logM    transform length (the minimum, or twice it)
     logC    four-step row length (the longest allowed, or 2x / 4x / 8x shorter)
+    flags   THREE: a 3 2^(logM-2)-point transform (radix-3 column stage) where
+            the product fits it; SPLIT: chunks of the long operand against one
+            transform of the short one (unbalanced products)
 
 Every valid configuration gives the same exact product; only time differs.
 
@@ -20,7 +23,12 @@ Every valid configuration gives the same exact product; only time differs.
   the library's own CUDA training and inference kernels) that predicts the
   log device time of (request, configuration); ``choose`` takes the argmin
   over a request's candidates in one batched forward pass;
-* ``regret`` compares chosen configurations with the exhaustive optimum.
+* ``regret`` compares chosen configurations with the exhaustive optimum;
+* ``reference_rule`` is the reference's own profile choice
+  (mpn_ctx_best_profile, src/fft_small/mpn_mul.c:1248-1340) ported to this
+  configuration space: the least score (1 - ratio/4) np depth L_t over single
+  transforms, L_t the transform's points (truncated where a 3 2^k length
+  fits), depth = ceil(log2 L_t), ratio = L_t / 2^depth.
 
 A request is (kind, an, bn, aw, bw): kind 0 is an mpn product of an x bn
 limbs (aw = bw = 1), kind 1 an integer-polynomial product of an x bn
@@ -30,10 +38,12 @@ import math
 
 import numpy as np
 
-from . import (MulConfig, ROUTE_BASECASE, ROUTE_NTT, GpuFftSmallError, Mlp, resolve_config)
+from . import (FLAG_SPLIT, FLAG_THREE, MulConfig, ROUTE_BASECASE, ROUTE_NTT, GpuFftSmallError, Mlp,
+               resolve_config)
+from . import reference_rule as _reference_rule
 
 BASECASE_MAX = 1024
-N_FEATURES = 16
+N_FEATURES = 18
 
 
 def _req(r):
@@ -50,8 +60,10 @@ def default_config(r):
     return resolve_config(kind, an, bn, None, aw, bw)
 
 
-def candidates(r):
-    """All configurations the tuner considers for request r (resolved)."""
+def candidates(r, flags=True):
+    """All configurations the tuner considers for request r (resolved).
+    flags=False leaves out the THREE / SPLIT configurations (planned batches
+    run every class with plain transforms)."""
     kind, an, bn, aw, bw = _req(r)
     base = default_config(r)
     out = []
@@ -67,7 +79,32 @@ def candidates(r):
                     out.append(resolve_config(kind, an, bn, c, aw, bw))
                 except GpuFftSmallError:
                     pass
+    if flags and kind == 0:
+        for fl in (FLAG_THREE, FLAG_SPLIT):
+            try:
+                out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, base.np, base.logM, 0, fl)))
+            except GpuFftSmallError:
+                pass
     return out
+
+
+def transform_points(cfg):
+    """Points of the transform a resolved configuration runs (one transform;
+    a split product's chunks are not counted)."""
+    if cfg.route != ROUTE_NTT:
+        return 0
+    return 3 << (cfg.logM - 2) if cfg.flags & FLAG_THREE else 1 << cfg.logM
+
+
+def reference_rule(r):
+    """The reference's profile choice (mpn_ctx_best_profile,
+    src/fft_small/mpn_mul.c:1248-1340) in this configuration space, from the
+    library's host-C port (gpu_mul_reference_rule): the least score
+    (1 - ratio/4) np depth L_t over single transforms with the longest rows,
+    L_t the transform's points (3 2^k where the product fits), depth =
+    ceil(log2 L_t), ratio = L_t / 2^depth."""
+    kind, an, bn, aw, bw = _req(r)
+    return _reference_rule(kind, an, bn, aw, bw)
 
 
 def features(r, cfg):
@@ -89,12 +126,15 @@ def features(r, cfg):
     if bc:
         f[9] = math.log2(an * bn) / 44
     else:
+        lt = math.log2(transform_points(cfg))
         f[10] = cfg.np - base.np
         f[11] = cfg.logM - base.logM
-        f[12] = cfg.logM / 25
+        f[12] = lt / 25
         f[13] = cfg.logC / 14
-        f[14] = (cfg.logM - cfg.logC) / 11
-        f[15] = math.log2(pts) / 25 - cfg.logM / 25
+        f[14] = (lt - cfg.logC) / 11
+        f[15] = math.log2(pts) / 25 - lt / 25
+        f[16] = 1.0 if cfg.flags & FLAG_THREE else 0.0
+        f[17] = 1.0 if cfg.flags & FLAG_SPLIT else 0.0
     return f
 
 
@@ -122,18 +162,20 @@ class Autotuner:
         kind, an, bn, aw, bw = _req(r)
         key = (kind, an, bn, aw, bw, cfg.key())
         if key not in self.cache:
-            if self.batched and kind == 0:
+            # planned batches take no flags: such configurations run per
+            # instance, so they are timed alone
+            if self.batched and kind == 0 and not cfg.flags:
                 self.cache[key] = self.ctx.time_batched(an, bn, cfg, batch_copies(an, bn), self.reps)
             else:
                 self.cache[key] = self.ctx.time_config(kind, an, bn, cfg, aw, bw, self.reps)
         return self.cache[key]
 
-    def table(self, r):
+    def table(self, r, flags=True):
         """[(cfg, ms)] for every candidate of r."""
-        return [(c, self.time(r, c)) for c in candidates(r)]
+        return [(c, self.time(r, c)) for c in candidates(r, flags)]
 
-    def best(self, r):
-        return min(self.table(r), key=lambda x: x[1])
+    def best(self, r, flags=True):
+        return min(self.table(r, flags), key=lambda x: x[1])
 
 
 def dataset(tuner, reqs):
@@ -161,9 +203,10 @@ class CostModel:
     def fit(self, X, t, epochs=300, batch=256, lr=2e-3, seed=7):
         return self.net.train(X, t, epochs=epochs, batch=batch, lr=lr, seed=seed)
 
-    def choose(self, reqs):
-        """Chosen configuration per request (one batched forward pass)."""
-        cands = [candidates(r) for r in reqs]
+    def choose(self, reqs, flags=True):
+        """Chosen configuration per request (one batched forward pass);
+        flags=False chooses among plain transforms only (planned batches)."""
+        cands = [candidates(r, flags) for r in reqs]
         rows = [features(r, c) for r, cs in zip(reqs, cands) for c in cs]
         pred = self.net.predict(np.array(rows, dtype=np.float32))
         keep = math.log(1.0 - self.margin) if self.margin > 0 else 0.0
@@ -181,24 +224,32 @@ class CostModel:
         return out
 
 
-def regret(tuner, reqs, chosen):
-    """Per-request regret t(chosen) / t(best) - 1 against the exhaustive tuner,
-    and the total-time ratios of the default rule and of the choices."""
-    reg, t_best, t_chosen, t_default = [], 0.0, 0.0, 0.0
+def regret(tuner, reqs, chosen, flags=True):
+    """Per-request regret t(chosen) / t(best) - 1 against the exhaustive tuner
+    (over the same candidate space, flags as for candidates), and the
+    total-time ratios of the fixed rule, of the reference's rule
+    (reference_rule; flags=False keeps it to plain transforms) and of the
+    choices."""
+    reg, t_best, t_chosen, t_default, t_ref = [], 0.0, 0.0, 0.0, 0.0
     for r, c in zip(reqs, chosen):
-        _, b = tuner.best(r)
+        _, b = tuner.best(r, flags)
         tc = tuner.time(r, c)
         td = tuner.time(r, default_config(r))
+        rc = reference_rule(r) if flags else default_config(r)
+        tr = tuner.time(r, rc)
         reg.append(tc / b - 1.0)
         t_best += b
         t_chosen += tc
         t_default += td
+        t_ref += tr
     reg = np.array(reg)
     return {
         "requests": len(reqs),
         "mean_regret": float(reg.mean()), "median_regret": float(np.median(reg)),
         "p90_regret": float(np.quantile(reg, 0.9)), "max_regret": float(reg.max()),
         "total_ms_best": t_best, "total_ms_chosen": t_chosen, "total_ms_default": t_default,
+        "total_ms_reference_rule": t_ref,
         "gain_over_default": t_default / t_chosen,
+        "gain_over_reference_rule": t_ref / t_chosen,
         "total_regret": t_chosen / t_best - 1.0,
     }

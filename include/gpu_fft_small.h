@@ -388,7 +388,18 @@ typedef struct {
     int logM;    /* transform length 2^logM, minimal .. 2^25 */
     int logC;    /* four-step row length 2^logC, max(5, logM - 11) .. min(logM, 14); below
                     2^14 points at most 16 columns (logC >= logM - 4) */
+    int flags;   /* GPU_MUL_FLAG_*: 0 = one transform of 2^logM points */
 } gpu_mul_config;
+/* flags of a transform configuration (whole products on device pointers,
+   gpu_mpn_mul_device_config and the per-instance list; planned batches take
+   flags = 0):
+   THREE: run a transform of 3 2^(logM - 2) points (valid when the product
+     fits it, five primes, 2^18 <= 3 2^(logM - 2) / 3 <= 2^23; rows of 2^13);
+   SPLIT: run the product as chunks of the long operand against one
+     transform of the short one, chunk length by the default rule (valid when
+     that rule splits the product). */
+#define GPU_MUL_FLAG_THREE 1
+#define GPU_MUL_FLAG_SPLIT 2
 
 /* Fills the zero fields of cfg with the defaults for an an x bn product and
    checks the rest; returns 0 or GPU_FFT_SMALL_EINVAL naming the bad field. */
@@ -397,6 +408,18 @@ GPU_FFT_SMALL_API int gpu_mpn_mul_config_resolve(gpu_ulong an, gpu_ulong bn, gpu
 GPU_FFT_SMALL_API int gpu_mpn_mul_device_config(gpu_mpn_ctx_t R, uint64_t *z_dev, const uint64_t *a_dev,
                                                 gpu_ulong an, const uint64_t *b_dev, gpu_ulong bn,
                                                 const gpu_mul_config *cfg, void *stream);
+
+/* The configuration the reference's own profile choice would make
+   (mpn_ctx_best_profile, src/fft_small/mpn_mul.c:1248-1340, ported to this
+   configuration space): among single transforms with the longest rows --
+   the fewest primes or one more, the shortest power-of-two length or the
+   3 2^k length where the product fits it -- the least score
+   (1 - ratio / 4) np depth L_t (L_t the transform's points,
+   depth = ceil(log2 L_t), ratio = L_t / 2^depth).  kind 0: an x bn limbs
+   (aw, bw ignored); kind 1: integer polynomials of aw- and bw-limb
+   coefficients.  The autotuner's "method without the model" baseline. */
+GPU_FFT_SMALL_API int gpu_mul_reference_rule(int kind, gpu_ulong an, gpu_ulong aw, gpu_ulong bn,
+                                             gpu_ulong bw, gpu_mul_config *cfg);
 
 /* Integer-polynomial counterparts (raw coefficient rows, transform route;
    the window must lie inside the product). */

@@ -72,3 +72,22 @@ def test_learned_schedule_regret_and_gain(ctx):
     print("learned schedule:", rep)
     assert rep["gain_over_default"] > 1.0
     assert rep["total_regret"] < 0.25
+
+
+def test_learned_schedule_gain_over_reference_rule(ctx):
+    """The method without the model, as the reference makes it: its own
+    profile choice (mpn_ctx_best_profile, ported to host C as
+    gpu_mul_reference_rule).  On held-out requests that include products
+    above 2^19 coefficients (where 3 2^k lengths and split products apply),
+    the trained model takes less total time than that rule."""
+    reqs = request_stream(2031, 200, mpn_log=(10.0, 21.0), mpn_ratio_log=(0.0, 5.0),
+                          fmpz_len_log=(8.0, 12.0), fmpz_bits=(64, 1024))
+    train, test = reqs[:150], reqs[150:]
+    tun = tuner.Autotuner(ctx, reps=3)
+    X, t = tuner.dataset(tun, train)
+    model = tuner.CostModel(seed=13)
+    model.fit(X, t, epochs=400, batch=256, lr=2e-3)
+    rep = tuner.regret(tun, test, model.choose(test))
+    print("learned vs reference rule:", rep)
+    assert rep["gain_over_reference_rule"] > 1.0
+    assert rep["total_regret"] < 0.25

@@ -47,9 +47,9 @@ def test_invalid_configs_are_rejected():
         FB.resolve_config(0, 600, 500, FB.MulConfig(FB.ROUTE_NTT, 0, 11, 5))          # 32 below 2^14
     assert FB.resolve_config(0, 600, 500, FB.MulConfig(FB.ROUTE_NTT, 0, 11, 7)).logC == 7
     c = FB.resolve_config(0, 1 << 20, 1 << 20)
-    assert c.key() == (FB.ROUTE_NTT, 5, 21, 13)       # 2^13-point rows from 2^15 to 2^24
-    assert FB.resolve_config(0, 1 << 24, 1 << 24).key() == (FB.ROUTE_NTT, 5, 25, 14)
-    assert FB.resolve_config(0, 5000, 3000).key() == (FB.ROUTE_NTT, 5, 13, 13)
+    assert c.key() == (FB.ROUTE_NTT, 5, 21, 13, 0)       # 2^13-point rows from 2^15 to 2^24
+    assert FB.resolve_config(0, 1 << 24, 1 << 24).key() == (FB.ROUTE_NTT, 5, 25, 14, 0)
+    assert FB.resolve_config(0, 5000, 3000).key() == (FB.ROUTE_NTT, 5, 13, 13, 0)
 
 
 def test_request_stream_shape():
@@ -65,3 +65,30 @@ def test_request_stream_shape():
     ws = [r[3] for r in fz]
     assert min(ws) >= 2 and max(ws) <= 65
     assert all(2 ** 8 - 1 <= r[1] <= 2 ** 16 + 1 and 2 ** 8 - 1 <= r[2] <= 2 ** 16 + 1 for r in fz)
+
+
+def test_configuration_flags():
+    """THREE and SPLIT resolve where the product allows them and are refused
+    elsewhere; the reference rule (host-C port of mpn_ctx_best_profile) takes
+    the 3 2^k length where it fits."""
+    three = FB.resolve_config(0, 3 << 22, 3 << 22, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE))
+    assert three.key() == (FB.ROUTE_NTT, 5, 25, 13, FB.FLAG_THREE)
+    assert FB.resolve_config(0, 1 << 24, 1 << 20,
+                             FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_SPLIT)).flags == FB.FLAG_SPLIT
+    for an, bn, fl in [(1 << 24, 1 << 24, FB.FLAG_THREE),        # L = 2^25 - 1: no 3 2^23 fit
+                       (1000, 1000, FB.FLAG_THREE),               # below the radix-3 kernels
+                       (3 << 22, 3 << 22, FB.FLAG_THREE | FB.FLAG_SPLIT),
+                       (1 << 20, 1 << 20, FB.FLAG_SPLIT),         # balanced: does not split
+                       (100, 100, 8)]:                            # unknown flag
+        with pytest.raises(FB.GpuFftSmallError):
+            FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, fl))
+    with pytest.raises(FB.GpuFftSmallError):                     # six primes: no cube roots
+        FB.resolve_config(0, 3 << 22, 3 << 22, FB.MulConfig(FB.ROUTE_NTT, 6, 0, 0, FB.FLAG_THREE))
+    with pytest.raises(FB.GpuFftSmallError):                     # integer polynomials take none
+        FB.resolve_config(1, 300, 200, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE), 2, 2)
+    assert tuner.reference_rule((0, 3 << 22, 3 << 22)).flags == FB.FLAG_THREE
+    assert tuner.reference_rule((0, 1 << 24, 1 << 24)).key() == (FB.ROUTE_NTT, 5, 25, 14, 0)
+    assert tuner.reference_rule((1, 300, 200, 3, 3)).flags == 0
+    keys = [c.key() for c in tuner.candidates((0, 3 << 22, 3 << 22))]
+    assert (FB.ROUTE_NTT, 5, 25, 13, FB.FLAG_THREE) in keys
+    assert all(c.flags == 0 for c in tuner.candidates((0, 3 << 22, 3 << 22), flags=False))
