@@ -91,7 +91,7 @@ class MulConfig(ctypes.Structure):
 
 
 ROUTE_NTT, ROUTE_BASECASE = 0, 1
-FLAG_THREE, FLAG_SPLIT = 1, 2
+FLAG_THREE, FLAG_SPLIT, FLAG_ROWS16, FLAG_ROWS32 = 1, 2, 4, 8
 
 
 class BatchOptions(ctypes.Structure):

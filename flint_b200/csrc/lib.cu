@@ -451,6 +451,14 @@ static const fwd_cols_fn FWD_COLS_FZ_C13[3] = {k_fwd_cols<9, tmpl_cols<9>(), tru
 static const inv_cols_fn INV_COLS_C13[3] = {k_inv_cols<9, tmpl_cols<9>(), 13>,
                                             k_inv_cols<10, tmpl_cols<10>(), 13>,
                                             k_inv_cols<11, tmpl_cols<11>(), 13>};
+// narrow tiles (a quarter of the columns, 128 threads) for columns of 2^5 to
+// 2^8 points (index logR - 5): small transforms get four times the CTAs
+static const fwd_cols_fn FWD_COLS_S[4] = {k_fwd_cols<5, cols_per_tile(5) / 4, false>,
+                                          k_fwd_cols<6, cols_per_tile(6) / 4, false>,
+                                          k_fwd_cols<7, cols_per_tile(7) / 4, false>,
+                                          k_fwd_cols<8, cols_per_tile(8) / 4, false>};
+static const inv_cols_fn INV_COLS_S[4] = {k_inv_cols<5, cols_per_tile(5) / 4>, k_inv_cols<6, cols_per_tile(6) / 4>,
+                                          k_inv_cols<7, cols_per_tile(7) / 4>, k_inv_cols<8, cols_per_tile(8) / 4>};
 static const fwd_cols_fn FWD_COLS_C14 = k_fwd_cols<11, tmpl_cols<11>(), false, 14>;
 static const fwd_cols_fn FWD_COLS_FZ_C14 = k_fwd_cols<11, tmpl_cols<11>(), true, 14>;
 static const inv_cols_fn INV_COLS_C14 = k_inv_cols<11, tmpl_cols<11>(), 14>;
@@ -480,15 +488,18 @@ static inv_cols_fn inv_cols_kernel(int logR, int logC)
     if (logR >= 9 && logR <= 11 && logC == 13) return INV_COLS_C13[logR - 9];
     return INV_COLS[logR];
 }
-// Rows run with 32 elements per thread (k_rows<LOGC, 5>).  The kernel also
-// builds with 16 per thread (k_rows<14, 4>: 1024 threads, 32 warps per SM, 64
-// registers); measured on the 2^24 product that is slower (1.88 against
-// 1.74 ms: one more shared-memory pass, and the register cap), so the
-// dispatch keeps 32.
+// Rows run with 32 elements per thread (k_rows<LOGC, 5>) or 16 (k_rows<LOGC,
+// 4>: twice the threads, 64 registers).  On the 2^24 product 16 is slower
+// (1.88 against 1.74 ms: one more shared-memory pass, and the register cap);
+// small transforms, whose row launch has only a few warps per SM and runs
+// latency-bound, take 16 (rows_loge).
 static const rows_fn ROWS[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
                                  k_rows<5>, k_rows<6>, k_rows<7>, k_rows<8>, k_rows<9>,
                                  k_rows<10>, k_rows<11>, k_rows<12>, k_rows<13>, k_rows<14>};
-static int row_loge(int) { return 5; }
+constexpr int ROWS16_MIN_LOGC = 9;
+static const rows_fn ROWS16[15] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                   nullptr, k_rows<9, 4>, k_rows<10, 4>, k_rows<11, 4>, k_rows<12, 4>,
+                                   k_rows<13, 4>, k_rows<14, 4>};
 #undef FB_COLS
 typedef void (*rows_op_fn)(DevTables, uint32_t *, int, int, int, int);
 static const rows_op_fn ROWS_FWD[15] = {nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -506,21 +517,26 @@ struct LaunchShape {
     MulShape S;
     int col_threads, col_grid;   // column kernels
     size_t col_smem;
-    int nv, row_threads, row_grid;
+    int nv, row_threads, row_grid;   // row_threads: at 32 elements per thread
     size_t row_smem;
+    int loge = 0;                    // row elements per thread 2^loge; 0: rows_loge's rule
 };
 
 // Four-step split of a 2^logM transform: rows of 2^logC, columns of
 // 2^(logM - logC); logC < 0 takes the longest rows (2^14), which leaves the
 // shortest columns.
 constexpr int LOG_MAXR = 11;
-// Default row length: the whole transform up to 2^14 points, 2^13-point rows
-// from 2^15 to 2^24 (more row items for mid sizes; measured 10-20% faster
-// products from 2^16 to 2^20 points and equal above), 2^14 at 2^25 where the
-// columns reach their longest length.
+// Default row length: the whole transform up to 2^13 points; 2^5-point
+// columns from 2^14 to 2^17 points and 2^6 at 2^18 (small transforms are
+// latency-bound, and 32-point columns spread a product over the most CTAs:
+// measured 2^15-point products 0.056 -> 0.030 ms, 2^17-point 0.062 -> 0.038
+// ms); 2^13-point rows from 2^19 to 2^24 (more row items for mid sizes), 2^14
+// at 2^25 where the columns reach their longest length.
 static int default_logC(int logM)
 {
-    if (logM <= LOG_MAXC) return logM;
+    if (logM <= LOG_MAXC - 1) return logM;
+    if (logM <= 17) return logM - 5;
+    if (logM == 18) return 12;
     return std::max(LOG_MAXC - 1, logM - LOG_MAXR);
 }
 // Shortest row for a transform of 2^logM points: columns at most 2^11 long,
@@ -558,7 +574,7 @@ static LaunchShape make_shape(int logM, int logC = -1)
     // 13% faster than two per CTA; 2^12-point rows two per CTA 6% faster than
     // four)
     L.nv = std::min(R, 1 << std::max(0, LOG_MAXC - 1 - L.S.logC));
-    L.row_threads = (L.nv * C) >> row_loge(L.S.logC);
+    L.row_threads = (L.nv * C) >> 5;
     L.row_grid = (R + L.nv - 1) / L.nv;                // items per prime; launch clamps
     L.row_smem = (size_t)3 * L.nv * padw(C) * sizeof(uint32_t);   // b and two a buffers
     return L;
@@ -598,6 +614,8 @@ static int configure_kernels()
         CU(cudaFuncSetAttribute(FWD_COLS3[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
         CU(cudaFuncSetAttribute(INV_COLS3[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
+    for (int c = ROWS16_MIN_LOGC; c <= LOG_MAXC; c++)
+        CU(cudaFuncSetAttribute(ROWS16[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     for (int c = 5; c <= LOG_MAXC; c++) {
         CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
         CU(cudaFuncSetAttribute(ROWS_FWD[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
@@ -770,8 +788,15 @@ static int plan_mpn_cfg(uint64_t an, uint64_t bn, const gpu_mul_config *cfg, Mul
     if (!(fl & GPU_MUL_FLAG_THREE) && !valid_logC(P->logM, logC))
         return set_error(GPU_FFT_SMALL_EINVAL, "row length 2^%d invalid for a 2^%d transform", logC, P->logM);
     P->L = make_shape(P->logM, (fl & GPU_MUL_FLAG_THREE) ? -1 : logC);
-    if (fl & ~(GPU_MUL_FLAG_THREE | GPU_MUL_FLAG_SPLIT))
+    if (fl & ~(GPU_MUL_FLAG_THREE | GPU_MUL_FLAG_SPLIT | GPU_MUL_FLAG_ROWS16 | GPU_MUL_FLAG_ROWS32))
         return set_error(GPU_FFT_SMALL_EINVAL, "unknown configuration flags 0x%x", fl);
+    if ((fl & GPU_MUL_FLAG_ROWS16) && (fl & GPU_MUL_FLAG_ROWS32))
+        return set_error(GPU_FFT_SMALL_EINVAL, "ROWS16 and ROWS32 exclude each other");
+    if ((fl & GPU_MUL_FLAG_ROWS16) && ((fl & (GPU_MUL_FLAG_THREE | GPU_MUL_FLAG_SPLIT)) || logC < ROWS16_MIN_LOGC))
+        return set_error(GPU_FFT_SMALL_EINVAL, "16 points per thread need rows of 2^%d points or more "
+                         "and neither THREE nor SPLIT", ROWS16_MIN_LOGC);
+    if (fl & GPU_MUL_FLAG_ROWS16) P->L.loge = 4;
+    if (fl & GPU_MUL_FLAG_ROWS32) P->L.loge = 5;
     if ((fl & GPU_MUL_FLAG_THREE) && (fl & GPU_MUL_FLAG_SPLIT))
         return set_error(GPU_FFT_SMALL_EINVAL, "THREE and SPLIT exclude each other");
     if ((fl & GPU_MUL_FLAG_THREE) && !three_length(an + bn - 1, P->np, P->logM))
@@ -871,18 +896,61 @@ static int upload_scales(Ctx *X)
 // Resident row CTAs per SM for a shape: 1 for long rows (512 threads, ~135 KB
 // of shared memory), several for short ones.  The row launch depends on the
 // row length and the rows per item.
-static int rows_per_sm(const LaunchShape &L)
+static int rows_per_sm(const LaunchShape &L, int loge = 5)
 {
-    static int occ[LOG_MAXC + 1][LOG_MAXC + 1] = {{0}};
-    const int c = L.S.logC, v = __builtin_ctz((unsigned)L.nv);
-    if (occ[c][v] == 0) {
+    static int occ[2][LOG_MAXC + 1][LOG_MAXC + 1] = {{{0}}};
+    const int c = L.S.logC, v = __builtin_ctz((unsigned)L.nv), e = loge == 4;
+    if (occ[e][c][v] == 0) {
         int n = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, ROWS[c], L.row_threads, L.row_smem) !=
-                cudaSuccess || n < 1)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, e ? ROWS16[c] : ROWS[c], (L.nv << c) >> loge,
+                                                          L.row_smem) != cudaSuccess || n < 1)
             n = 1;
-        occ[c][v] = n;
+        occ[e][c][v] = n;
     }
-    return occ[c][v];
+    return occ[e][c][v];
+}
+
+// Row elements per thread (log2) for a launch of ninst products of np primes:
+// the shape's choice, else 16 where 32 would give the launch fewer than 16
+// warps per SM (measured on 2^15- to 2^18-point products, whose row items
+// run latency-bound at 8 warps per CTA), else 32.
+static int rows_loge(const Ctx *X, const LaunchShape &L, int np, int ninst)
+{
+    if (L.loge) return L.loge;
+    if (L.S.logC < ROWS16_MIN_LOGC) return 5;
+    const uint64_t warps = ((uint64_t)np * (uint64_t)ninst << (L.S.logR + L.S.logC)) >> 10;
+    return warps < (uint64_t)X->nsm * 16 ? 4 : 5;
+}
+
+// A column launch: the shape's 2^14-word tiles, or narrow ones (a quarter of
+// the columns) where the launch would have fewer than two CTAs per SM --
+// small transforms, whose column passes are bound by latency, not by HBM.
+struct ColLaunch {
+    int G, grid, threads;
+    size_t smem;
+    bool narrow;
+};
+static ColLaunch col_launch(const Ctx *X, const LaunchShape &L, int np, int zdim, bool fz)
+{
+    const MulShape &S = L.S;
+    ColLaunch c{S.G, L.col_grid, L.col_threads, L.col_smem, false};
+    const int64_t want = 2 * (int64_t)X->nsm;
+    if (!fz && S.logR >= 5 && S.logR <= 8 && (int64_t)L.col_grid * np * zdim < want) {
+        c.G = S.G / 4;
+        c.grid = L.col_grid * 4;
+        c.threads = L.col_threads / 4;
+        c.smem = (size_t)(padw((1 << S.logR) * c.G) + 32) * sizeof(uint32_t);
+        c.narrow = true;
+    } else if (S.logR < 5) {
+        // short columns (one thread per column, tile width at run time):
+        // halve the tile down to 128 columns
+        const int C = 1 << S.logC;
+        while (c.G > 128 && (int64_t)(C / c.G) * np * zdim < want) c.G >>= 1;
+        c.grid = C / c.G;
+        c.threads = std::min(512, c.G);
+        c.smem = (size_t)(padw((1 << S.logR) * c.G) + 32) * sizeof(uint32_t);
+    }
+    return c;
 }
 
 static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
@@ -893,6 +961,11 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
 {
     const MulShape &S = L.S;
     const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
+    const int ni = desc ? ninst : 1;
+    const ColLaunch cf = col_launch(X, L, np, zdim, fz != nullptr);
+    const ColLaunch ci = col_launch(X, L, np, ni, false);
+    const fwd_cols_fn fwd = cf.narrow ? FWD_COLS_S[S.logR - 5] : fwd_cols_kernel(S.logR, S.logC, fz != nullptr);
+    const inv_cols_fn inv = ci.narrow ? INV_COLS_S[S.logR - 5] : inv_cols_kernel(S.logR, S.logC);
     const FzShape shape = fz ? *fz : FzShape{1, 1, 1};
     // Products of two operands whose columns are long enough for the
     // per-thread twist (2^5 points or more) fold the pointwise scale into
@@ -901,26 +974,34 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     const bool fold = !(sq && !desc) && S.logR >= 5;
     if (b_ready && !desc && !sq) {
         // b is still arriving: a's column pass first, b's after its copy
-        fwd_cols_kernel(S.logR, S.logC, fz != nullptr)<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
-            X->T, a, an, a, an, ra, ra, S.logC, S.G, nullptr, np, shape, d_scale, 0);
+        fwd<<<dim3(np, cf.grid, 1), cf.threads, cf.smem, st>>>(X->T, a, an, a, an, ra, ra, S.logC, cf.G, nullptr,
+                                                               np, shape, d_scale, 0);
         cudaStreamWaitEvent(st, b_ready, 0);
         const FzShape shb = fz ? FzShape{shape.S, shape.wb, shape.wb} : shape;
-        fwd_cols_kernel(S.logR, S.logC, fz != nullptr)<<<dim3(np, L.col_grid, 1), L.col_threads, L.col_smem, st>>>(
-            X->T, b, bn, b, bn, rb, rb, S.logC, S.G, nullptr, np, shb, d_scale, fold ? 1 : 0);
+        fwd<<<dim3(np, cf.grid, 1), cf.threads, cf.smem, st>>>(X->T, b, bn, b, bn, rb, rb, S.logC, cf.G, nullptr,
+                                                               np, shb, d_scale, fold ? 1 : 0);
     } else {
         if (b_ready) cudaStreamWaitEvent(st, b_ready, 0);
-        fwd_cols_kernel(S.logR, S.logC, fz != nullptr)<<<dim3(np, L.col_grid, zdim), L.col_threads, L.col_smem, st>>>(
-            X->T, a, an, b, bn, ra, rb, S.logC, S.G, desc, np, shape, d_scale, fold ? 2 : 0);
+        fwd<<<dim3(np, cf.grid, zdim), cf.threads, cf.smem, st>>>(X->T, a, an, b, bn, ra, rb, S.logC, cf.G, desc,
+                                                                  np, shape, d_scale, fold ? 2 : 0);
     }
     timing_mark(tr, 1, st);
-    const int items = L.row_grid * np * (desc ? ninst : 1);
-    ROWS[S.logC]<<<std::min(items, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
-        X->T, ra, rb, S.logR, L.nv, np, fold ? nullptr : d_scale, (sq && !desc) ? 1 : 0, desc,
-        desc ? ninst : 1, 1 << S.logR);
+    // rows per item: the shape's (up to 2^13 points per CTA), halved while the
+    // launch would have fewer than two items per SM (small transforms)
+    LaunchShape Lr = L;
+    const int R = 1 << S.logR;
+    while (Lr.nv > 1 && (int64_t)(R / Lr.nv) * np * ni < 2 * (int64_t)X->nsm) Lr.nv >>= 1;
+    Lr.row_grid = (R + Lr.nv - 1) / Lr.nv;
+    Lr.row_smem = (size_t)3 * Lr.nv * padw(1 << S.logC) * sizeof(uint32_t);
+    const int items = Lr.row_grid * np * ni;
+    const int loge = rows_loge(X, Lr, np, ni);
+    (loge == 4 ? ROWS16 : ROWS)[S.logC]<<<std::min(items, X->nsm * rows_per_sm(Lr, loge)),
+                                         (Lr.nv << S.logC) >> loge, Lr.row_smem, st>>>(
+        X->T, ra, rb, S.logR, Lr.nv, np, fold ? nullptr : d_scale, (sq && !desc) ? 1 : 0, desc, ni, R);
     timing_mark(tr, 2, st);
     if (S.logR > 0)
-        inv_cols_kernel(S.logR, S.logC)<<<dim3(L.col_grid, np, desc ? ninst : 1), L.col_threads, L.col_smem, st>>>(
-            X->T, ra, S.logC, S.G, desc, co ? *co : ChunkOut{nullptr, 0, 0, 0, 0});
+        inv<<<dim3(ci.grid, np, ni), ci.threads, ci.smem, st>>>(X->T, ra, S.logC, ci.G, desc,
+                                                                co ? *co : ChunkOut{nullptr, 0, 0, 0, 0});
     timing_mark(tr, 3, st);
 }
 
@@ -1121,8 +1202,10 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     if (lo > 0 && !(cfg && cfg->logM)) {
         const int lw = window_logM(an, bn, lo, hi);
         if (lw < P.logM) {
+            const int loge = P.L.loge;
             P.logM = lw;
             P.L = make_shape(lw, cfg && cfg->logC && valid_logC(lw, cfg->logC) ? cfg->logC : -1);
+            if (P.L.S.logC >= ROWS16_MIN_LOGC) P.L.loge = loge;
         }
     }
     const bool sq = (a == b) && (an == bn);
@@ -2450,6 +2533,8 @@ static int na_setup(int dev, NaDevice &D)
     }
     for (int c = 5; c <= LOG_MAXC; c++)
         NA_CU(cudaFuncSetAttribute(ROWS[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
+    for (int c = ROWS16_MIN_LOGC; c <= LOG_MAXC; c++)
+        NA_CU(cudaFuncSetAttribute(ROWS16[c], cudaFuncAttributeMaxDynamicSharedMemorySize, 220 * 1024));
     NA_CU(cudaMemcpyToSymbol(c_na_primes, PRIMES, sizeof(uint32_t) * NA_NP));
     NA_CU(cudaMemcpyToSymbol(c_na_roots, roots, sizeof roots));
     // the module-wide constant tables (all MAX_NP primes), unless a context

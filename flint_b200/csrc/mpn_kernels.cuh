@@ -216,14 +216,18 @@ fwd_cols_body(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
     const uint32_t p = P.p;
     const uint64_t M = (uint64_t)1 << logM;
     const int tot = R * GR;
+    // threads of a tile with columns of 2^5 points or more: one per 32-point
+    // column segment (512 for the 2^14-word tiles, fewer for narrow ones)
+    constexpr int NT = G ? (G * R / 32 < 512 ? G * R / 32 : 512) : 512;
+    constexpr int PNT = NT + NT / 32;     // padw(NT)
 
     if (LOGR >= 5 && (FZ || xn <= M)) {
-        // blockDim == G R / 32 == 512: thread t loads elements t + 512 k, i.e.
-        // rows u_t + k 512/G of its fixed column; shared offsets are constants
+        // blockDim == G R / 32 == NT: thread t loads elements t + NT k, i.e.
+        // rows u_t + k NT/G of its fixed column; shared offsets are constants
         const int t = threadIdx.x;
         const int GG = G ? G : 1;
         const int u_t = t / GG, c = t & (GG - 1);
-        const uint64_t step = (uint64_t)(512 / GG) * C;
+        const uint64_t step = (uint64_t)(NT / GG) * C;
         uint64_t n = (uint64_t)u_t * C + i0 + c;
         uint32_t* d = sm + padw(u_t * GG) + c;
         if constexpr (!FZ && LOGR >= 5) {
@@ -231,8 +235,8 @@ fwd_cols_body(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             // is a shift, and a pointer bump per row keeps the 64-bit address
             // arithmetic off the FMA pipe (measured 1.267 -> 1.249 ms for the
             // two operands of a 2^24 x 2^24 product)
-            constexpr int K = R * GG / 512;
-            const int lstep = (31 - __clz(512 / GG)) + logC;
+            constexpr int K = R * GG / NT;
+            const int lstep = (31 - __clz(NT / GG)) + logC;
             int kin = 0;
             if (n < xn) {
                 const uint64_t q = ((xn - n - 1) >> lstep) + 1;
@@ -241,17 +245,29 @@ fwd_cols_body(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
             const uint64_t* px = x + n;
 #pragma unroll 8
             for (int k = 0; k < K; k++, px += step)
-                d[k * 528] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
+                d[k * PNT] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
         } else {
 #pragma unroll 8
-            for (int k = 0; k < R * GG / 512; k++, n += step)
-                d[k * 528] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
+            for (int k = 0; k < R * GG / NT; k++, n += step)
+                d[k * PNT] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
         }
     } else if (FZ || xn <= M) {
-        for (int f = threadIdx.x; f < tot; f += blockDim.x) {
-            const int u = f / GR, c = f - u * GR;
-            const uint64_t n = (uint64_t)u * C + i0 + c;
-            sm[padw(u * GR) + c] = load_residue<FZ>(x, n, xn, fz.S, xw, P);
+        // four loads in flight per thread (small transforms are bound by
+        // their latency)
+        for (int f0 = threadIdx.x; f0 < tot; f0 += 4 * blockDim.x) {
+            uint32_t v[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int f = f0 + q * (int)blockDim.x;
+                const int u = f / GR, c = f - u * GR;
+                v[q] = f < tot ? load_residue<FZ>(x, (uint64_t)u * C + i0 + c, xn, fz.S, xw, P) : 0u;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int f = f0 + q * (int)blockDim.x;
+                const int u = f / GR, c = f - u * GR;
+                if (f < tot) sm[padw(u * GR) + c] = v[q];
+            }
         }
     } else {
         // cyclic fold: an operand longer than M wraps around (x mod X^M - 1)
@@ -486,8 +502,12 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         uint32_t xr[E];
         uint32_t breg[E];
         if (squaring == 0) {
-            if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all2<LOGC, QMAX, LOGE, true>(sa, sb, nv, twf, p);
-            else gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
+            if constexpr (LOGE == 5) {
+                if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all2<LOGC, QMAX, LOGE, true>(sa, sb, nv, twf, p);
+                else gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
+            } else {
+                gs_strided_all2<LOGC, QMAX, LOGE>(sa, sb, nv, twf, p);
+            }
 #pragma unroll
             for (int m = 0; m < E; m++) {
                 xr[m] = sa[pb + m];
@@ -500,8 +520,12 @@ k_rows(DevTables T, uint32_t* __restrict__ ra, const uint32_t* __restrict__ rb,
         } else {
             // a squaring, or b's rows already hold its spectrum in this
             // kernel's order (squaring == 2: k_rows_fwd output, landed padded)
-            if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all<LOGC, 0, QMAX, LOGE, true>(sa, nv, twf, p);
-            else gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
+            if constexpr (LOGE == 5) {
+                if (rows_unpadded<LOGC, LOGE>(nv)) gs_strided_all<LOGC, 0, QMAX, LOGE, true>(sa, nv, twf, p);
+                else gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
+            } else {
+                gs_strided_all<LOGC, 0, QMAX, LOGE>(sa, nv, twf, p);
+            }
 #pragma unroll
             for (int m = 0; m < E; m++) xr[m] = sa[pb + m];
             gs_contig<LOGE, ROW_GS_FMA_ADDS>(xr, c_w32[j], p);
@@ -612,24 +636,26 @@ inv_cols_body(DevTables T, uint32_t* __restrict__ ra, int logC, int gcols,
         }
         __syncthreads();
         ct_strided_all<LOGR, G>(sm, 1, T.twi + (size_t)j * TW_SZ, p);
-        // blockDim == G R / 32 == 512: thread t stores rows u_t + k 512/G of
+        // blockDim == G R / 32 == NT: thread t stores rows u_t + k NT/G of
         // its column (the inverse of the forward pass's load mapping)
+        constexpr int NT = G * R / 32 < 512 ? G * R / 32 : 512;
+        constexpr int PNT = NT + NT / 32;     // padw(NT)
         const int t = threadIdx.x;
         const int u_t = t / G, c = t & (G - 1);
-        const size_t step = (size_t)(512 / G) * C;
+        const size_t step = (size_t)(NT / G) * C;
         const uint32_t* s_ = sm + padw(u_t * G) + c;
         if (!co.acc) {
             uint32_t* dst = buf + (size_t)u_t * C + i0 + c;
 #pragma unroll 8
-            for (int k = 0; k < R * G / 512; k++) dst[k * step] = s_[k * 528];
+            for (int k = 0; k < R * G / NT; k++) dst[k * step] = s_[k * PNT];
         } else {
             uint32_t* __restrict__ out = co.acc + ((size_t)j << co.logMf) + co.shift;
             const uint64_t n0 = (uint64_t)u_t * C + i0 + c;
 #pragma unroll 8
-            for (int k = 0; k < R * G / 512; k++) {
+            for (int k = 0; k < R * G / NT; k++) {
                 const uint64_t n = n0 + (uint64_t)k * step;
                 if (n < co.nvalid) {
-                    const uint32_t v = s_[k * 528];
+                    const uint32_t v = s_[k * PNT];
                     out[n] = n < co.overlap ? add_mod(out[n], v, p) : v;
                 }
             }

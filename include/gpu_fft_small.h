@@ -379,9 +379,10 @@ GPU_FFT_SMALL_API int gpu_mulmod_2expp1_mul_cached(const gpu_mulmod_2expp1_ctx_s
 
 /* How one product is computed.  Zero fields take the default: the fewest
    primes that hold the coefficient bound, the shortest transform that holds
-   the product, rows of 2^logM points up to 2^14, 2^13-point rows from 2^15
-   to 2^24 points, 2^14 at 2^25.  Any valid choice gives the same
-   (exact) product; only the time differs. */
+   the product, rows of 2^logM points up to 2^13, 32-point columns from 2^14
+   to 2^17 points, 64-point columns at 2^18, 2^13-point rows from 2^19 to
+   2^24 points, 2^14 at 2^25.  Any valid choice gives the same (exact)
+   product; only the time differs. */
 typedef struct {
     int route;   /* GPU_MUL_ROUTE_* */
     int np;      /* primes, minimal .. 6 */
@@ -397,9 +398,15 @@ typedef struct {
      fits it, five primes, 2^18 <= 3 2^(logM - 2) / 3 <= 2^23; rows of 2^13);
    SPLIT: run the product as chunks of the long operand against one
      transform of the short one, chunk length by the default rule (valid when
-     that rule splits the product). */
+     that rule splits the product);
+   ROWS16 / ROWS32: the row pass with 16 / 32 points per thread (ROWS16
+     needs rows of 2^9 points or more, and neither THREE nor SPLIT).
+     Without either the launch takes 16 where 32 would leave it fewer than
+     16 warps per SM. */
 #define GPU_MUL_FLAG_THREE 1
 #define GPU_MUL_FLAG_SPLIT 2
+#define GPU_MUL_FLAG_ROWS16 4
+#define GPU_MUL_FLAG_ROWS32 8
 
 /* Fills the zero fields of cfg with the defaults for an an x bn product and
    checks the rest; returns 0 or GPU_FFT_SMALL_EINVAL naming the bad field. */

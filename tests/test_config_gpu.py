@@ -46,9 +46,9 @@ def _valid_logC(logM):
 
 @pytest.mark.parametrize("logM", list(range(5, 18)) + [20, 22])
 def test_mpn_every_row_length_exact(ctx, logM):
-    """Every (transform length, row length) a caller may configure -- not only
-    the tuner's candidates -- gives the exact product; row lengths just outside
-    the rule are rejected."""
+    """Every (transform length, row length, row-pass width) a caller may
+    configure -- not only the tuner's candidates -- gives the exact product;
+    row lengths just outside the rule are rejected."""
     torch = pytest.importorskip("torch")
     an = (1 << (logM - 1)) - 3 if logM > 5 else 9
     bn = max(1, (1 << (logM - 1)) - an + 7) if logM > 5 else 7
@@ -61,12 +61,15 @@ def test_mpn_every_row_length_exact(ctx, logM):
     dz = torch.empty(an + bn, dtype=torch.int64, device="cuda")
     s = torch.cuda.current_stream()
     for logC in _valid_logC(logM):
-        c = FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, logM, logC))
-        dz.fill_(-1)
-        ctx.mpn_mul_device_config(dz.data_ptr(), da.data_ptr(), an, db.data_ptr(), bn, c,
-                                  s.cuda_stream)
-        s.synchronize()
-        assert (dz.cpu().numpy().view(np.uint64) == want).all(), c
+        # the row pass's width by the launch rule, and forced to 16 and 32
+        # points per thread
+        for fl in (0, FB.FLAG_ROWS16, FB.FLAG_ROWS32) if logC >= 9 else (0, FB.FLAG_ROWS32):
+            c = FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, logM, logC, fl))
+            dz.fill_(-1)
+            ctx.mpn_mul_device_config(dz.data_ptr(), da.data_ptr(), an, db.data_ptr(), bn, c,
+                                      s.cuda_stream)
+            s.synchronize()
+            assert (dz.cpu().numpy().view(np.uint64) == want).all(), c
     lo = _valid_logC(logM)[0]
     if lo > 5:
         with pytest.raises(FB.GpuFftSmallError):

@@ -79,13 +79,18 @@ def test_configuration_flags():
                        (1000, 1000, FB.FLAG_THREE),               # below the radix-3 kernels
                        (3 << 22, 3 << 22, FB.FLAG_THREE | FB.FLAG_SPLIT),
                        (1 << 20, 1 << 20, FB.FLAG_SPLIT),         # balanced: does not split
-                       (100, 100, 8)]:                            # unknown flag
+                       (1 << 16, 1 << 16, FB.FLAG_ROWS16 | FB.FLAG_ROWS32),
+                       (100, 100, FB.FLAG_ROWS16),                # rows of 2^8 points
+                       (1 << 24, 1 << 20, FB.FLAG_ROWS16 | FB.FLAG_SPLIT),
+                       (100, 100, 64)]:                           # unknown flag
         with pytest.raises(FB.GpuFftSmallError):
             FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, fl))
     with pytest.raises(FB.GpuFftSmallError):                     # six primes: no cube roots
         FB.resolve_config(0, 3 << 22, 3 << 22, FB.MulConfig(FB.ROUTE_NTT, 6, 0, 0, FB.FLAG_THREE))
     with pytest.raises(FB.GpuFftSmallError):                     # integer polynomials take none
         FB.resolve_config(1, 300, 200, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE), 2, 2)
+    for fl in (FB.FLAG_ROWS16, FB.FLAG_ROWS32):                  # row pass width: kept as given
+        assert FB.resolve_config(0, 1 << 16, 1 << 16, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, fl)).flags == fl
     assert tuner.reference_rule((0, 3 << 22, 3 << 22)).flags == FB.FLAG_THREE
     assert tuner.reference_rule((0, 1 << 24, 1 << 24)).key() == (FB.ROUTE_NTT, 5, 25, 14, 0)
     assert tuner.reference_rule((1, 300, 200, 3, 3)).flags == 0
