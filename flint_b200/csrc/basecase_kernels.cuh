@@ -16,7 +16,8 @@
 
 namespace fb {
 
-constexpr int BASECASE_MAX = 1024;
+constexpr int BASECASE_MAX = 4096;          // short operand of a single product
+constexpr int BASECASE_BATCH_MAX = 1024;    // short operand of a planned batch's product
 constexpr int BASECASE_THREADS = 256;
 constexpr int BASECASE_PER = 4;                                  // positions per thread
 constexpr int BASECASE_TILE = BASECASE_THREADS * BASECASE_PER;   // = the carry kernel's tile
@@ -42,8 +43,8 @@ k_basecase_sums(const uint64_t* __restrict__ x, uint64_t xn, const uint64_t* __r
                 uint64_t yn, uint64_t* __restrict__ s, int logM,
                 const InstDesc* __restrict__ desc, const uint32_t* __restrict__ tile_inst)
 {
-    __shared__ uint64_t sy[BASECASE_MAX];
-    __shared__ uint64_t sx[BASECASE_TILE + BASECASE_MAX];
+    __shared__ uint64_t sy[BASECASE_BATCH_MAX];
+    __shared__ uint64_t sx[BASECASE_TILE + BASECASE_BATCH_MAX];
     uint32_t tile = blockIdx.x;
     if (desc) {
         const InstDesc& D = desc[tile_inst[blockIdx.x]];
@@ -87,6 +88,96 @@ k_basecase_sums(const uint64_t* __restrict__ x, uint64_t xn, const uint64_t* __r
             s[k] = a[q][0];
             s[P + k] = a[q][1];
             s[2 * P + k] = a[q][2];
+        }
+    }
+}
+
+// Single products: the column sums split over both dimensions, so that a
+// small product spreads over many blocks instead of one block per 1024
+// positions.  Block (t, c) adds the partial sums of positions k0 .. k0 +
+// BC_POS - 1 (k0 = t BC_POS) over y limbs j0 .. j0 + BC_JCH - 1 (j0 = c
+// BC_JCH) into the planes by 64-bit atomic additions: the planes start at
+// zero and the thread that adds word w of a partial also adds the carry out
+// of that addition into word w + 1, so once every block has finished the
+// planes hold the exact 192-bit sums (in any order of the additions).
+// Inside a block, thread (p, r) takes positions k0 + 4p .. k0 + 4p + 3 over
+// the r-th BC_JCH / BC_SPLIT limbs of the chunk; the BC_SPLIT partials of a
+// position are summed in shared memory before the atomics.
+constexpr int BC_POS = 128;                           // positions per block
+constexpr int BC_SPLIT = 8;                           // sub-ranges of a chunk
+constexpr int BC_JCH = 256;                           // y limbs per block
+constexpr int BC_THREADS = (BC_POS / 4) * BC_SPLIT;   // 256
+
+__device__ __forceinline__ void add192(uint64_t& a0, uint64_t& a1, uint64_t& a2, uint64_t b0, uint64_t b1,
+                                       uint64_t b2)
+{
+    asm("add.cc.u64  %0, %0, %3;\n\t"
+        "addc.cc.u64 %1, %1, %4;\n\t"
+        "addc.u64    %2, %2, %5;"
+        : "+l"(a0), "+l"(a1), "+l"(a2)
+        : "l"(b0), "l"(b1), "l"(b2));
+}
+
+__global__ void __launch_bounds__(BC_THREADS)
+k_basecase_split(const uint64_t* __restrict__ x, uint64_t xn, const uint64_t* __restrict__ y, uint64_t yn,
+                 unsigned long long* __restrict__ s, int logM)
+{
+    __shared__ uint64_t sy[BC_JCH];
+    __shared__ uint64_t sx[BC_POS + BC_JCH];
+    __shared__ uint64_t part[BC_SPLIT][3][BC_POS];
+    const int64_t k0 = (int64_t)blockIdx.x * BC_POS;
+    const int64_t j0 = (int64_t)blockIdx.y * BC_JCH;
+    // x indices k - j of the block: k0 - j0 - (BC_JCH - 1) .. k0 - j0 + BC_POS - 1;
+    // a block entirely outside [0, xn) adds nothing (the test is the same for
+    // every thread of the block)
+    if (k0 - j0 + BC_POS - 1 < 0 || k0 - j0 - (BC_JCH - 1) >= (int64_t)xn) return;
+    const int jn = (int)((int64_t)yn - j0 < BC_JCH ? (int64_t)yn - j0 : BC_JCH);
+    for (int i = threadIdx.x; i < BC_JCH; i += BC_THREADS) sy[i] = i < jn ? y[j0 + i] : 0ull;
+    const int64_t xb = k0 - j0 - (BC_JCH - 1);
+    for (int i = threadIdx.x; i < BC_POS + BC_JCH - 1; i += BC_THREADS) {
+        const int64_t xi = xb + i;
+        sx[i] = (xi >= 0 && xi < (int64_t)xn) ? x[xi] : 0ull;
+    }
+    __syncthreads();
+    constexpr int SUB = BC_JCH / BC_SPLIT;
+    const int p = threadIdx.x % (BC_POS / 4), r = threadIdx.x / (BC_POS / 4);
+    // position k0 + 4p + q times limb j0 + r SUB + i reads
+    // x[k - j] = sx[4p + q - r SUB - i + BC_JCH - 1]
+    const uint64_t* px = sx + 4 * p + (BC_JCH - 1) - r * SUB;
+    uint64_t a[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const int cnt = jn - r * SUB < SUB ? jn - r * SUB : SUB;   // <= 0: this sub-range is past y
+    if (cnt > 0) {
+        uint64_t w0 = px[0], w1 = px[1], w2 = px[2], w3 = px[3];
+        for (int i = 0; i < cnt; i++) {
+            const uint64_t yj = sy[r * SUB + i];
+            mac192(a[0][0], a[0][1], a[0][2], w0, yj);
+            mac192(a[1][0], a[1][1], a[1][2], w1, yj);
+            mac192(a[2][0], a[2][1], a[2][2], w2, yj);
+            mac192(a[3][0], a[3][1], a[3][2], w3, yj);
+            w3 = w2; w2 = w1; w1 = w0;
+            w0 = i + 1 < SUB ? px[-(i + 1)] : 0ull;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int w = 0; w < 3; w++) part[r][w][4 * p + q] = a[q][w];
+    __syncthreads();
+    if (threadIdx.x < BC_POS) {
+        const int k = threadIdx.x;
+        uint64_t s0 = 0, s1 = 0, s2 = 0;
+#pragma unroll
+        for (int rr = 0; rr < BC_SPLIT; rr++) add192(s0, s1, s2, part[rr][0][k], part[rr][1][k], part[rr][2][k]);
+        const uint64_t kk = (uint64_t)k0 + k;
+        if (kk < xn + yn - 1 && (s0 | s1 | s2)) {
+            const size_t P = (size_t)1 << logM;
+            const uint64_t o0 = atomicAdd(&s[kk], (unsigned long long)s0);
+            const uint64_t c0 = o0 + s0 < o0;
+            const uint64_t t1 = s1 + c0;
+            const uint64_t c1a = t1 < s1;
+            const uint64_t o1 = atomicAdd(&s[P + kk], (unsigned long long)t1);
+            const uint64_t c1b = o1 + t1 < o1;
+            atomicAdd(&s[2 * P + kk], (unsigned long long)(s2 + c1a + c1b));
         }
     }
 }

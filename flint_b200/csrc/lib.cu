@@ -922,6 +922,19 @@ static int rows_loge(const Ctx *X, const LaunchShape &L, int np, int ninst)
     return warps < (uint64_t)X->nsm * 16 ? 4 : 5;
 }
 
+// The row launch of ninst products of np primes: rows per item as the
+// shape has them (up to 2^13 points per CTA), halved while the launch would
+// have fewer than two items per SM (small transforms).
+static LaunchShape row_launch_shape(const Ctx *X, const LaunchShape &L, int np, int ninst)
+{
+    LaunchShape Lr = L;
+    const int R = 1 << L.S.logR;
+    while (Lr.nv > 1 && (int64_t)(R / Lr.nv) * np * ninst < 2 * (int64_t)X->nsm) Lr.nv >>= 1;
+    Lr.row_grid = (R + Lr.nv - 1) / Lr.nv;
+    Lr.row_smem = (size_t)3 * Lr.nv * padw(1 << L.S.logC) * sizeof(uint32_t);
+    return Lr;
+}
+
 // A column launch: the shape's 2^14-word tiles, or narrow ones (a quarter of
 // the columns) where the launch would have fewer than two CTAs per SM --
 // small transforms, whose column passes are bound by latency, not by HBM.
@@ -986,13 +999,8 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
                                                                   np, shape, d_scale, fold ? 2 : 0);
     }
     timing_mark(tr, 1, st);
-    // rows per item: the shape's (up to 2^13 points per CTA), halved while the
-    // launch would have fewer than two items per SM (small transforms)
-    LaunchShape Lr = L;
     const int R = 1 << S.logR;
-    while (Lr.nv > 1 && (int64_t)(R / Lr.nv) * np * ni < 2 * (int64_t)X->nsm) Lr.nv >>= 1;
-    Lr.row_grid = (R + Lr.nv - 1) / Lr.nv;
-    Lr.row_smem = (size_t)3 * Lr.nv * padw(1 << S.logC) * sizeof(uint32_t);
+    const LaunchShape Lr = row_launch_shape(X, L, np, ni);
     const int items = Lr.row_grid * np * ni;
     const int loge = rows_loge(X, Lr, np, ni);
     (loge == 4 ? ROWS16 : ROWS)[S.logC]<<<std::min(items, X->nsm * rows_per_sm(Lr, loge)),
@@ -1063,7 +1071,11 @@ static int mpn_mul_basecase_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint
         X->epoch = 1;
     }
     TimingRecord *tr = timing_begin(X, st);
-    k_basecase_sums<<<(unsigned)tiles, BASECASE_THREADS, 0, st>>>(x, xn, y, yn, sums, logM, nullptr, nullptr);
+    // column sums split over positions and short-operand chunks, added into
+    // zeroed planes (k_basecase_split)
+    CU(cudaMemsetAsync(sums, 0, 3 * plane * sizeof(uint64_t), st));
+    k_basecase_split<<<dim3((unsigned)((L + BC_POS - 1) / BC_POS), (unsigned)((yn + BC_JCH - 1) / BC_JCH)),
+                       BC_THREADS, 0, st>>>(x, xn, y, yn, (unsigned long long *)sums, logM);
     timing_mark(tr, 1, st);
     timing_mark(tr, 2, st);
     timing_mark(tr, 3, st);

@@ -8,8 +8,10 @@ the configuration a chooser gives it:
 * mpn requests go in chunks (at most ``chunk_limbs`` operand limbs each) into
   planned batches (gpu_mpn_batch_init_config), so products that share a
   configuration share launches; requests whose configuration carries flags
-  (a 3 2^k-point transform, a split product) go in chunks through the
-  per-instance list call (gpu_mpn_mul_device_list) instead;
+  (a 3 2^k-point transform, a split product, a forced row-pass width) or
+  takes the basecase route beyond a planned batch's limit (a short operand
+  above 1024 limbs) go in chunks through the per-instance list call
+  (gpu_mpn_mul_device_list) instead;
 * integer-polynomial requests go in chunks through one list call each
   (gpu_fmpz_poly_mul_mid_device_list): every product of a chunk is queued by
   native code on one stream, with the scratch sized before the timing.
@@ -26,7 +28,15 @@ a caller copy selected products (with their operands) to the host.
 """
 import numpy as np
 
-from . import FmpzMulReq, MpnBatch, MulReq
+from . import ROUTE_BASECASE, FmpzMulReq, MpnBatch, MulReq
+from .tuner import BASECASE_BATCH_MAX
+
+
+def _per_instance(r, cfg):
+    """True for an mpn request whose configuration a planned batch does not
+    take (flags, or the basecase route with a short operand above the
+    batch's limit)."""
+    return bool(cfg.flags) or (cfg.route == ROUTE_BASECASE and min(r[1], r[2]) > BASECASE_BATCH_MAX)
 
 
 def _weights(torch, n, dev):
@@ -95,8 +105,8 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27
     res = {"mpn_ms": 0.0, "fmpz_ms": 0.0, "mpn_limbs": 0, "fmpz_coeff_limbs": 0,
            "mpn_requests": 0, "fmpz_requests": 0, "kept": {}}
     digests = np.zeros(len(reqs), dtype=np.int64)
-    mpn = [k for k, r in enumerate(reqs) if r[0] == 0 and not configs[k].flags]
-    mpn_list = [k for k, r in enumerate(reqs) if r[0] == 0 and configs[k].flags]
+    mpn_list = [k for k, r in enumerate(reqs) if r[0] == 0 and _per_instance(r, configs[k])]
+    mpn = [k for k, r in enumerate(reqs) if r[0] == 0 and not _per_instance(r, configs[k])]
     fz = [k for k, r in enumerate(reqs) if r[0] == 1]
     wmax = 1
     for r in reqs:

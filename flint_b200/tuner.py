@@ -38,12 +38,13 @@ import math
 
 import numpy as np
 
-from . import (FLAG_SPLIT, FLAG_THREE, MulConfig, ROUTE_BASECASE, ROUTE_NTT, GpuFftSmallError, Mlp,
-               resolve_config)
+from . import (FLAG_ROWS16, FLAG_ROWS32, FLAG_SPLIT, FLAG_THREE, MulConfig, ROUTE_BASECASE, ROUTE_NTT,
+               GpuFftSmallError, Mlp, resolve_config)
 from . import reference_rule as _reference_rule
 
-BASECASE_MAX = 1024
-N_FEATURES = 18
+BASECASE_MAX = 4096          # short operand of the basecase route, single products
+BASECASE_BATCH_MAX = 1024    # ... in a planned batch
+N_FEATURES = 20
 
 
 def _req(r):
@@ -62,12 +63,13 @@ def default_config(r):
 
 def candidates(r, flags=True):
     """All configurations the tuner considers for request r (resolved).
-    flags=False leaves out the THREE / SPLIT configurations (planned batches
-    run every class with plain transforms)."""
+    flags=False leaves out the flagged configurations (THREE, SPLIT, the row
+    pass's width) and keeps the basecase route to the batch limit: planned
+    batches run every class with plain transforms."""
     kind, an, bn, aw, bw = _req(r)
     base = default_config(r)
     out = []
-    if kind == 0 and min(an, bn) <= BASECASE_MAX:
+    if kind == 0 and min(an, bn) <= (BASECASE_MAX if flags else BASECASE_BATCH_MAX):
         out.append(MulConfig(ROUTE_BASECASE, 0, 0, 0))
     for dnp in (0, 1):
         for dm in (0, 1):
@@ -83,6 +85,13 @@ def candidates(r, flags=True):
         for fl in (FLAG_THREE, FLAG_SPLIT):
             try:
                 out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, base.np, base.logM, 0, fl)))
+            except GpuFftSmallError:
+                pass
+        # the row pass at 16 and at 32 points per thread (the launch rule
+        # picks one of them by the warps the launch has)
+        for fl in (FLAG_ROWS16, FLAG_ROWS32):
+            try:
+                out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, base.np, base.logM, base.logC, fl)))
             except GpuFftSmallError:
                 pass
     return out
@@ -135,6 +144,8 @@ def features(r, cfg):
         f[15] = math.log2(pts) / 25 - lt / 25
         f[16] = 1.0 if cfg.flags & FLAG_THREE else 0.0
         f[17] = 1.0 if cfg.flags & FLAG_SPLIT else 0.0
+        f[18] = 1.0 if cfg.flags & FLAG_ROWS16 else 0.0
+        f[19] = 1.0 if cfg.flags & FLAG_ROWS32 else 0.0
     return f
 
 
@@ -162,9 +173,11 @@ class Autotuner:
         kind, an, bn, aw, bw = _req(r)
         key = (kind, an, bn, aw, bw, cfg.key())
         if key not in self.cache:
-            # planned batches take no flags: such configurations run per
-            # instance, so they are timed alone
-            if self.batched and kind == 0 and not cfg.flags:
+            # planned batches take no flags, and basecase products only up to
+            # a short operand of BASECASE_BATCH_MAX limbs: other
+            # configurations run per instance, so they are timed alone
+            batchable = not cfg.flags and not (cfg.route == ROUTE_BASECASE and min(an, bn) > BASECASE_BATCH_MAX)
+            if self.batched and kind == 0 and batchable:
                 self.cache[key] = self.ctx.time_batched(an, bn, cfg, batch_copies(an, bn), self.reps)
             else:
                 self.cache[key] = self.ctx.time_config(kind, an, bn, cfg, aw, bw, self.reps)

@@ -375,7 +375,8 @@ GPU_FFT_SMALL_API int gpu_mulmod_2expp1_mul_cached(const gpu_mulmod_2expp1_ctx_s
        1248-1340, which is internal) --------------------------------------- */
 
 #define GPU_MUL_ROUTE_NTT       0   /* number-theoretic transform */
-#define GPU_MUL_ROUTE_BASECASE  1   /* schoolbook; shorter operand <= 1024 limbs */
+#define GPU_MUL_ROUTE_BASECASE  1   /* schoolbook; shorter operand <= 4096 limbs
+                                       (<= 1024 in a planned batch) */
 
 /* How one product is computed.  Zero fields take the default: the fewest
    primes that hold the coefficient bound, the shortest transform that holds

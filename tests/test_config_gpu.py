@@ -80,7 +80,8 @@ def test_basecase_all_ones_and_operand_order(ctx):
     torch = pytest.importorskip("torch")
     s = torch.cuda.current_stream()
     bc = FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0)
-    for an, bn in [(1024, 1024), (7, 5000), (1, 1), (50000, 1024)]:
+    for an, bn in [(1024, 1024), (7, 5000), (1, 1), (50000, 1024), (4096, 4096), (3000, 2000),
+                   (300000, 4000), (1, 4096)]:
         a = np.full(an, (1 << 64) - 1, dtype=np.uint64)
         b = np.full(bn, (1 << 64) - 1, dtype=np.uint64)
         da = torch.from_numpy(a.view(np.int64)).cuda()
@@ -90,6 +91,25 @@ def test_basecase_all_ones_and_operand_order(ctx):
                                   s.cuda_stream)
         s.synchronize()
         assert (dz.cpu().numpy().view(np.uint64) == O.gmp_mpn_mul(a, b)).all()
+
+
+@pytest.mark.parametrize("an,bn", [(129, 257), (128, 256), (4095, 4096), (4096, 2049), (10 ** 6, 4096),
+                                   (255, 3), (5000, 4096)])
+def test_basecase_split_blocks_exact(ctx, an, bn):
+    """The single-product basecase (column sums split over positions and
+    short-operand chunks, added atomically) at block-boundary shapes, random
+    limbs, against GMP."""
+    torch = pytest.importorskip("torch")
+    a = O.rand_limbs(an + 5, an)
+    b = O.rand_limbs(bn + 11, bn)
+    da = torch.from_numpy(a.view(np.int64)).cuda()
+    db = torch.from_numpy(b.view(np.int64)).cuda()
+    dz = torch.full((an + bn,), -1, dtype=torch.int64, device="cuda")
+    s = torch.cuda.current_stream()
+    ctx.mpn_mul_device_config(dz.data_ptr(), da.data_ptr(), an, db.data_ptr(), bn,
+                              FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0), s.cuda_stream)
+    s.synchronize()
+    assert (dz.cpu().numpy().view(np.uint64) == O.gmp_mpn_mul(a, b)).all()
 
 
 @pytest.mark.parametrize("r", [(1, 300, 200, 2, 2), (1, 4000, 3000, 3, 1), (1, 256, 256, 65, 65)])

@@ -11,7 +11,7 @@ from flint_b200 import tuner
 from flint_b200.workload import request_stream
 
 
-REQS = [(0, 1, 1), (0, 64, 64), (0, 1000, 3), (0, 1 << 20, 1 << 14), (0, 1 << 22, 1 << 22),
+REQS = [(0, 1, 1), (0, 64, 64), (0, 1000, 3), (0, 3000, 2000), (0, 1 << 20, 1 << 14), (0, 1 << 22, 1 << 22),
         (1, 256, 300, 2, 2), (1, 1 << 16, 1 << 16, 65, 65), (1, 5000, 40, 10, 3)]
 
 
@@ -24,6 +24,8 @@ def test_candidates_are_valid_and_include_default(r):
     kind, an, bn = r[:3]
     has_bc = any(c.route == FB.ROUTE_BASECASE for c in cs)
     assert has_bc == (kind == 0 and min(an, bn) <= tuner.BASECASE_MAX)
+    has_bc_batch = any(c.route == FB.ROUTE_BASECASE for c in tuner.candidates(r, flags=False))
+    assert has_bc_batch == (kind == 0 and min(an, bn) <= tuner.BASECASE_BATCH_MAX)
     for c in cs:
         if c.route == FB.ROUTE_NTT:
             assert max(5, c.logM - 11) <= c.logC <= min(c.logM, 14)
@@ -34,7 +36,8 @@ def test_candidates_are_valid_and_include_default(r):
 
 def test_invalid_configs_are_rejected():
     with pytest.raises(FB.GpuFftSmallError):
-        FB.resolve_config(0, 5000, 5000, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0))   # > 1024
+        FB.resolve_config(0, 5000, 5000, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0))   # > 4096
+    assert FB.resolve_config(0, 4096, 10 ** 6, FB.MulConfig(FB.ROUTE_BASECASE, 0, 0, 0)).route == FB.ROUTE_BASECASE
     with pytest.raises(FB.GpuFftSmallError):
         FB.resolve_config(0, 100, 100, FB.MulConfig(FB.ROUTE_NTT, 4, 0, 0))          # too few primes
     with pytest.raises(FB.GpuFftSmallError):
