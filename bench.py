@@ -838,8 +838,9 @@ def main():
                     help="skip the products mod 2^N + 1")
     ap.add_argument("--negacyclic-only", action="store_true",
                     help="run only the products mod 2^N + 1 (profiling); prints their results")
-    ap.add_argument("--stream-requests", type=int, default=2000,
-                    help="requests of the mixed mpn / integer-polynomial stream (0 = skip)")
+    ap.add_argument("--stream-requests", type=int, default=100000,
+                    help="requests of the mixed mpn / integer-polynomial stream (0 = skip; the "
+                         "configuration's stated size is 100000)")
     args = ap.parse_args()
     an, bn, desc = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -48,17 +48,21 @@ def _weights(torch, n, dev):
 
 def _digests(torch, out, starts, lens, weights):
     """Per-product digests sum_i out[s + i] * weights[i] (mod 2^64) for the
-    products at out[starts[k] : starts[k] + lens[k]]."""
+    products at out[starts[k] : starts[k] + lens[k]] (consecutive, in
+    order).  A scan, not atomics: each limb's position inside its product
+    comes from a running count of product starts, and a product's digest is
+    the difference of the wrapping prefix sums at its two ends."""
     dev = out.device
+    n = int(starts[-1] + lens[-1])
     st = torch.tensor(starts, dtype=torch.int64, device=dev)
-    ln = torch.tensor(lens, dtype=torch.int64, device=dev)
-    # position of every limb inside its product
-    owner = torch.repeat_interleave(torch.arange(len(starts), device=dev), ln)
-    local = torch.arange(out.numel(), device=dev) - torch.repeat_interleave(st, ln)
-    prod = out[:owner.numel()] * weights[local]
-    d = torch.zeros(len(starts), dtype=torch.int64, device=dev)
-    d.index_add_(0, owner, prod)
-    return d
+    ends = st + torch.tensor(lens, dtype=torch.int64, device=dev)
+    marks = torch.zeros(n, dtype=torch.int32, device=dev)
+    marks[st[1:]] = 1
+    owner = torch.cumsum(marks, 0)
+    local = torch.arange(n, device=dev) - st[owner]
+    cs = torch.cumsum(out[:n] * weights[local], 0)
+    lo = torch.where(st > 0, cs[(st - 1).clamp(min=0)], torch.zeros_like(st))
+    return cs[ends - 1] - lo
 
 
 POOL_LIMBS = 1 << 27
