@@ -250,14 +250,19 @@ def train_cost_model(ctx):
     loss = model.fit(X, t, epochs=400)
     info = {"train_requests": len(train), "train_rows": int(len(X)), "tuning_s": t_tune,
             "fit_s": time.perf_counter() - t0, "fit_mse_log_ms": loss,
-            "decision_margin": model.margin,
+            "decision_margin": model.margin, "min_class": MIN_CLASS,
             "network": "%d -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels" % tuner.N_FEATURES,
-            "candidates": "route (transform / basecase), primes (min, +1), length (min, x2), rows "
-                          "(longest .. 8x shorter), THREE (3 2^k length) and SPLIT flags for mpn"}
+            "candidates": "route (transform / basecase: short operand up to 4096 limbs alone, 1024 in "
+                          "a planned batch), primes (min, +1), length (min, x2), rows (longest .. 8x "
+                          "shorter), and for mpn requests run alone the THREE (3 2^k length), SPLIT and "
+                          "row-pass width (16 / 32 points per thread) flags"}
     return model, tun, info
 
 
 STREAM_SEED = 5005
+# a learned choice that would leave an mpn request in a batch class of fewer
+# products than this falls back to the fixed rule (tuner.CostModel.choose)
+MIN_CLASS = 16
 
 
 def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_held=1000):
@@ -273,7 +278,7 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
     from flint_b200.workload import request_stream
     reqs = request_stream(STREAM_SEED, n_req)
     t0 = time.perf_counter()
-    learned = model.choose(reqs)
+    learned = model.choose(reqs, min_class=MIN_CLASS)
     t_choose = time.perf_counter() - t0
     default = [tuner.default_config(r) for r in reqs]
     refrule = [tuner.reference_rule(r) for r in reqs]
@@ -284,6 +289,7 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
     rd = run_stream(ctx, torch, reqs, default, 17, stream, dev)
     w2 = time.perf_counter()
     rr = run_stream(ctx, torch, reqs, refrule, 17, stream, dev)
+    w3 = time.perf_counter()
     same = (rl["digests"] == rd["digests"]) & (rl["digests"] == rr["digests"])
     held = request_stream(STREAM_SEED + 2, n_held)
     t0 = time.perf_counter()
@@ -312,8 +318,10 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
         "gain_over_default_rule": rd["total_ms"] / rl["total_ms"],
         "gain_over_reference_rule": rr["total_ms"] / rl["total_ms"],
         "flags_chosen": {"three": sum(bool(c.flags & FB.FLAG_THREE) for c in learned),
-                         "split": sum(bool(c.flags & FB.FLAG_SPLIT) for c in learned)},
-        "choose_s": t_choose, "wall_s": {"learned_run": w1 - w0, "default_run": w2 - w1},
+                         "split": sum(bool(c.flags & FB.FLAG_SPLIT) for c in learned),
+                         "rows16": sum(bool(c.flags & FB.FLAG_ROWS16) for c in learned),
+                         "rows32": sum(bool(c.flags & FB.FLAG_ROWS32) for c in learned)},
+        "choose_s": t_choose, "wall_s": {"learned_run": w1 - w0, "default_run": w2 - w1, "reference_rule_run": w3 - w2},
         "routes": {"transform": sum(c.route == 0 for c in learned),
                    "basecase": sum(c.route == 1 for c in learned)},
         "identical_to_default_rule": bool(same.all()),
@@ -439,7 +447,7 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
     held = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 2, 48)]
     reg = tuner.regret(tun, held, model.choose(held, flags=False), flags=False)
     t0 = time.perf_counter()
-    configs = model.choose([(0, a, b) for a, b in sizes], flags=False)
+    configs = model.choose([(0, a, b) for a, b in sizes], flags=False, min_class=MIN_CLASS)
     t_choose = time.perf_counter() - t0
     B = FB.MpnBatch(ctx, reqs, configs=configs)
     d_out.fill_(0)

@@ -216,9 +216,30 @@ class CostModel:
     def fit(self, X, t, epochs=300, batch=256, lr=2e-3, seed=7):
         return self.net.train(X, t, epochs=epochs, batch=batch, lr=lr, seed=seed)
 
-    def choose(self, reqs, flags=True):
+    def choose(self, reqs, flags=True, min_class=0):
         """Chosen configuration per request (one batched forward pass);
-        flags=False chooses among plain transforms only (planned batches)."""
+        flags=False chooses among plain transforms only (planned batches).
+
+        min_class > 0: the requests are run as planned batches, whose
+        products share launches by configuration class; the model is trained
+        on the marginal cost of a product inside a populated class, so a
+        choice that leaves a request in a class of fewer than min_class
+        products of this request list (where that cost does not hold) falls
+        back to the fixed rule.  Configurations that run per instance
+        (flags, a basecase product beyond a batch's limit) are exempt."""
+        out = self._choose(reqs, flags)
+        if min_class > 0:
+            for _ in range(2):
+                count = {}
+                for r, c in zip(reqs, out):
+                    k = _class_key(r, c)
+                    if k is not None:
+                        count[k] = count.get(k, 0) + 1
+                out = [default_config(r) if (k := _class_key(r, c)) is not None and count[k] < min_class
+                       and c.key() != default_config(r).key() else c for r, c in zip(reqs, out)]
+        return out
+
+    def _choose(self, reqs, flags):
         cands = [candidates(r, flags) for r in reqs]
         rows = [features(r, c) for r, cs in zip(reqs, cands) for c in cs]
         pred = self.net.predict(np.array(rows, dtype=np.float32))
@@ -235,6 +256,15 @@ class CostModel:
             out.append(cs[i])
             k += len(cs)
         return out
+
+
+def _class_key(r, c):
+    """The planned-batch class of mpn request r under configuration c (None
+    for requests that run per instance, and for integer polynomials)."""
+    kind, an, bn, _, _ = _req(r)
+    if kind != 0 or c.flags or (c.route == ROUTE_BASECASE and min(an, bn) > BASECASE_BATCH_MAX):
+        return None
+    return (c.route, c.np, c.logM, c.logC)
 
 
 def regret(tuner, reqs, chosen, flags=True):

@@ -100,3 +100,20 @@ def test_configuration_flags():
     keys = [c.key() for c in tuner.candidates((0, 3 << 22, 3 << 22))]
     assert (FB.ROUTE_NTT, 5, 25, 13, FB.FLAG_THREE) in keys
     assert all(c.flags == 0 for c in tuner.candidates((0, 3 << 22, 3 << 22), flags=False))
+
+
+def test_min_class_falls_back_to_rule():
+    """A learned choice that leaves a request in a batch class of fewer than
+    min_class products falls back to the fixed rule; per-instance
+    configurations (flags) are kept."""
+    reqs = [(0, 1 << 12, 1 << 12)] * 20 + [(0, 1 << 14, 1 << 13)] * 3 + [(0, 3 << 20, 3 << 20)]
+    alt = FB.resolve_config(0, 1 << 12, 1 << 12, FB.MulConfig(FB.ROUTE_NTT, 6, 0, 0))
+    alt2 = FB.resolve_config(0, 1 << 14, 1 << 13, FB.MulConfig(FB.ROUTE_NTT, 6, 0, 0))
+    three = FB.resolve_config(0, 3 << 20, 3 << 20, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE))
+    m = tuner.CostModel.__new__(tuner.CostModel)
+    m._choose = lambda rs, flags: [alt] * 20 + [alt2] * 3 + [three]
+    out = m.choose(reqs, min_class=16)
+    assert all(c.key() == alt.key() for c in out[:20])                     # a class of 20: kept
+    assert all(c.key() == tuner.default_config(reqs[20]).key() for c in out[20:23])   # 3: rule
+    assert out[23].key() == three.key()                                      # per instance: kept
+    assert [c.key() for c in m.choose(reqs)] == [c.key() for c in [alt] * 20 + [alt2] * 3 + [three]]
