@@ -39,6 +39,8 @@ WORKLOADS = {
     "mpn24x20": (1 << 24, 1 << 20, "mpn_mul 2^24 x 2^20 limbs (unbalanced), uniform random limbs"),
     # profiling-sized case: operands 64 MB, residues 320 MB (larger than L2)
     "mpn22": (1 << 22, 1 << 22, "mpn_mul 2^22 x 2^22 limbs, uniform random limbs"),
+    # the small-product (latency-bound) case, 2^17-point transforms
+    "mpn16": (1 << 16, 1 << 16, "mpn_mul 2^16 x 2^16 limbs, uniform random limbs"),
 }
 NS_LIMB_BITS = 64
 
