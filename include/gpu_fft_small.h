@@ -166,7 +166,12 @@ GPU_FFT_SMALL_API int gpu_mpn_mul_device(gpu_mpn_ctx_t R, uint64_t *z_dev,
        any stream capture.
      * All calls share the scratch, which keeps the last call's contents:
        calls whose work overlaps on the GPU (other streams, other host
-       threads) race, so the caller must serialise them. */
+       threads) race, so the caller must serialise them.
+     * The return code covers argument checks, the set-up and the launches
+       only.  The carry pass's bounded wait (which valid inputs never
+       exhaust) flags a timeout in the library's scratch, which a call that
+       does not synchronise cannot read back, so such a device-side error is
+       not reported here. */
 GPU_FFT_SMALL_API int gpu_mpn_mul_device_noalloc(uint64_t *z_dev, const uint64_t *a_dev,
                                                  gpu_ulong an, const uint64_t *b_dev,
                                                  gpu_ulong bn, void *stream);
