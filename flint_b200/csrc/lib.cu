@@ -583,8 +583,10 @@ static LaunchShape make_shape(int logM, int logC = -1)
 // the three transform launches shared by every product type; with a batch
 // descriptor array (ninst products of this shape) a, b, ra, rb are ignored;
 // with fz the operands are integer polynomials (an, bn coefficients); with co
-// the inverse column pass writes a split product's chunk (ChunkOut)
-static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
+// the inverse column pass writes a split product's chunk (ChunkOut).  Returns
+// the residue array that holds the product (ra, or rb for a large product
+// whose b arrives late: b_ready)
+static uint32_t *launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
                               uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
                               uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
                               TimingRecord *tr, const InstDesc *desc = nullptr, int ninst = 1,
@@ -966,11 +968,11 @@ static ColLaunch col_launch(const Ctx *X, const LaunchShape &L, int np, int zdim
     return c;
 }
 
-static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
-                              uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
-                              uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
-                              TimingRecord *tr, const InstDesc *desc, int ninst, const FzShape *fz,
-                              cudaEvent_t b_ready, const ChunkOut *co)
+static uint32_t *launch_transforms(const Ctx *X, const LaunchShape &L, int np, const uint64_t *a,
+                                   uint64_t an, const uint64_t *b, uint64_t bn, uint32_t *ra,
+                                   uint32_t *rb, bool sq, const uint32_t *d_scale, cudaStream_t st,
+                                   TimingRecord *tr, const InstDesc *desc, int ninst, const FzShape *fz,
+                                   cudaEvent_t b_ready, const ChunkOut *co)
 {
     const MulShape &S = L.S;
     const int zdim = desc ? 2 * ninst : (sq ? 1 : 2);
@@ -985,21 +987,42 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
     // b's twist factors, so the row pass multiplies the spectra once instead
     // of twice; squarings keep the scale in the row pass.
     const bool fold = !(sq && !desc) && S.logR >= 5;
+    const int R = 1 << S.logR;
     if (b_ready && !desc && !sq) {
         // b is still arriving: a's column pass first, b's after its copy
         fwd<<<dim3(np, cf.grid, 1), cf.threads, cf.smem, st>>>(X->T, a, an, a, an, ra, ra, S.logC, cf.G, nullptr,
                                                                np, shape, d_scale, 0);
+        // A large product also runs a's forward row transforms before b has
+        // arrived (k_rows_fwd); the row pass then transforms b alone and
+        // multiplies it by a's spectrum (squaring mode 2, as the chunks of a
+        // split product do), so less of the transform waits for b's upload.
+        // The product ends in b's residues.
+        const bool early = !fz && !co && fold && S.logR + S.logC >= 20;
+        if (early) {
+            const int C = 1 << S.logC, groups = (R + L.nv - 1) / L.nv;
+            ROWS_FWD[S.logC]<<<groups * np, L.nv * C / 32, (size_t)L.nv * padw(C) * sizeof(uint32_t), st>>>(
+                X->T, ra, S.logR, L.nv, np, R);
+        }
         cudaStreamWaitEvent(st, b_ready, 0);
         const FzShape shb = fz ? FzShape{shape.S, shape.wb, shape.wb} : shape;
         fwd<<<dim3(np, cf.grid, 1), cf.threads, cf.smem, st>>>(X->T, b, bn, b, bn, rb, rb, S.logC, cf.G, nullptr,
                                                                np, shb, d_scale, fold ? 1 : 0);
+        if (early) {
+            timing_mark(tr, 1, st);
+            ROWS[S.logC]<<<std::min(L.row_grid * np, X->nsm * rows_per_sm(L)), L.row_threads, L.row_smem, st>>>(
+                X->T, rb, ra, S.logR, L.nv, np, nullptr, 2, nullptr, 1, R);
+            timing_mark(tr, 2, st);
+            inv<<<dim3(ci.grid, np, 1), ci.threads, ci.smem, st>>>(X->T, rb, S.logC, ci.G, nullptr,
+                                                                   ChunkOut{nullptr, 0, 0, 0, 0});
+            timing_mark(tr, 3, st);
+            return rb;
+        }
     } else {
         if (b_ready) cudaStreamWaitEvent(st, b_ready, 0);
         fwd<<<dim3(np, cf.grid, zdim), cf.threads, cf.smem, st>>>(X->T, a, an, b, bn, ra, rb, S.logC, cf.G, desc,
                                                                   np, shape, d_scale, fold ? 2 : 0);
     }
     timing_mark(tr, 1, st);
-    const int R = 1 << S.logR;
     const LaunchShape Lr = row_launch_shape(X, L, np, ni);
     const int items = Lr.row_grid * np * ni;
     const int loge = rows_loge(X, Lr, np, ni);
@@ -1011,6 +1034,7 @@ static void launch_transforms(const Ctx *X, const LaunchShape &L, int np, const 
         inv<<<dim3(ci.grid, np, ni), ci.threads, ci.smem, st>>>(X->T, ra, S.logC, ci.G, desc,
                                                                 co ? *co : ChunkOut{nullptr, 0, 0, 0, 0});
     timing_mark(tr, 3, st);
+    return ra;
 }
 
 // Transform of M = 3 2^k points (k - 13 in [LOG3_RMIN, LOG3_RMAX]): columns of
@@ -1291,8 +1315,9 @@ static int mpn_mul_enqueue(Ctx *X, uint64_t *z, const uint64_t *a, uint64_t an,
     } else if (k3) {
         launch_transforms3(X, k3, logM, a, an, b, bn, ra, rb, sq, st, tr, b_ready);
     } else {
-        launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr, nullptr, 1,
-                          nullptr, b_ready);
+        // the product's residues: ra, or rb when b arrived late (launch_transforms)
+        ra = launch_transforms(X, P.L, np, a, an, b, bn, ra, rb, sq, scale_ptr(X, np, logM), st, tr, nullptr, 1,
+                               nullptr, b_ready);
     }
     // tiles take their index from the ticket counter, so consecutive launches
     // with the same ticket base continue one carry chain: tile k's look-back
