@@ -255,8 +255,8 @@ def train_cost_model(ctx):
             "decision_margin": model.margin, "min_class": MIN_CLASS,
             "network": "%d -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels" % tuner.N_FEATURES,
             "candidates": "route (transform / basecase: short operand up to 4096 limbs alone, 1024 in "
-                          "a planned batch), primes (min, +1), length (min, x2), rows (longest .. 8x "
-                          "shorter), and for mpn requests run alone the THREE (3 2^k length), SPLIT and "
+                          "a planned batch), primes (min, +1), length (min, x2), rows (the rule's, the longest .. "
+                          "8x shorter), and for mpn requests run alone the THREE (3 2^k length), SPLIT and "
                           "row-pass width (16 / 32 points per thread) flags"}
     return model, tun, info
 

@@ -71,14 +71,22 @@ def candidates(r, flags=True):
     out = []
     if kind == 0 and min(an, bn) <= (BASECASE_MAX if flags else BASECASE_BATCH_MAX):
         out.append(MulConfig(ROUTE_BASECASE, 0, 0, 0))
+    seen = set()
     for dnp in (0, 1):
         for dm in (0, 1):
-            for dc in (0, 1, 2, 3):
-                np_, logM = base.np + dnp, base.logM + dm
-                logC = min(logM, 14) - dc
-                c = MulConfig(ROUTE_NTT, np_, logM, logC)
+            np_, logM = base.np + dnp, base.logM + dm
+            # the rule's row length for this length, then the longest rows
+            # and 2x / 4x / 8x shorter
+            try:
+                rule_logC = [resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, np_, logM, 0), aw, bw).logC]
+            except GpuFftSmallError:
+                rule_logC = []
+            for logC in rule_logC + [min(logM, 14) - dc for dc in (0, 1, 2, 3)]:
+                if (np_, logM, logC) in seen:
+                    continue
+                seen.add((np_, logM, logC))
                 try:
-                    out.append(resolve_config(kind, an, bn, c, aw, bw))
+                    out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, np_, logM, logC), aw, bw))
                 except GpuFftSmallError:
                     pass
     if flags and kind == 0:

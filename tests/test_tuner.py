@@ -11,7 +11,8 @@ from flint_b200 import tuner
 from flint_b200.workload import request_stream
 
 
-REQS = [(0, 1, 1), (0, 64, 64), (0, 1000, 3), (0, 3000, 2000), (0, 1 << 20, 1 << 14), (0, 1 << 22, 1 << 22),
+REQS = [(0, 1, 1), (0, 64, 64), (0, 1000, 3), (0, 3000, 2000), (0, 1 << 14, 1 << 14), (0, 40000, 30000),
+        (0, 1 << 20, 1 << 14), (0, 1 << 22, 1 << 22),
         (1, 256, 300, 2, 2), (1, 1 << 16, 1 << 16, 65, 65), (1, 5000, 40, 10, 3)]
 
 
