@@ -249,10 +249,13 @@ def train_cost_model(ctx):
     # predicts at least 10% saving (measured: batch 446 -> 463 Gbit/s, stream
     # 0.98 -> 1.00 of the rule, held-out regret 2.3% -> 0.2%, against no margin)
     model = tuner.CostModel(seed=11, margin=0.10)
-    loss = model.fit(X, t, epochs=400)
+    loss = model.fit(X, t, epochs=800)
     info = {"train_requests": len(train), "train_rows": int(len(X)), "tuning_s": t_tune,
             "fit_s": time.perf_counter() - t0, "fit_mse_log_ms": loss,
-            "decision_margin": model.margin, "min_class": MIN_CLASS,
+            "decision_margin": model.margin, "min_class": MIN_CLASS, "class_margin": CLASS_MARGIN,
+            "decisions": "planned batch: per class of the fixed rule, by the model's summed prediction "
+                         "(class_margin); request stream: per request (decision_margin), falling back to "
+                         "the rule in batch classes of fewer than min_class requests",
             "network": "%d -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels" % tuner.N_FEATURES,
             "candidates": "route (transform / basecase: short operand up to 4096 limbs alone, 1024 in "
                           "a planned batch), primes (min, +1), length (min, x2), rows (the rule's, the longest .. "
@@ -265,6 +268,10 @@ STREAM_SEED = 5005
 # a learned choice that would leave an mpn request in a batch class of fewer
 # products than this falls back to the fixed rule (tuner.CostModel.choose)
 MIN_CLASS = 16
+# a planned batch's classes move to the learned configuration where the model
+# predicts at least this saving over the class's requests
+# (tuner.CostModel.choose_classes)
+CLASS_MARGIN = 0.05
 
 
 def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_held=1000):
@@ -447,9 +454,9 @@ def bench_batch(torch, FB, ctx, dev, stream, steps, warmup, cpu_seconds, model, 
     # cost model; its regret on held-out requests of this distribution
     # planned batches run plain transforms: the model chooses among those
     held = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 2, 48)]
-    reg = tuner.regret(tun, held, model.choose(held, flags=False), flags=False)
+    reg = tuner.regret(tun, held, model.choose_classes(held, margin=CLASS_MARGIN), flags=False)
     t0 = time.perf_counter()
-    configs = model.choose([(0, a, b) for a, b in sizes], flags=False, min_class=MIN_CLASS)
+    configs = model.choose_classes([(0, a, b) for a, b in sizes], margin=CLASS_MARGIN)
     t_choose = time.perf_counter() - t0
     B = FB.MpnBatch(ctx, reqs, configs=configs)
     d_out.fill_(0)

@@ -44,7 +44,7 @@ from . import reference_rule as _reference_rule
 
 BASECASE_MAX = 4096          # short operand of the basecase route, single products
 BASECASE_BATCH_MAX = 1024    # ... in a planned batch
-N_FEATURES = 20
+N_FEATURES = 26
 
 
 def _req(r):
@@ -154,6 +154,12 @@ def features(r, cfg):
         f[17] = 1.0 if cfg.flags & FLAG_SPLIT else 0.0
         f[18] = 1.0 if cfg.flags & FLAG_ROWS16 else 0.0
         f[19] = 1.0 if cfg.flags & FLAG_ROWS32 else 0.0
+        # the column length selects the kernel variants (no column pass, one
+        # thread per short column, 32-point columns in registers, strided
+        # passes, constant-stride instances): one indicator per group
+        logR = round(lt) - cfg.logC if not cfg.flags & FLAG_THREE else 0
+        for i, (lo, hi) in enumerate(((0, 0), (1, 4), (5, 5), (6, 8), (9, 10), (11, 11))):
+            f[20 + i] = 1.0 if lo <= logR <= hi else 0.0
     return f
 
 
@@ -223,6 +229,38 @@ class CostModel:
 
     def fit(self, X, t, epochs=300, batch=256, lr=2e-3, seed=7):
         return self.net.train(X, t, epochs=epochs, batch=batch, lr=lr, seed=seed)
+
+    def choose_classes(self, reqs, margin=0.05):
+        """Configurations for requests run as one planned batch (plain
+        transforms), decided per class: the requests whose fixed-rule
+        configuration is the same form a class, and the class moves as a
+        whole to the configuration whose predicted total time over its
+        requests is least, where that total is at least `margin` below the
+        rule's.  Summing over a class averages out the model's per-request
+        error, and moving a class whole keeps the batch's classes as
+        populated as the rule's."""
+        cands = [candidates(r, False) for r in reqs]
+        rows = [features(r, c) for r, cs in zip(reqs, cands) for c in cs]
+        pred = np.exp(self.net.predict(np.array(rows, dtype=np.float32)).astype(np.float64))
+        groups = {}
+        k = 0
+        for n, (r, cs) in enumerate(zip(reqs, cands)):
+            groups.setdefault(default_config(r).key(), []).append((n, {c.key(): (c, pred[k + i])
+                                                                       for i, c in enumerate(cs)}))
+            k += len(cs)
+        out = [default_config(r) for r in reqs]
+        for dk, members in groups.items():
+            common = set(members[0][1])
+            for _, m in members[1:]:
+                common &= set(m)
+            if dk not in common:
+                continue
+            tot = {key: sum(m[key][1] for _, m in members) for key in common}
+            best = min(tot, key=tot.get)
+            if tot[best] <= (1.0 - margin) * tot[dk]:
+                for n, m in members:
+                    out[n] = m[best][0]
+        return out
 
     def choose(self, reqs, flags=True, min_class=0):
         """Chosen configuration per request (one batched forward pass);

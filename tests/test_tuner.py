@@ -118,3 +118,31 @@ def test_min_class_falls_back_to_rule():
     assert all(c.key() == tuner.default_config(reqs[20]).key() for c in out[20:23])   # 3: rule
     assert out[23].key() == three.key()                                      # per instance: kept
     assert [c.key() for c in m.choose(reqs)] == [c.key() for c in [alt] * 20 + [alt2] * 3 + [three]]
+
+
+class _FakeNet:
+    """Predicts log time from the row-length feature alone: scale * logC/14."""
+
+    def __init__(self, scale):
+        self.scale = scale
+
+    def predict(self, X):
+        return (self.scale * X[:, 13]).astype(np.float32)
+
+
+def test_choose_classes_moves_whole_classes():
+    """Planned-batch choice per class of the fixed rule: every request of a
+    class moves to the configuration of least predicted total, and only when
+    that total saves at least the margin."""
+    reqs = [(0, 100000 + 37 * k, 60000 + 11 * k) for k in range(12)] + [(0, 3000, 2000)] * 5
+    m = tuner.CostModel.__new__(tuner.CostModel)
+    m.net = _FakeNet(-3.0)                 # longer rows predicted faster
+    out = m.choose_classes(reqs, margin=0.05)
+    for r, c in zip(reqs, out):
+        # the predicted-fastest candidate: the longest rows on offer
+        assert c.logC == max(x.logC for x in tuner.candidates(r, flags=False) if x.route == FB.ROUTE_NTT)
+    # each class of the rule moves whole: one configuration per class
+    assert len({c.key() for c in out[:12]}) == 1 and len({c.key() for c in out[12:]}) == 1
+    m.net = _FakeNet(-0.01)                # a saving below the margin: the rule stays
+    assert [c.key() for c in m.choose_classes(reqs, margin=0.05)] == \
+        [tuner.default_config(r).key() for r in reqs]
