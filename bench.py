@@ -252,10 +252,11 @@ def train_cost_model(ctx):
     loss = model.fit(X, t, epochs=800)
     info = {"train_requests": len(train), "train_rows": int(len(X)), "tuning_s": t_tune,
             "fit_s": time.perf_counter() - t0, "fit_mse_log_ms": loss,
-            "decision_margin": model.margin, "min_class": MIN_CLASS, "class_margin": CLASS_MARGIN,
-            "decisions": "planned batch: per class of the fixed rule, by the model's summed prediction "
-                         "(class_margin); request stream: per request (decision_margin), falling back to "
-                         "the rule in batch classes of fewer than min_class requests",
+            "decision_margin": model.margin, "class_margin": CLASS_MARGIN,
+            "decisions": "per class of the fixed rule (requests of one kind and one rule configuration), by "
+                         "the model's summed prediction over the class (class_margin); in the request stream "
+                         "an mpn request moves to a flagged configuration (run alone) only where the model "
+                         "predicts decision_margin below its class's choice",
             "network": "%d -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels" % tuner.N_FEATURES,
             "candidates": "route (transform / basecase: short operand up to 4096 limbs alone, 1024 in "
                           "a planned batch), primes (min, +1), length (min, x2), rows (the rule's, the longest .. "
@@ -265,9 +266,6 @@ def train_cost_model(ctx):
 
 
 STREAM_SEED = 5005
-# a learned choice that would leave an mpn request in a batch class of fewer
-# products than this falls back to the fixed rule (tuner.CostModel.choose)
-MIN_CLASS = 16
 # a planned batch's classes move to the learned configuration where the model
 # predicts at least this saving over the class's requests
 # (tuner.CostModel.choose_classes)
@@ -287,7 +285,7 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
     from flint_b200.workload import request_stream
     reqs = request_stream(STREAM_SEED, n_req)
     t0 = time.perf_counter()
-    learned = model.choose(reqs, min_class=MIN_CLASS)
+    learned = model.choose_stream(reqs, class_margin=CLASS_MARGIN)
     t_choose = time.perf_counter() - t0
     default = [tuner.default_config(r) for r in reqs]
     refrule = [tuner.reference_rule(r) for r in reqs]
@@ -302,7 +300,7 @@ def bench_stream(torch, FB, ctx, dev, stream, model, tun, n_req, cpu_seconds, n_
     same = (rl["digests"] == rd["digests"]) & (rl["digests"] == rr["digests"])
     held = request_stream(STREAM_SEED + 2, n_held)
     t0 = time.perf_counter()
-    reg = tuner.regret(tun, held, model.choose(held))
+    reg = tuner.regret(tun, held, model.choose_stream(held, class_margin=CLASS_MARGIN))
     reg["seconds"] = time.perf_counter() - t0
     bits_mpn = NS_LIMB_BITS * rl["mpn_limbs"]
     res = {

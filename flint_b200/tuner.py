@@ -245,11 +245,12 @@ class CostModel:
         groups = {}
         k = 0
         for n, (r, cs) in enumerate(zip(reqs, cands)):
-            groups.setdefault(default_config(r).key(), []).append((n, {c.key(): (c, pred[k + i])
-                                                                       for i, c in enumerate(cs)}))
+            groups.setdefault((r[0],) + default_config(r).key(), []).append(
+                (n, {c.key(): (c, pred[k + i]) for i, c in enumerate(cs)}))
             k += len(cs)
         out = [default_config(r) for r in reqs]
-        for dk, members in groups.items():
+        for gk, members in groups.items():
+            dk = gk[1:]
             common = set(members[0][1])
             for _, m in members[1:]:
                 common &= set(m)
@@ -260,6 +261,37 @@ class CostModel:
             if tot[best] <= (1.0 - margin) * tot[dk]:
                 for n, m in members:
                     out[n] = m[best][0]
+        return out
+
+    def choose_stream(self, reqs, class_margin=0.05, flag_margin=None):
+        """Configurations for a mixed request stream: plain transforms chosen
+        per class of the fixed rule (choose_classes; mpn requests then share
+        planned batches as under the rule), and an mpn request moved to a
+        flagged configuration (run alone: THREE, SPLIT, a forced row-pass
+        width) only where the model predicts at least flag_margin (default:
+        the model's decision margin) below the class choice."""
+        if flag_margin is None:
+            flag_margin = self.margin
+        out = self.choose_classes(reqs, class_margin)
+        idx = [n for n, r in enumerate(reqs) if r[0] == 0]
+        flagged = [[c for c in candidates(reqs[n], True) if c.flags] for n in idx]
+        rows, own = [], []
+        for n, fl in zip(idx, flagged):
+            if fl:
+                rows.append(features(reqs[n], out[n]))
+                rows += [features(reqs[n], c) for c in fl]
+                own.append((n, fl))
+        if not rows:
+            return out
+        pred = self.net.predict(np.array(rows, dtype=np.float32))
+        keep = math.log(1.0 - flag_margin)
+        k = 0
+        for n, fl in own:
+            base, p = pred[k], pred[k + 1:k + 1 + len(fl)]
+            i = int(np.argmin(p))
+            if p[i] - base <= keep:
+                out[n] = fl[i]
+            k += 1 + len(fl)
         return out
 
     def choose(self, reqs, flags=True, min_class=0):

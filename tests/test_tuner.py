@@ -146,3 +146,28 @@ def test_choose_classes_moves_whole_classes():
     m.net = _FakeNet(-0.01)                # a saving below the margin: the rule stays
     assert [c.key() for c in m.choose_classes(reqs, margin=0.05)] == \
         [tuner.default_config(r).key() for r in reqs]
+
+
+class _FakeFlagNet:
+    """Predicts log time: `three` for THREE configurations, 0 otherwise."""
+
+    def __init__(self, three):
+        self.three = three
+
+    def predict(self, X):
+        return (self.three * X[:, 16]).astype(np.float32)
+
+
+def test_choose_stream_flag_override():
+    """In a stream, an mpn request moves to a flagged configuration only where
+    the predicted saving over its class's choice reaches the margin;
+    integer-polynomial requests take no flags."""
+    reqs = [(0, 3 << 20, 3 << 20), (0, 1000, 900), (1, 300, 200, 2, 2)]
+    m = tuner.CostModel.__new__(tuner.CostModel)
+    m.margin = 0.10
+    m.net = _FakeFlagNet(-0.3)             # THREE predicted 26% faster
+    out = m.choose_stream(reqs, class_margin=0.05)
+    assert out[0].flags == FB.FLAG_THREE
+    assert out[1].key() == tuner.default_config(reqs[1]).key() and out[2].flags == 0
+    m.net = _FakeFlagNet(-0.05)            # 5% faster: below the margin
+    assert m.choose_stream(reqs, class_margin=0.05)[0].flags == 0
