@@ -153,16 +153,20 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27
         res["mpn_limbs"] += tot
         res["mpn_requests"] += len(idx)
 
-    # flagged mpn requests: one list call per chunk, queued by native code
+    # flagged mpn requests: one list call per chunk, queued by native code;
+    # the context's scratch is sized outside the timing by untimed products of
+    # the largest request and of the request whose configuration needs the
+    # most residue words (a list call grows the scratch to its products' need)
     if mpn_list:
-        big = max(mpn_list, key=lambda k: reqs[k][1] + reqs[k][2])
-        an, bn = reqs[big][1], reqs[big][2]
-        ta = torch.zeros(an + bn, dtype=torch.int64, device=dev)
-        tz = torch.empty(an + bn, dtype=torch.int64, device=dev)
-        ctx.mpn_mul_device_list([MulReq(tz.data_ptr(), ta.data_ptr(), an, ta.data_ptr() + 8 * an, bn)],
-                                [configs[big]], s)      # scratch sized outside the timing
-        stream.synchronize()
-        del ta, tz
+        for big in {max(mpn_list, key=lambda k: reqs[k][1] + reqs[k][2]),
+                    max(mpn_list, key=lambda k: (configs[k].np << configs[k].logM, reqs[k][1] + reqs[k][2]))}:
+            an, bn = reqs[big][1], reqs[big][2]
+            ta = torch.zeros(an + bn, dtype=torch.int64, device=dev)
+            tz = torch.empty(an + bn, dtype=torch.int64, device=dev)
+            ctx.mpn_mul_device_list([MulReq(tz.data_ptr(), ta.data_ptr(), an, ta.data_ptr() + 8 * an, bn)],
+                                    [configs[big]], s)
+            stream.synchronize()
+            del ta, tz
     for ci, idx in enumerate(_chunks(mpn_list, lambda k: reqs[k][1] + reqs[k][2], chunk_limbs)):
         tot = sum(reqs[k][1] + reqs[k][2] for k in idx)
         d_in = operands(idx, lambda k: reqs[k][1] + reqs[k][2])
@@ -192,17 +196,20 @@ def run_stream(ctx, torch, reqs, configs, seed, stream, dev, chunk_limbs=1 << 27
         res["mpn_listed_requests"] = res.get("mpn_listed_requests", 0) + len(idx)
 
     if fz:
-        # size the context's scratch for the stream's largest integer-polynomial
-        # product outside the timing (one untimed product)
-        big = max(fz, key=lambda k: (reqs[k][1] + reqs[k][2] - 1) * (reqs[k][3] + reqs[k][4] - 1))
-        _, an, bn, aw, bw = reqs[big]
-        ta = torch.zeros(an * aw + bn * bw, dtype=torch.int64, device=dev)
-        tz = torch.empty((an + bn - 1) * (aw + bw + 1), dtype=torch.int64, device=dev)
-        ctx.fmpz_poly_mul_device_list(
-            [FmpzMulReq(tz.data_ptr(), aw + bw + 1, 0, an + bn - 1, ta.data_ptr(), aw, an,
-                        ta.data_ptr() + 8 * an * aw, bw, bn)], [configs[big]], s)
-        stream.synchronize()
-        del ta, tz
+        # size the context's scratch outside the timing: untimed products of
+        # the largest integer-polynomial request and of the one whose
+        # configuration needs the most residue words
+        for big in {max(fz, key=lambda k: (reqs[k][1] + reqs[k][2] - 1) * (reqs[k][3] + reqs[k][4] - 1)),
+                    max(fz, key=lambda k: (configs[k].np << configs[k].logM,
+                                           (reqs[k][1] + reqs[k][2] - 1) * (reqs[k][3] + reqs[k][4] - 1)))}:
+            _, an, bn, aw, bw = reqs[big]
+            ta = torch.zeros(an * aw + bn * bw, dtype=torch.int64, device=dev)
+            tz = torch.empty((an + bn - 1) * (aw + bw + 1), dtype=torch.int64, device=dev)
+            ctx.fmpz_poly_mul_device_list(
+                [FmpzMulReq(tz.data_ptr(), aw + bw + 1, 0, an + bn - 1, ta.data_ptr(), aw, an,
+                            ta.data_ptr() + 8 * an * aw, bw, bn)], [configs[big]], s)
+            stream.synchronize()
+            del ta, tz
 
     def fz_size(k):
         _, an, bn, aw, bw = reqs[k]

@@ -263,18 +263,20 @@ class CostModel:
                     out[n] = m[best][0]
         return out
 
-    def choose_stream(self, reqs, class_margin=0.05, flag_margin=None):
+    def choose_stream(self, reqs, class_margin=0.05, flag_margin=None, alone_points=1 << 20):
         """Configurations for a mixed request stream: plain transforms chosen
         per class of the fixed rule (choose_classes; mpn requests then share
         planned batches as under the rule), and an mpn request moved to a
-        flagged configuration (run alone: THREE, SPLIT, a forced row-pass
-        width) only where the model predicts at least flag_margin (default:
-        the model's decision margin) below the class choice."""
+        THREE or SPLIT configuration (run alone) only where its transform has
+        at least `alone_points` points (a product that fills the GPU by
+        itself, so leaving the batch costs nothing) and the model predicts at
+        least flag_margin (default: the model's decision margin) below the
+        class choice.  The row-pass width flags stay with the launch rule."""
         if flag_margin is None:
             flag_margin = self.margin
         out = self.choose_classes(reqs, class_margin)
-        idx = [n for n, r in enumerate(reqs) if r[0] == 0]
-        flagged = [[c for c in candidates(reqs[n], True) if c.flags] for n in idx]
+        idx = [n for n, r in enumerate(reqs) if r[0] == 0 and transform_points(out[n]) >= alone_points]
+        flagged = [[c for c in candidates(reqs[n], True) if c.flags & (FLAG_THREE | FLAG_SPLIT)] for n in idx]
         rows, own = [], []
         for n, fl in zip(idx, flagged):
             if fl:

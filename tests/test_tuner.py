@@ -162,12 +162,13 @@ def test_choose_stream_flag_override():
     """In a stream, an mpn request moves to a flagged configuration only where
     the predicted saving over its class's choice reaches the margin;
     integer-polynomial requests take no flags."""
-    reqs = [(0, 3 << 20, 3 << 20), (0, 1000, 900), (1, 300, 200, 2, 2)]
+    reqs = [(0, 3 << 20, 3 << 20), (0, 1000, 900), (1, 300, 200, 2, 2), (0, 3 << 10, 3 << 10)]
     m = tuner.CostModel.__new__(tuner.CostModel)
     m.margin = 0.10
     m.net = _FakeFlagNet(-0.3)             # THREE predicted 26% faster
     out = m.choose_stream(reqs, class_margin=0.05)
     assert out[0].flags == FB.FLAG_THREE
     assert out[1].key() == tuner.default_config(reqs[1]).key() and out[2].flags == 0
+    assert out[3].flags == 0               # a small product stays in the batch
     m.net = _FakeFlagNet(-0.05)            # 5% faster: below the margin
     assert m.choose_stream(reqs, class_margin=0.05)[0].flags == 0
