@@ -240,7 +240,7 @@ def train_cost_model(ctx):
     from flint_b200.workload import request_stream, uneven_batch
     t0 = time.perf_counter()
     train = [(0, a, b) for a, b in uneven_batch(BATCH_SEED + 1, 160)]
-    train += request_stream(STREAM_SEED + 1, 96)
+    train += request_stream(STREAM_SEED + 1, 192)
     tun = tuner.Autotuner(ctx, reps=3, batched=True)
     X, t = tuner.dataset(tun, train)
     t_tune = time.perf_counter() - t0
@@ -254,7 +254,8 @@ def train_cost_model(ctx):
             "fit_s": time.perf_counter() - t0, "fit_mse_log_ms": loss,
             "decision_margin": model.margin, "class_margin": CLASS_MARGIN,
             "decisions": "per class of the fixed rule (requests of one kind and one rule configuration), by "
-                         "the model's summed prediction over the class (class_margin); in the request stream "
+                         "the model's summed prediction over the class (class_margin for mpn classes, "
+                         "decision_margin for integer-polynomial ones); in the request stream "
                          "an mpn request moves to a flagged configuration (run alone) only where the model "
                          "predicts decision_margin below its class's choice",
             "network": "%d -> 64 -> 64 -> 64 -> 1 ReLU fp32, Adam, library CUDA kernels" % tuner.N_FEATURES,

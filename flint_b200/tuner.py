@@ -230,7 +230,7 @@ class CostModel:
     def fit(self, X, t, epochs=300, batch=256, lr=2e-3, seed=7):
         return self.net.train(X, t, epochs=epochs, batch=batch, lr=lr, seed=seed)
 
-    def choose_classes(self, reqs, margin=0.05):
+    def choose_classes(self, reqs, margin=0.05, margin_fmpz=None):
         """Configurations for requests run as one planned batch (plain
         transforms), decided per class: the requests whose fixed-rule
         configuration is the same form a class, and the class moves as a
@@ -238,7 +238,11 @@ class CostModel:
         requests is least, where that total is at least `margin` below the
         rule's.  Summing over a class averages out the model's per-request
         error, and moving a class whole keeps the batch's classes as
-        populated as the rule's."""
+        populated as the rule's.  Integer-polynomial classes (products
+        that run one after another, never batched) take margin_fmpz
+        (default: the model's decision margin)."""
+        if margin_fmpz is None:
+            margin_fmpz = self.margin
         cands = [candidates(r, False) for r in reqs]
         rows = [features(r, c) for r, cs in zip(reqs, cands) for c in cs]
         pred = np.exp(self.net.predict(np.array(rows, dtype=np.float32)).astype(np.float64))
@@ -258,7 +262,7 @@ class CostModel:
                 continue
             tot = {key: sum(m[key][1] for _, m in members) for key in common}
             best = min(tot, key=tot.get)
-            if tot[best] <= (1.0 - margin) * tot[dk]:
+            if tot[best] <= (1.0 - (margin if gk[0] == 0 else margin_fmpz)) * tot[dk]:
                 for n, m in members:
                     out[n] = m[best][0]
         return out

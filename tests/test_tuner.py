@@ -136,6 +136,7 @@ def test_choose_classes_moves_whole_classes():
     that total saves at least the margin."""
     reqs = [(0, 100000 + 37 * k, 60000 + 11 * k) for k in range(12)] + [(0, 3000, 2000)] * 5
     m = tuner.CostModel.__new__(tuner.CostModel)
+    m.margin = 0.10
     m.net = _FakeNet(-3.0)                 # longer rows predicted faster
     out = m.choose_classes(reqs, margin=0.05)
     for r, c in zip(reqs, out):
