@@ -57,4 +57,67 @@ k_fmpz_crt(const uint32_t* __restrict__ res, int logM, uint64_t Ly, uint32_t S, 
     }
 }
 
+// The same coefficients, J = max(1, min(256, FZ_CRT_POS / S)) per block
+// (slot strides S <= FZ_CRT_POS): the block first recombines every chunk
+// position of its J coefficients by CRT -- one thread per position, so the
+// residue loads are coalesced and all positions are in flight at once -- into
+// shared memory, then one thread per coefficient runs k_fmpz_crt's limb loop
+// on those values.  k_fmpz_crt ran one thread per coefficient over all its
+// positions (a wide coefficient is a long chain of dependent loads, and a
+// product has few coefficients per SM).
+constexpr uint32_t FZ_CRT_POS = 2048;
+
+template <int NP>
+__global__ void __launch_bounds__(256)
+k_fmpz_crt_tiled(const uint32_t* __restrict__ res, int logM, uint64_t Ly, uint32_t S, uint32_t J,
+                 uint64_t zl, uint64_t zh, uint32_t zw, uint64_t* __restrict__ z, CrtConst K)
+{
+    __shared__ uint64_t sc0[FZ_CRT_POS], sc1[FZ_CRT_POS], sc2[FZ_CRT_POS];
+    const uint64_t j0 = zl + (uint64_t)blockIdx.x * J;
+    if (j0 >= zh) return;
+    const uint32_t nj = (uint32_t)(zh - j0 < J ? zh - j0 : J);
+    const uint64_t p0 = j0 * S;
+    const uint32_t npos = nj * S;
+    for (uint32_t t = threadIdx.x; t < npos; t += blockDim.x) {
+        const uint64_t n = p0 + t;
+        uint64_t c0 = 0, c1 = 0, c2 = 0;
+        if (n < Ly) {
+            uint32_t y[NP];
+#pragma unroll
+            for (int jp = 0; jp < NP; jp++) y[jp] = res[((size_t)jp << logM) + n];
+            crt_values<NP>(y, K, c0, c1, c2);
+            if (NP == 5) c2 = (uint64_t)(int64_t)(int32_t)(uint32_t)c2;   // 160-bit sign
+        }
+        sc0[t] = c0;
+        sc1[t] = c1;
+        sc2[t] = c2;
+    }
+    __syncthreads();
+    for (uint32_t q = threadIdx.x; q < nj; q += blockDim.x) {
+        uint64_t* __restrict__ out = z + (j0 + q - zl) * zw;
+        const uint32_t base = q * S;
+        uint64_t mid1 = 0, hi1 = 0, hi2 = 0;
+        __int128 carry = 0;
+        const uint32_t top = S + 2;
+        for (uint32_t u = 0; u < zw; u++) {
+            uint64_t c0 = 0, c1 = 0, c2 = 0;
+            if (u < S) {
+                c0 = sc0[base + u];
+                c1 = sc1[base + u];
+                c2 = sc2[base + u];
+            }
+            if (u < top) {
+                const __int128 acc = carry + (__int128)c0 + (__int128)mid1 + (__int128)(int64_t)hi2;
+                out[u] = (uint64_t)acc;
+                carry = acc >> 64;
+            } else {
+                out[u] = (uint64_t)(int64_t)carry;
+            }
+            hi2 = hi1;
+            hi1 = c2;
+            mid1 = c1;
+        }
+    }
+}
+
 }  // namespace fb

@@ -155,6 +155,20 @@ struct FzShape {
     uint32_t wa, wb;  // limbs per coefficient of a and of b
 };
 
+// Residue (times 2^-32) of chunk k of coefficient i of an xn-coefficient
+// polynomial with w limbs per coefficient (zero beyond the coefficient's
+// limbs or the polynomial).
+__device__ __forceinline__ uint32_t load_chunk(const uint64_t* __restrict__ x, uint32_t i, uint32_t k,
+                                               uint64_t xn, uint32_t w, const PrimeInfo& P)
+{
+    if (k >= w || i >= xn) return 0u;
+    const uint64_t v = x[(size_t)i * w + k];
+    uint32_t r = limb_redc(v, P.p, P.pneg_inv, P.c32);
+    // a negative top limb stands for v - 2^64, and 2^64 2^-32 = 2^32
+    if (k == w - 1 && (int64_t)v < 0) r = sub_mod(r, P.c32, P.p);
+    return r;
+}
+
 // Residue (times 2^-32) of operand element n.  Limb source: limb n of an
 // xn-limb integer.  Coefficient source: chunk (n mod S) of coefficient n / S
 // of an xn-coefficient polynomial with w limbs per coefficient.
@@ -167,12 +181,7 @@ __device__ __forceinline__ uint32_t load_residue(const uint64_t* __restrict__ x,
     } else {
         const uint32_t nn = (uint32_t)n;      // y-lengths stay below 2^32
         const uint32_t i = nn / S, k = nn - i * S;
-        if (k >= w || i >= xn) return 0u;
-        const uint64_t v = x[(size_t)i * w + k];
-        uint32_t r = limb_redc(v, P.p, P.pneg_inv, P.c32);
-        // a negative top limb stands for v - 2^64, and 2^64 2^-32 = 2^32
-        if (k == w - 1 && (int64_t)v < 0) r = sub_mod(r, P.c32, P.p);
-        return r;
+        return load_chunk(x, i, k, xn, w, P);
     }
 }
 
@@ -246,6 +255,35 @@ fwd_cols_body(DevTables T, const uint64_t* __restrict__ a, uint64_t an,
 #pragma unroll 8
             for (int k = 0; k < K; k++, px += step)
                 d[k * PNT] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
+        } else if constexpr (FZ) {
+            // integer-polynomial source: n advances by `step`, so its slot
+            // n / S and chunk n mod S advance by fixed amounts (one division
+            // per thread instead of one per element)
+            const uint32_t S = fz.S;
+            uint32_t ci = (uint32_t)n / S, ck = (uint32_t)n - ci * S;
+            const uint32_t sq = (uint32_t)step / S, sr = (uint32_t)step - sq * S;
+            // the limb offset ci w + ck advances the same way
+            size_t off = (size_t)ci * xw + ck;
+            const size_t doff = (size_t)sq * xw + sr;
+#pragma unroll 8
+            for (int k = 0; k < R * GG / NT; k++) {
+                uint32_t r = 0;
+                if (ck < xw && ci < xn) {
+                    const uint64_t v = x[off];
+                    r = limb_redc(v, p, P.pneg_inv, P.c32);
+                    // a negative top limb stands for v - 2^64
+                    if (ck == xw - 1 && (int64_t)v < 0) r = sub_mod(r, P.c32, p);
+                }
+                d[k * PNT] = r;
+                ci += sq;
+                ck += sr;
+                off += doff;
+                if (ck >= S) {
+                    ck -= S;
+                    ci++;
+                    off -= (size_t)(S - xw);   // S >= xw: one slot on, minus the chunks it carries
+                }
+            }
         } else {
 #pragma unroll 8
             for (int k = 0; k < R * GG / NT; k++, n += step)
