@@ -38,6 +38,39 @@ def test_vs_python(ctx, an, bn, ba, bb):
     assert _gpu_ints(ctx, a, b) == want
 
 
+@pytest.mark.parametrize("an,bn,ba,bb", [
+    (40, 30, 250, 300),              # slot stride S = 4 + 5 - 1 = 8: one thread per coefficient
+    (40, 30, 300, 300),              # S = 9: the tiled CRT, 227 coefficients per block
+    (3, 2, 65535, 65536),            # S = 1024 + 1025 - 1 = 2048: tiled, one coefficient per block
+    (3, 2, 65536, 65536),            # S = 2049: one thread per coefficient again
+])
+def test_crt_layout_boundaries(ctx, an, bn, ba, bb):
+    """Both integer-polynomial CRT kernels at the slot strides where the
+    library switches between them, whole products and windows that start
+    and end inside a block's run of coefficients."""
+    a = O.rand_fmpz_raw(an + ba, an, ba)
+    b = O.rand_fmpz_raw(bn + 3 * bb, bn, bb)
+    full = O.fmpz_poly_mul_python(O.raw_to_ints(a), O.raw_to_ints(b))
+    zn = len(full)
+    assert _gpu_ints(ctx, a, b) == full
+    for zl, zh in [(1, zn), (zn // 2, zn - 1), (zn - 1, zn + 2)]:
+        want = [full[k] if k < zn else 0 for k in range(zl, zh)]
+        assert _gpu_ints(ctx, a, b, zl, zh) == want, (zl, zh)
+
+
+def test_crt_tiled_many_blocks(ctx):
+    """The tiled CRT over many blocks (S = 9, 227 coefficients each), with
+    windows that start and end mid-block, and a squaring."""
+    a = O.rand_fmpz_raw(77, 400, 300)
+    b = O.rand_fmpz_raw(78, 350, 290)
+    full = O.fmpz_poly_mul_python(O.raw_to_ints(a), O.raw_to_ints(b))
+    zn = len(full)
+    for zl, zh in [(0, zn), (5, 460), (226, 229), (227, 681), (zn - 300, zn + 10)]:
+        want = [full[k] if k < zn else 0 for k in range(zl, zh)]
+        assert _gpu_ints(ctx, a, b, zl, zh) == want, (zl, zh)
+    assert _gpu_ints(ctx, a, a) == O.fmpz_poly_mul_python(O.raw_to_ints(a), O.raw_to_ints(a))
+
+
 def test_windows_and_zero_fill(ctx):
     a = O.rand_fmpz_raw(1, 50, 90)
     b = O.rand_fmpz_raw(2, 30, 200)
