@@ -465,12 +465,17 @@ static const inv_cols_fn INV_COLS_C14 = k_inv_cols<11, tmpl_cols<11>(), 14>;
 
 // columns of 3 2^r points, r = 5 .. 10 (index r - 5)
 typedef void (*fwd_cols3_fn)(DevTables, const uint64_t *, uint64_t, const uint64_t *, uint64_t, uint32_t *,
-                             uint32_t *, int, int, const uint32_t *, int);
+                             uint32_t *, int, int, const uint32_t *, int, FzShape);
 typedef void (*inv_cols3_fn)(DevTables, uint32_t *, int, int);
 constexpr int LOG3_RMIN = 5, LOG3_RMAX = 10;
 static const fwd_cols3_fn FWD_COLS3[6] = {
     k_fwd_cols3<5, cols_per_tile3(5)>, k_fwd_cols3<6, cols_per_tile3(6)>, k_fwd_cols3<7, cols_per_tile3(7)>,
     k_fwd_cols3<8, cols_per_tile3(8)>, k_fwd_cols3<9, cols_per_tile3(9)>, k_fwd_cols3<10, cols_per_tile3(10)>};
+// the same for integer-polynomial operands
+static const fwd_cols3_fn FWD_COLS3_FZ[6] = {
+    k_fwd_cols3<5, cols_per_tile3(5), true>, k_fwd_cols3<6, cols_per_tile3(6), true>,
+    k_fwd_cols3<7, cols_per_tile3(7), true>, k_fwd_cols3<8, cols_per_tile3(8), true>,
+    k_fwd_cols3<9, cols_per_tile3(9), true>, k_fwd_cols3<10, cols_per_tile3(10), true>};
 static const inv_cols3_fn INV_COLS3[6] = {
     k_inv_cols3<5, cols_per_tile3(5)>, k_inv_cols3<6, cols_per_tile3(6)>, k_inv_cols3<7, cols_per_tile3(7)>,
     k_inv_cols3<8, cols_per_tile3(8)>, k_inv_cols3<9, cols_per_tile3(9)>, k_inv_cols3<10, cols_per_tile3(10)>};
@@ -614,6 +619,7 @@ static int configure_kernels()
     CU(cudaFuncSetAttribute(INV_COLS_C14, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     for (int r = 0; r < 6; r++) {
         CU(cudaFuncSetAttribute(FWD_COLS3[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
+        CU(cudaFuncSetAttribute(FWD_COLS3_FZ[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
         CU(cudaFuncSetAttribute(INV_COLS3[r], cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024));
     }
     for (int c = ROWS16_MIN_LOGC; c <= LOG_MAXC; c++)
@@ -1040,10 +1046,12 @@ static uint32_t *launch_transforms(const Ctx *X, const LaunchShape &L, int np, c
 // Transform of M = 3 2^k points (k - 13 in [LOG3_RMIN, LOG3_RMAX]): columns of
 // 3 2^(k - 13) points with a radix-3 stage, 2^13-point rows; residue planes
 // of 2^logMs words (logMs = k + 2).  The pointwise scale is folded into b's
-// twist as in launch_transforms (squarings keep it in the row pass).
+// twist as in launch_transforms (squarings keep it in the row pass).  With fz
+// the operands are integer polynomials (an, bn coefficients).
 static void launch_transforms3(const Ctx *X, int k, int logMs, const uint64_t *a, uint64_t an,
                                const uint64_t *b, uint64_t bn, uint32_t *ra, uint32_t *rb, bool sq,
-                               cudaStream_t st, TimingRecord *tr, cudaEvent_t b_ready)
+                               cudaStream_t st, TimingRecord *tr, cudaEvent_t b_ready,
+                               const FzShape *fz = nullptr)
 {
     const int np = NP3, r = k - LOGC3;
     const int G = cols_per_tile3(r);
@@ -1051,8 +1059,8 @@ static void launch_transforms3(const Ctx *X, int k, int logMs, const uint64_t *a
     const size_t smem = (size_t)(padw(3 * (1 << r) * G) + 32) * sizeof(uint32_t);
     const uint32_t *sc = scale3_ptr(X, k);
     if (b_ready) cudaStreamWaitEvent(st, b_ready, 0);
-    FWD_COLS3[r - LOG3_RMIN]<<<dim3(np, C / G, sq ? 1 : 2), 512, smem, st>>>(X->T, a, an, b, bn, ra, rb, logMs, k,
-                                                                             sc, sq ? 0 : 2);
+    (fz ? FWD_COLS3_FZ : FWD_COLS3)[r - LOG3_RMIN]<<<dim3(np, C / G, sq ? 1 : 2), 512, smem, st>>>(
+        X->T, a, an, b, bn, ra, rb, logMs, k, sc, sq ? 0 : 2, fz ? *fz : FzShape{1, 1, 1});
     timing_mark(tr, 1, st);
     const LaunchShape L = make_shape(logMs, LOGC3);   // row launch shape (one 2^13-point row per item)
     const int items = rows * np;
@@ -1799,7 +1807,6 @@ int gpu_mul_reference_rule(int kind, gpu_ulong an, gpu_ulong aw, gpu_ulong bn, g
     int rc = 0;
     for (int dnp = 0; dnp <= 1; dnp++)
         for (int fl = 0; fl <= GPU_MUL_FLAG_THREE; fl += GPU_MUL_FLAG_THREE) {
-            if (kind != 0 && fl) continue;
             gpu_mul_config c{GPU_MUL_ROUTE_NTT, 0, 0, 0, fl};
             rc = kind == 0 ? gpu_mpn_mul_config_resolve(an, bn, &c)
                            : gpu_fmpz_poly_mul_config_resolve(an, aw, bn, bw, &c);
@@ -1973,7 +1980,7 @@ int gpu_fmpz_poly_mul_config_resolve(gpu_ulong an, gpu_ulong aw, gpu_ulong bn, g
     if (rc) return rc;
     cfg->np = P.np;
     cfg->logM = P.logM;
-    cfg->logC = P.L.S.logC;
+    cfg->logC = P.k3 ? LOGC3 : P.L.S.logC;
     return 0;
 }
 

@@ -76,13 +76,15 @@ __device__ __forceinline__ void twist32_3(uint32_t (&x)[32], uint32_t col, int s
 // Forward column pass of a 3 2^k-point transform: limbs -> residues, radix-3
 // stage, three length-2^LOGR transforms, twist.  grid = (np, C / G, operands);
 // block 512; smem = padw(3 2^LOGR G) + 32 words.  logMs: log2 of the residue
-// plane stride; rows of C = 2^LOGC3 points.  fscale / fmask as in k_fwd_cols.
+// plane stride; rows of C = 2^LOGC3 points.  fscale / fmask as in k_fwd_cols;
+// FZ: integer-polynomial operands (an, bn coefficients, chunk layout fz) as in
+// k_fwd_cols.
 constexpr int LOGC3 = 13;
-template <int LOGR, int G>
+template <int LOGR, int G, bool FZ = false>
 __global__ void __launch_bounds__(512)
 k_fwd_cols3(DevTables T, const uint64_t* __restrict__ a, uint64_t an, const uint64_t* __restrict__ b,
             uint64_t bn, uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int logMs, int k,
-            const uint32_t* __restrict__ fscale, int fmask)
+            const uint32_t* __restrict__ fscale, int fmask, FzShape fz)
 {
     extern __shared__ uint32_t sm[];
     constexpr int RP = 1 << LOGR;           // R' (power-of-two part of the column)
@@ -107,17 +109,47 @@ k_fwd_cols3(DevTables T, const uint64_t* __restrict__ a, uint64_t an, const uint
         const int u_t = t / G, c = t & (G - 1);
         const uint64_t n0 = (uint64_t)u_t * C + i0 + c;
         static_assert(RP * G == 8192, "tiles of 3 2^13 words");
-        constexpr int lstep = LOGR - 4 + LOGC3;   // log2(ROWS_PER C): ROWS_PER = 2^(LOGR - 4)
-        int kin = 0;
-        if (n0 < xn) {
-            const uint64_t q = ((xn - n0 - 1) >> lstep) + 1;
-            kin = q < (uint64_t)K ? (int)q : K;
-        }
-        const uint64_t* px = x + n0;
         uint32_t* d = sm + padw(u_t * G) + c;
+        if constexpr (!FZ) {
+            constexpr int lstep = LOGR - 4 + LOGC3;   // log2(ROWS_PER C): ROWS_PER = 2^(LOGR - 4)
+            int kin = 0;
+            if (n0 < xn) {
+                const uint64_t q = ((xn - n0 - 1) >> lstep) + 1;
+                kin = q < (uint64_t)K ? (int)q : K;
+            }
+            const uint64_t* px = x + n0;
 #pragma unroll 8
-        for (int k = 0; k < K; k++, px += (size_t)ROWS_PER * C)
-            d[k * (ROWS_PER * G + ROWS_PER * G / 32)] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
+            for (int k = 0; k < K; k++, px += (size_t)ROWS_PER * C)
+                d[k * (ROWS_PER * G + ROWS_PER * G / 32)] = k < kin ? limb_redc(*px, p, P.pneg_inv, P.c32) : 0u;
+        } else {
+            // chunk (n mod S) of coefficient n / S, with the slot, the chunk
+            // and the limb offset advanced incrementally (as in k_fwd_cols)
+            const uint32_t S = fz.S, xw = opb ? fz.wb : fz.wa;
+            const uint32_t step = (uint32_t)ROWS_PER * C;
+            uint32_t ci = (uint32_t)n0 / S, ck = (uint32_t)n0 - ci * S;
+            const uint32_t sq = step / S, sr = step - sq * S;
+            size_t off = (size_t)ci * xw + ck;
+            const size_t doff = (size_t)sq * xw + sr;
+#pragma unroll 8
+            for (int k = 0; k < K; k++) {
+                uint32_t r = 0;
+                if (ck < xw && ci < xn) {
+                    const uint64_t v = x[off];
+                    r = limb_redc(v, p, P.pneg_inv, P.c32);
+                    // a negative top limb stands for v - 2^64
+                    if (ck == xw - 1 && (int64_t)v < 0) r = sub_mod(r, P.c32, p);
+                }
+                d[k * (ROWS_PER * G + ROWS_PER * G / 32)] = r;
+                ci += sq;
+                ck += sr;
+                off += doff;
+                if (ck >= S) {
+                    ck -= S;
+                    ci++;
+                    off -= (size_t)(S - xw);   // S >= xw
+                }
+            }
+        }
     }
     __syncthreads();
     // radix-3 stage: (u1, u1 + R', u1 + 2R') -> t0, t1 omega^u1, t2 omega^(2 u1)

@@ -89,12 +89,14 @@ def candidates(r, flags=True):
                     out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, np_, logM, logC), aw, bw))
                 except GpuFftSmallError:
                     pass
-    if flags and kind == 0:
-        for fl in (FLAG_THREE, FLAG_SPLIT):
+    if flags:
+        # 3 2^k lengths for both kinds; splitting for mpn products only
+        for fl in ((FLAG_THREE, FLAG_SPLIT) if kind == 0 else (FLAG_THREE,)):
             try:
-                out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, base.np, base.logM, 0, fl)))
+                out.append(resolve_config(kind, an, bn, MulConfig(ROUTE_NTT, base.np, base.logM, 0, fl), aw, bw))
             except GpuFftSmallError:
                 pass
+    if flags and kind == 0:
         # the row pass at 16 and at 32 points per thread (the launch rule
         # picks one of them by the warps the launch has)
         for fl in (FLAG_ROWS16, FLAG_ROWS32):
@@ -270,16 +272,18 @@ class CostModel:
     def choose_stream(self, reqs, class_margin=0.05, flag_margin=None, alone_points=1 << 20):
         """Configurations for a mixed request stream: plain transforms chosen
         per class of the fixed rule (choose_classes; mpn requests then share
-        planned batches as under the rule), and an mpn request moved to a
-        THREE or SPLIT configuration (run alone) only where its transform has
-        at least `alone_points` points (a product that fills the GPU by
-        itself, so leaving the batch costs nothing) and the model predicts at
-        least flag_margin (default: the model's decision margin) below the
-        class choice.  The row-pass width flags stay with the launch rule."""
+        planned batches as under the rule), and a request moved to a THREE
+        (3 2^k-point) or, for mpn, SPLIT configuration only where the model
+        predicts at least flag_margin (default: the model's decision margin)
+        below the class choice -- for an mpn request (which then runs alone)
+        also only where its transform has at least `alone_points` points (a
+        product that fills the GPU by itself, so leaving the batch costs
+        nothing).  The row-pass width flags stay with the launch rule."""
         if flag_margin is None:
             flag_margin = self.margin
         out = self.choose_classes(reqs, class_margin)
-        idx = [n for n, r in enumerate(reqs) if r[0] == 0 and transform_points(out[n]) >= alone_points]
+        # integer-polynomial products run alone anyway: any size may move
+        idx = [n for n, r in enumerate(reqs) if r[0] == 1 or transform_points(out[n]) >= alone_points]
         flagged = [[c for c in candidates(reqs[n], True) if c.flags & (FLAG_THREE | FLAG_SPLIT)] for n in idx]
         rows, own = [], []
         for n, fl in zip(idx, flagged):

@@ -402,6 +402,9 @@ typedef struct {
    flags = 0):
    THREE: run a transform of 3 2^(logM - 2) points (valid when the product
      fits it, five primes, 2^18 <= 3 2^(logM - 2) / 3 <= 2^23; rows of 2^13);
+     also the one flag integer-polynomial products take (their chunk product
+     must fit it), and both kinds take that length by default, without a
+     configuration, where it fits;
    SPLIT: run the product as chunks of the long operand against one
      transform of the short one, chunk length by the default rule (valid when
      that rule splits the product);

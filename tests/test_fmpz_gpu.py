@@ -201,3 +201,42 @@ def test_golden_fmpz(ctx, golden, name):
         assert ["%016x" % int(v) for v in flat] == case["full"]
     else:
         assert O.digest(flat) == case["digest"] and len(flat) == case["len"]
+
+
+@pytest.mark.parametrize("an,bn,aw,bw,sq", [
+    (4500, 4500, 32, 32, False),      # 8999 x 63 positions: 3 2^18 points instead of 2^20
+    (9000, 5000, 20, 20, False),      # 13999 x 39: 3 2^18
+    (17000, 17000, 32, 32, False),    # 33999 x 63: 3 2^20 instead of 2^22
+    (4500, 4500, 32, 32, True),       # a squaring on 3 2^18 points
+])
+def test_three_length_equals_power_of_two(ctx, an, bn, aw, bw, sq):
+    """Integer-polynomial products on 3 2^k-point transforms (the default
+    without a configuration, and the THREE flag) equal the same products on
+    the power-of-two transform, coefficient for coefficient; the largest
+    request-size test checks the 3 2^23-point case against the reference."""
+    torch = pytest.importorskip("torch")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(an + 3 * bn + aw)
+    a = torch.randint(-(1 << 63), (1 << 63) - 1, (an * aw,), dtype=torch.int64, device="cuda", generator=g)
+    b = a if sq else torch.randint(-(1 << 63), (1 << 63) - 1, (bn * bw,), dtype=torch.int64, device="cuda",
+                                   generator=g)
+    if sq:
+        bn, bw = an, aw
+    zw, zn = aw + bw + 1, an + bn - 1
+    plain = FB.resolve_config(1, an, bn, None, aw, bw)
+    assert plain.flags == 0
+    three = FB.resolve_config(1, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE), aw, bw)
+    assert three.logM == plain.logM and three.logC == 13
+    s = torch.cuda.current_stream()
+    outs = []
+    for cfg in (plain, three, None):
+        z = torch.full((zn * zw,), -1, dtype=torch.int64, device="cuda")
+        if cfg is None:
+            ctx.fmpz_poly_mul_device(z.data_ptr(), zw, 0, zn, a.data_ptr(), aw, an, b.data_ptr(), bw, bn,
+                                     s.cuda_stream)
+        else:
+            ctx.fmpz_poly_mul_device_config(z.data_ptr(), zw, 0, zn, a.data_ptr(), aw, an, b.data_ptr(), bw,
+                                            bn, cfg, s.cuda_stream)
+        s.synchronize()
+        outs.append(z.cpu())
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])

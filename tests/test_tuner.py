@@ -28,7 +28,9 @@ def test_candidates_are_valid_and_include_default(r):
     has_bc_batch = any(c.route == FB.ROUTE_BASECASE for c in tuner.candidates(r, flags=False))
     assert has_bc_batch == (kind == 0 and min(an, bn) <= tuner.BASECASE_BATCH_MAX)
     for c in cs:
-        if c.route == FB.ROUTE_NTT:
+        if c.route == FB.ROUTE_NTT and c.flags & FB.FLAG_THREE:
+            assert c.logC == 13                  # 3 2^k-point transforms: 2^13-point rows
+        elif c.route == FB.ROUTE_NTT:
             assert max(5, c.logM - 11) <= c.logC <= min(c.logM, 14)
             assert c.logM >= 14 or c.logM - c.logC <= 4
         f = tuner.features(r, c)
@@ -91,8 +93,15 @@ def test_configuration_flags():
             FB.resolve_config(0, an, bn, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, fl))
     with pytest.raises(FB.GpuFftSmallError):                     # six primes: no cube roots
         FB.resolve_config(0, 3 << 22, 3 << 22, FB.MulConfig(FB.ROUTE_NTT, 6, 0, 0, FB.FLAG_THREE))
-    with pytest.raises(FB.GpuFftSmallError):                     # integer polynomials take none
+    with pytest.raises(FB.GpuFftSmallError):                     # too short for the radix-3 kernels
         FB.resolve_config(1, 300, 200, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE), 2, 2)
+    # integer polynomials: a chunk product of 8999 x 63 positions fits 3 2^18
+    fz3 = FB.resolve_config(1, 4500, 4500, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, FB.FLAG_THREE), 32, 32)
+    assert fz3.key() == (FB.ROUTE_NTT, 5, 20, 13, FB.FLAG_THREE)
+    for fl in (FB.FLAG_SPLIT, FB.FLAG_ROWS16):                  # the only flag they take is THREE
+        with pytest.raises(FB.GpuFftSmallError):
+            FB.resolve_config(1, 4500, 4500, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, fl), 32, 32)
+    assert tuner.reference_rule((1, 4500, 4500, 32, 32)).flags == FB.FLAG_THREE
     for fl in (FB.FLAG_ROWS16, FB.FLAG_ROWS32):                  # row pass width: kept as given
         assert FB.resolve_config(0, 1 << 16, 1 << 16, FB.MulConfig(FB.ROUTE_NTT, 0, 0, 0, fl)).flags == fl
     assert tuner.reference_rule((0, 3 << 22, 3 << 22)).flags == FB.FLAG_THREE
