@@ -41,6 +41,8 @@ WORKLOADS = {
     "mpn22": (1 << 22, 1 << 22, "mpn_mul 2^22 x 2^22 limbs, uniform random limbs"),
     # the small-product (latency-bound) case, 2^17-point transforms
     "mpn16": (1 << 16, 1 << 16, "mpn_mul 2^16 x 2^16 limbs, uniform random limbs"),
+    # a 3 2^23-point (truncated-length) transform
+    "mpn3x22": (3 << 22, 3 << 22, "mpn_mul 3 2^22 x 3 2^22 limbs, uniform random limbs"),
 }
 NS_LIMB_BITS = 64
 
