@@ -73,6 +73,45 @@ __device__ __forceinline__ void twist32_3(uint32_t (&x)[32], uint32_t col, int s
     }
 }
 
+// The strided passes of the three thirds of a column tile (three independent
+// transforms of 2^LOGL points down G columns, `third` words apart): each pass
+// runs on all three before one barrier, instead of three pass sequences with
+// a barrier after every pass.
+template <int LOGL, int G, int QMAX, int H, int REM>
+__device__ __forceinline__ void gs_passes3(uint32_t* sm, int third, const uint2* __restrict__ tw, uint32_t p)
+{
+    if constexpr (REM > 0) {
+        constexpr int Q = balanced_pass<REM, QMAX>();
+#pragma unroll 1
+        for (int t = 0; t < 3; t++) gs_pass_smem<LOGL, Q, H, G>(sm + t * third, 1, tw, p);
+        __syncthreads();
+        gs_passes3<LOGL, G, QMAX, (H >> Q), REM - Q>(sm, third, tw, p);
+    }
+}
+template <int LOGL, int G, int QMAX, int H, int REM>
+__device__ __forceinline__ void ct_passes3(uint32_t* sm, int third, const uint2* __restrict__ twi, uint32_t p)
+{
+    if constexpr (REM > 0) {
+        constexpr int Q = balanced_pass<REM, QMAX>();
+#pragma unroll 1
+        for (int t = 0; t < 3; t++) ct_pass_smem<LOGL, Q, H, G>(sm + t * third, 1, twi, p);
+        __syncthreads();
+        ct_passes3<LOGL, G, QMAX, (H << Q), REM - Q>(sm, third, twi, p);
+    }
+}
+// as gs_strided_all / ct_strided_all with their column-layout defaults (QMAX
+// 4, the five lowest levels left to the register pass)
+template <int LOGL, int G>
+__device__ __forceinline__ void gs_strided_all3(uint32_t* sm, int third, const uint2* __restrict__ tw, uint32_t p)
+{
+    if constexpr (LOGL > 5) gs_passes3<LOGL, G, 4, (1 << (LOGL - 1)), LOGL - 5>(sm, third, tw, p);
+}
+template <int LOGL, int G>
+__device__ __forceinline__ void ct_strided_all3(uint32_t* sm, int third, const uint2* __restrict__ twi, uint32_t p)
+{
+    if constexpr (LOGL > 5) ct_passes3<LOGL, G, 4, (1 << 5), LOGL - 5>(sm, third, twi, p);
+}
+
 // Forward column pass of a 3 2^k-point transform: limbs -> residues, radix-3
 // stage, three length-2^LOGR transforms, twist.  grid = (np, C / G, operands);
 // block 512; smem = padw(3 2^LOGR G) + 32 words.  logMs: log2 of the residue
@@ -172,8 +211,7 @@ k_fwd_cols3(DevTables T, const uint64_t* __restrict__ a, uint64_t an, const uint
     }
     __syncthreads();
     const uint2* __restrict__ twf = T.twf + (size_t)j * TW_SZ;
-#pragma unroll 1
-    for (int t = 0; t < 3; t++) gs_strided_all<LOGR, G>(sm + padw(t * RP * G), 1, twf, p);
+    gs_strided_all3<LOGR, G>(sm, padw(RP * G), twf, p);
     const uint32_t fsc = (fmask >> (opb ? 1 : 0)) & 1 ? fscale[j] : 0u;
     const uint2* __restrict__ th3 = T.th3 + (size_t)j * TH3_SZ;
     const uint2* __restrict__ tl3 = T.tl3 + (size_t)j * TL_SZ;
@@ -228,8 +266,7 @@ k_inv_cols3(DevTables T, uint32_t* __restrict__ ra, int logMs, int k)
     }
     __syncthreads();
     const uint2* __restrict__ twi = T.twi + (size_t)j * TW_SZ;
-#pragma unroll 1
-    for (int t = 0; t < 3; t++) ct_strided_all<LOGR, G>(sm + padw(t * RP * G), 1, twi, p);
+    ct_strided_all3<LOGR, G>(sm, padw(RP * G), twi, p);
     __syncthreads();
     const uint2 cw = T.w3c[(size_t)j * 2 + 1];
     const uint2* __restrict__ tw3 = T.tw3i + (size_t)j * TW3_SZ;
